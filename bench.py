@@ -1,0 +1,382 @@
+"""Benchmark: D3Q19 collide-stream MLUPS on B200 (one JSON line on rank 0).
+
+Workload (default): D3Q19 TRT (Lambda = 1/4), 256^3 periodic box, Taylor-Green
+vortex (u0 = 0.05, rho = 1) plus seeded Gaussian velocity noise (sigma 1e-3),
+tau = 0.55, FP32 populations. One step = one fused pull collide-stream launch
+over the whole box. Inputs (1.27 GB per population buffer) are larger than L2,
+so no flush is needed between steps.
+
+value   MLUPS with the populations resident in HBM (CUDA events, max over ranks)
+e2e     MLUPS through the reference-facing C ABI (lbm_launch_step_gpu_*) with
+        host buffers: the pinned host field is copied in, K steps run, the
+        field is copied back, all inside the timed region
+roofline achieved HBM GB/s of the step kernel = 152 B/LU x cells / mean launch
+        time, against the measured copy bandwidth (MEASURED_PEAKS.json)
+
+`--impl reference` times LB-Cube's own CPU step (oracle/_ref, or the oracle
+restatement when the reference build is absent) on a bounded sample of the
+same workload and prints the same metric.
+
+Multi-GPU (torchrun): each rank runs the same box on its own GPU (replicas,
+weak scaling); value is the sum over ranks with the time taken as the max.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lb-cube_b200"))
+
+METRIC = "D3Q19 MLUPS, %HBM peak: FP32 vs FP16-store @L2err<=1e-3; adjoint cost/fwd"
+UNIT = "MLUPS"
+NX = NY = NZ = 256
+TAU = 0.55
+U0 = 0.05
+NOISE = 1e-3
+SEED = 20261203
+BYTES_PER_LU = 2 * 19 * 4  # read Q + write Q FP32 populations
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--size", type=int, default=256,
+                    help="cube edge; smaller sizes are for profiling captures only")
+    a = ap.parse_args()
+    global NX, NY, NZ
+    NX = NY = NZ = a.size
+    return a
+
+
+def config_dict():
+    return {
+        "workload": f"D3Q19 TRT (Lambda 1/4) {NX}^3 periodic, Taylor-Green u0 0.05 + N(0, 1e-3) "
+                    "velocity noise, tau 0.55, FP32 populations",
+        "lattice": "D3Q19", "collision": "TRT", "storage": "fp32",
+        "nx": NX, "ny": NY, "nz": NZ, "tau": TAU,
+        "l2": f"inputs larger than L2 ({19 * 4 * NX * NY * NZ / 1e9:.2f} GB per population buffer); no flush",
+        "parallelism": "replicas (one box per GPU)",
+    }
+
+
+# ----------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def committed_traffic(kernel_key):
+    """Per-launch DRAM bytes from a committed ncu summary, scaled to the bench box."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as fh:
+            return json.load(fh).get(kernel_key)
+    except (OSError, ValueError):
+        return None
+
+
+# ----------------------------------------------------------------------------
+# engine arm
+# ----------------------------------------------------------------------------
+def make_initial_state(torch, E, dev):
+    """Taylor-Green + seeded noise, rho = 1, built on the device and turned into
+    equilibrium populations by the engine's own init kernel."""
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED)
+    k = 2 * math.pi / NX
+    ax = torch.arange(NX, device=dev, dtype=torch.float64) * k
+    z, y, x = torch.meshgrid(ax, ax, ax, indexing="ij")
+    u = torch.empty((3, NZ, NY, NX), device=dev, dtype=torch.float64)
+    u[0] = U0 * torch.sin(x) * torch.cos(y) * torch.cos(z)
+    u[1] = -U0 * torch.cos(x) * torch.sin(y) * torch.cos(z)
+    u[2] = 0.0
+    u += NOISE * torch.randn(u.shape, generator=gen, device=dev, dtype=torch.float64)
+    del x, y, z
+    rho = torch.ones((NZ, NY, NX), device=dev, dtype=torch.float32)
+    u32 = u.to(torch.float32).contiguous()
+    del u
+    f = torch.empty((19, NZ, NY, NX), device=dev, dtype=torch.float32)
+    E.check(E.init_equilibrium_async("D3Q19", "float", rho, u32, f, NX, NY, NZ))
+    torch.cuda.synchronize()
+    return f
+
+
+def run_engine(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import lbcube as E
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    E.load()
+    omega = 1.0 / TAU
+    cells = NX * NY * NZ
+
+    f = make_initial_state(torch, E, dev)
+    g = torch.empty_like(f)
+
+    def step(cur, nxt):
+        return E.launch_step_gpu("D3Q19", "float", "TRT", cur, nxt, NX, NY, NZ, omega)
+
+    for _ in range(args.warmup):
+        E.check(step(f, g))
+        f, g = g, f
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    stream = torch.cuda.current_stream()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        rc = step(f, g)
+        f, g = g, f
+    t1.record(stream)
+    torch.cuda.synchronize()
+    E.check(rc)
+    clocks = sampler.stop() if sampler else None
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        dist.barrier()
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = cells * world * args.steps / (ms * 1e-3) / 1e6
+    achieved_gbs = BYTES_PER_LU * cells / (ms_per_step * 1e-3) / 1e9
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(f.shape, dtype=f.dtype, pin_memory=True)
+        host.copy_(f)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        f.copy_(host, non_blocking=True)
+        for _ in range(args.steps):
+            rc = step(f, g)
+            f, g = g, f
+        host.copy_(f, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        E.check(rc)
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        nbytes = f.numel() * f.element_size()
+        e2e = {"value": round(cells * world * args.steps / (ems * 1e-3) / 1e6, 1), "unit": UNIT,
+               "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
+               "note": "pinned host field copied in, K steps via lbm_launch_step_gpu_d3q19_float_trt, "
+                       "field copied back; copies amortised over K"}
+        del host
+
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_hbm_peak()
+    traffic = committed_traffic(f"d3q19_float_trt_{NX}")
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": config_dict(),
+        "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved_gbs / peak, 4),
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": BYTES_PER_LU * cells},
+        "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps,
+    }
+    return line
+
+
+# ----------------------------------------------------------------------------
+# CPU baseline (reference CPU path) and the reference arm
+# ----------------------------------------------------------------------------
+def _reference_lib():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    if O.REF.available:
+        return O, O.REF, "reference"
+    return O, O.ORACLE, "port"
+
+
+def cpu_sample(nz_sample, steps):
+    """Time `steps` serial step_cpu<D3Q19, float, TRT> calls on a 256 x 256 x
+    nz_sample periodic slab of the benchmark state (same per-cell work)."""
+    import numpy as np
+
+    O, lib, kind = _reference_lib()
+    n = NX * NY * nz_sample
+    rng = np.random.default_rng(SEED)
+    k = 2 * math.pi / NX
+    ax = np.arange(NX) * k
+    z, y, x = np.meshgrid(np.arange(nz_sample) * k, ax, ax, indexing="ij")
+    u = np.stack([U0 * np.sin(x) * np.cos(y) * np.cos(z), -U0 * np.cos(x) * np.sin(y) * np.cos(z),
+                  np.zeros_like(x)]).reshape(3, -1) + NOISE * rng.standard_normal((3, n))
+    f = O.init_equilibrium("D3Q19", np.ones(n), u, NX, NY, nz_sample, np.float32)
+    t = time.perf_counter()
+    O.step(f, "D3Q19", "TRT", NX, NY, nz_sample, 1 / TAU, steps=steps, lib=lib)
+    dt = time.perf_counter() - t
+    return n * steps / dt / 1e6, kind, dt
+
+
+def cpu_baseline():
+    nz_sample, steps = 128, 2
+    mlups, kind, dt = cpu_sample(nz_sample, steps)
+    return {"value": round(mlups, 3), "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{steps} steps of step_cpu<D3Q19,float,TRT> on a 256x256x{nz_sample} periodic slab "
+                      f"({dt:.1f} s); serial, as the reference is", "host_threads": os.cpu_count()}
+
+
+def run_reference(args):
+    # calibrate: one sample step, then size the per-step slab so the run stays within ~3 min
+    rate, kind, _ = cpu_sample(4, 1)
+    budget_s = 150.0
+    total = max(1, args.steps + args.warmup)
+    nz_s = int(max(1, min(64, budget_s * rate * 1e6 / total / (NX * NY))))
+    O, lib, kind = _reference_lib()
+    import numpy as np
+
+    n = NX * NY * nz_s
+    rng = np.random.default_rng(SEED)
+    u = 0.05 * rng.standard_normal((3, n))
+    f = O.init_equilibrium("D3Q19", np.ones(n), u, NX, NY, nz_s, np.float32)
+    for _ in range(args.warmup):
+        f = O.step(f, "D3Q19", "TRT", NX, NY, nz_s, 1 / TAU, steps=1, lib=lib)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        f = O.step(f, "D3Q19", "TRT", NX, NY, nz_s, 1 / TAU, steps=1, lib=lib)
+    dt = time.perf_counter() - t
+    value = n * args.steps / dt / 1e6
+    sample = (f"each step: step_cpu<D3Q19,float,TRT> on a 256x256x{nz_s} periodic slab of the "
+              f"256^3 workload (serial reference CPU path, 1 thread of {os.cpu_count()})")
+    return {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_dict(), "impl": "reference",
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": 1, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        line = run_engine(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,298 @@
+/*
+ * lbcube_b200.h -- C ABI of the B200 lattice Boltzmann engine.
+ *
+ * Drop-in boundary for LB-Cube's CUDA backend (include/lattice_cuda.cuh and
+ * src/lattice_cuda.cu, the lbm::cuda static library of CMakeLists.txt:39-75).
+ * Every symbol takes plain device pointers and element counts; no CUDA or
+ * C++ types cross the boundary. Populations are unpadded [Q, Z, Y, X] arrays
+ * with X fastest (include/lattice_memory.hpp:55-102), owned by the caller.
+ * The launchers never allocate, copy or free, and never synchronise.
+ *
+ * Return values are cudaError_t codes (0 = cudaSuccess). The reference's
+ * validation order is kept (src/lattice_cuda.cu:488-519):
+ *   1. a null pointer                     -> 17 cudaErrorInvalidDevicePointer
+ *   2. a zero block dimension             ->  9 cudaErrorInvalidConfiguration
+ *   3. (2D lattices: z and block.z := 1)
+ *   4. a zero extent                      ->  1 cudaErrorInvalidValue
+ *   5. otherwise the launch status (cudaGetLastError after the launch).
+ * Two checks are added, both returning 1 cudaErrorInvalidValue: a read
+ * buffer that overlaps a write buffer (the reference would race), and a
+ * domain with more than 2^31 - 1 cells (the kernels index a population
+ * plane with 32-bit offsets). The block arguments are validated as above but
+ * otherwise ignored: the kernels choose their own tiling.
+ *
+ * Launchers without a `stream` argument run on the legacy default stream,
+ * like the reference. The *_async extensions take a cudaStream_t passed as
+ * void* and cover the same kernels plus the engine's additions.
+ *
+ * Enum codes used by the extensions:
+ *   lattice   LBM_D2Q9 0, LBM_D3Q19 1, LBM_D3Q27 2, LBM_D2Q5 3, LBM_D3Q7 4
+ *   precision LBM_FLOAT 0, LBM_DOUBLE 1
+ *   collision LBM_BGK 0, LBM_TRT 1, LBM_MRT 2, LBM_RLBM 3
+ */
+#ifndef LBCUBE_B200_H
+#define LBCUBE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { LBM_D2Q9 = 0, LBM_D3Q19 = 1, LBM_D3Q27 = 2, LBM_D2Q5 = 3, LBM_D3Q7 = 4 };
+enum { LBM_FLOAT = 0, LBM_DOUBLE = 1 };
+enum { LBM_BGK = 0, LBM_TRT = 1, LBM_MRT = 2, LBM_RLBM = 3 };
+
+/* ---------------------------------------------------------------------------
+ * Fused pull collide-stream step, one symbol per instantiation. Each replaces
+ *   template <L, Real, CT> cudaError_t lbm::launch_step_gpu(
+ *       const Real* current, Real* next, size_t x, size_t y, size_t z,
+ *       Real omega, dim3 block = {16, 8, 1})
+ * declared at include/lattice_cuda.cuh:179-190, defined at
+ * src/lattice_cuda.cu:476-520 and instantiated at :808-858. The
+ * LatticeMemory overload (cuh:310-319, cu:680-698) forwards here with the
+ * memory object's extents.
+ * omega is the BGK relaxation frequency, the TRT even frequency (odd one from
+ * Lambda = 1/4, lattice_physics.hpp:336-344), the MRT shear rate s_nu, or the
+ * RLBM frequency.
+ * ------------------------------------------------------------------------- */
+/* lbm::launch_step_gpu<D2Q9, float, CollisionType::BGK> */
+int lbm_launch_step_gpu_d2q9_float_bgk(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D2Q9, float, CollisionType::TRT> */
+int lbm_launch_step_gpu_d2q9_float_trt(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D2Q9, float, CollisionType::MRT> */
+int lbm_launch_step_gpu_d2q9_float_mrt(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D2Q9, float, CollisionType::RLBM> */
+int lbm_launch_step_gpu_d2q9_float_rlbm(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D2Q9, double, CollisionType::BGK> */
+int lbm_launch_step_gpu_d2q9_double_bgk(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D2Q9, double, CollisionType::TRT> */
+int lbm_launch_step_gpu_d2q9_double_trt(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D2Q9, double, CollisionType::MRT> */
+int lbm_launch_step_gpu_d2q9_double_mrt(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D2Q9, double, CollisionType::RLBM> */
+int lbm_launch_step_gpu_d2q9_double_rlbm(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q19, float, CollisionType::BGK> */
+int lbm_launch_step_gpu_d3q19_float_bgk(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q19, float, CollisionType::TRT> */
+int lbm_launch_step_gpu_d3q19_float_trt(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q19, float, CollisionType::MRT> */
+int lbm_launch_step_gpu_d3q19_float_mrt(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q19, float, CollisionType::RLBM> */
+int lbm_launch_step_gpu_d3q19_float_rlbm(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q19, double, CollisionType::BGK> */
+int lbm_launch_step_gpu_d3q19_double_bgk(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q19, double, CollisionType::TRT> */
+int lbm_launch_step_gpu_d3q19_double_trt(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q19, double, CollisionType::MRT> */
+int lbm_launch_step_gpu_d3q19_double_mrt(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q19, double, CollisionType::RLBM> */
+int lbm_launch_step_gpu_d3q19_double_rlbm(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q27, float, CollisionType::BGK> */
+int lbm_launch_step_gpu_d3q27_float_bgk(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q27, float, CollisionType::TRT> */
+int lbm_launch_step_gpu_d3q27_float_trt(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q27, float, CollisionType::MRT> */
+int lbm_launch_step_gpu_d3q27_float_mrt(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q27, float, CollisionType::RLBM> */
+int lbm_launch_step_gpu_d3q27_float_rlbm(const float* current_populations, float* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q27, double, CollisionType::BGK> */
+int lbm_launch_step_gpu_d3q27_double_bgk(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q27, double, CollisionType::TRT> */
+int lbm_launch_step_gpu_d3q27_double_trt(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q27, double, CollisionType::MRT> */
+int lbm_launch_step_gpu_d3q27_double_mrt(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_step_gpu<D3Q27, double, CollisionType::RLBM> */
+int lbm_launch_step_gpu_d3q27_double_rlbm(const double* current_populations, double* next_populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+
+/* ---------------------------------------------------------------------------
+ * Passive-scalar advection-diffusion step. Each replaces
+ *   template <FL, SL, Real> cudaError_t lbm::launch_scalar_step_gpu(
+ *       const Real* current_scalar, Real* next_scalar, const Real* current_fluid,
+ *       size_t x, size_t y, size_t z, Real omega_c, Real source_term = 0,
+ *       dim3 block = {16, 8, 1})
+ * (include/lattice_cuda.cuh:209-222, src/lattice_cuda.cu:539-589, instantiated
+ * at :925-991). The fluid velocity is read at the destination cell.
+ * ------------------------------------------------------------------------- */
+/* lbm::launch_scalar_step_gpu<D2Q9, D2Q5, float> */
+int lbm_launch_scalar_step_gpu_d2q9_d2q5_float(const float* current_scalar, float* next_scalar,
+    const float* current_fluid, size_t x_extent, size_t y_extent, size_t z_extent,
+    float omega_c, float source_term, unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_scalar_step_gpu<D2Q9, D2Q5, double> */
+int lbm_launch_scalar_step_gpu_d2q9_d2q5_double(const double* current_scalar, double* next_scalar,
+    const double* current_fluid, size_t x_extent, size_t y_extent, size_t z_extent,
+    double omega_c, double source_term, unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_scalar_step_gpu<D3Q19, D3Q7, float> */
+int lbm_launch_scalar_step_gpu_d3q19_d3q7_float(const float* current_scalar, float* next_scalar,
+    const float* current_fluid, size_t x_extent, size_t y_extent, size_t z_extent,
+    float omega_c, float source_term, unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_scalar_step_gpu<D3Q19, D3Q7, double> */
+int lbm_launch_scalar_step_gpu_d3q19_d3q7_double(const double* current_scalar, double* next_scalar,
+    const double* current_fluid, size_t x_extent, size_t y_extent, size_t z_extent,
+    double omega_c, double source_term, unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_scalar_step_gpu<D3Q27, D3Q7, float> */
+int lbm_launch_scalar_step_gpu_d3q27_d3q7_float(const float* current_scalar, float* next_scalar,
+    const float* current_fluid, size_t x_extent, size_t y_extent, size_t z_extent,
+    float omega_c, float source_term, unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_scalar_step_gpu<D3Q27, D3Q7, double> */
+int lbm_launch_scalar_step_gpu_d3q27_d3q7_double(const double* current_scalar, double* next_scalar,
+    const double* current_fluid, size_t x_extent, size_t y_extent, size_t z_extent,
+    double omega_c, double source_term, unsigned block_x, unsigned block_y, unsigned block_z);
+
+/* ---------------------------------------------------------------------------
+ * Fused A + B -> C advection-diffusion-reaction step. Each replaces
+ *   template <FL, SL, Real> cudaError_t lbm::launch_reaction_AB_gpu(
+ *       const Real* current_a, Real* next_a, const Real* current_b,
+ *       Real* next_b, const Real* current_fluid, size_t x, size_t y, size_t z,
+ *       Real omega_c, Real k_react, dim3 block = {16, 8, 1})
+ * (include/lattice_cuda.cuh:276-291, src/lattice_cuda.cu:610-666,
+ * instantiated at :1012-1029).
+ * ------------------------------------------------------------------------- */
+/* lbm::launch_reaction_AB_gpu<D2Q9, D2Q5, float> */
+int lbm_launch_reaction_ab_gpu_d2q9_d2q5_float(const float* current_a, float* next_a,
+    const float* current_b, float* next_b, const float* current_fluid,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega_c, float k_react,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_reaction_AB_gpu<D2Q9, D2Q5, double> */
+int lbm_launch_reaction_ab_gpu_d2q9_d2q5_double(const double* current_a, double* next_a,
+    const double* current_b, double* next_b, const double* current_fluid,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega_c, double k_react,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_reaction_AB_gpu<D3Q19, D3Q7, float> */
+int lbm_launch_reaction_ab_gpu_d3q19_d3q7_float(const float* current_a, float* next_a,
+    const float* current_b, float* next_b, const float* current_fluid,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega_c, float k_react,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_reaction_AB_gpu<D3Q19, D3Q7, double> */
+int lbm_launch_reaction_ab_gpu_d3q19_d3q7_double(const double* current_a, double* next_a,
+    const double* current_b, double* next_b, const double* current_fluid,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega_c, double k_react,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_reaction_AB_gpu<D3Q27, D3Q7, float> */
+int lbm_launch_reaction_ab_gpu_d3q27_d3q7_float(const float* current_a, float* next_a,
+    const float* current_b, float* next_b, const float* current_fluid,
+    size_t x_extent, size_t y_extent, size_t z_extent, float omega_c, float k_react,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+/* lbm::launch_reaction_AB_gpu<D3Q27, D3Q7, double> */
+int lbm_launch_reaction_ab_gpu_d3q27_d3q7_double(const double* current_a, double* next_a,
+    const double* current_b, double* next_b, const double* current_fluid,
+    size_t x_extent, size_t y_extent, size_t z_extent, double omega_c, double k_react,
+    unsigned block_x, unsigned block_y, unsigned block_z);
+
+/* ---------------------------------------------------------------------------
+ * Stream-ordered extensions (no reference counterpart unless stated).
+ * `precision` selects float or double for every population pointer.
+ * ------------------------------------------------------------------------- */
+
+/* Any of the 24 step instantiations above, on `stream` (same validation). */
+int lbm_step_async(int lattice, int precision, int collision, const void* current_populations,
+    void* next_populations, size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+    void* stream);
+
+/* Any of the 6 scalar-step instantiations above; `fluid_lattice` picks the pair. */
+int lbm_scalar_step_async(int fluid_lattice, int precision, const void* current_scalar,
+    void* next_scalar, const void* current_fluid, size_t x_extent, size_t y_extent,
+    size_t z_extent, double omega_c, double source_term, void* stream);
+
+/* Any of the 6 reaction instantiations above. */
+int lbm_reaction_ab_async(int fluid_lattice, int precision, const void* current_a, void* next_a,
+    const void* current_b, void* next_b, const void* current_fluid, size_t x_extent,
+    size_t y_extent, size_t z_extent, double omega_c, double k_react, void* stream);
+
+/* One launch doing what the reference's reaction driver does with two
+ * (src/simulate_reaction.cpp:518-543): the fluid step, then the reaction step
+ * advected by the post-step fluid. The velocity is recomputed from the
+ * post-collision populations held in registers, which are the values the
+ * separate reaction launch would read back, so the result is the same and the
+ * fluid is not re-read. When `stats_partials` is non-null the launch also
+ * accumulates the reactive statistics of the post-step scalar fields into it
+ * (FP64 per-block partial sums; size from lbm_stats_partials_bytes);
+ * lbm_reactive_stats_finalize_async then turns them into the 8 diagnostics. */
+int lbm_fluid_reaction_ab_async(int fluid_lattice, int precision, int collision,
+    const void* current_fluid, void* next_fluid, const void* current_a, void* next_a,
+    const void* current_b, void* next_b, size_t x_extent, size_t y_extent, size_t z_extent,
+    double omega, double omega_c, double k_react, double* stats_partials,
+    size_t stats_partials_bytes, void* stream);
+
+/* Bytes of FP64 partial sums the statistics kernels write for this domain. */
+size_t lbm_stats_partials_bytes(int fluid_lattice, size_t x_extent, size_t y_extent,
+    size_t z_extent);
+
+/* Reactive-mixing statistics of two scalar fields, replacing the host loop of
+ * lbm::compute_reactive_stats (include/lattice_io.hpp:256-338). Sums of C_A,
+ * C_B, C_A^2, C_B^2 and C_A C_B are accumulated in FP64 with a fixed-order
+ * two-pass reduction (deterministic run to run). `partials` is caller-owned
+ * scratch of lbm_stats_partials_bytes bytes. `diagnostics` (device, 8
+ * doubles) receives mean_A, mean_B, var_A, var_B, covariance,
+ * segregation_intensity, true_reaction_rate, mixed_reaction_rate
+ * (ReactiveDiagnostics, include/lattice_io.hpp:148-166). */
+int lbm_reactive_stats_async(int scalar_lattice, int precision, const void* current_a,
+    const void* current_b, size_t x_extent, size_t y_extent, size_t z_extent, double k_react,
+    double* partials, size_t partials_bytes, double* diagnostics, void* stream);
+
+/* Second pass of the statistics over partials written by a fused launch. */
+int lbm_reactive_stats_finalize_async(int fluid_lattice, size_t x_extent, size_t y_extent,
+    size_t z_extent, double k_react, const double* partials, size_t partials_bytes,
+    double* diagnostics, void* stream);
+
+/* Equilibrium initialisation from macroscopic fields (device, `precision`):
+ * rho[N] (density, or concentration for D2Q5/D3Q7) and u[D*N] component-major.
+ * Per cell it evaluates lbm::compute_equilibrium (lattice_physics.hpp:267-290)
+ * or lbm::compute_scalar_equilibrium (:643-659), the initialisation every
+ * reference driver and test performs on the host. */
+int lbm_init_equilibrium_async(int lattice, int precision, const void* rho, const void* u,
+    void* populations, size_t x_extent, size_t y_extent, size_t z_extent, void* stream);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+#endif /* LBCUBE_B200_H */

@@ -1,0 +1,99 @@
+"""Builds the engine's shared library, lb-cube_b200/liblbcube_b200.so, in place.
+
+Every CUDA translation unit under csrc/ is compiled for sm_100a only
+(``-gencode arch=compute_100a,code=sm_100a``) in parallel, then linked into one
+library that exports the C ABI declared in include/lbcube_b200.h. Collision
+code is built with ``--fmad=false`` so that multiply-adds are rounded exactly
+as LB-Cube's CPU path rounds them (no contraction into FMA); that is what makes
+the engine's steps bit-identical to the reference.
+
+Usage: python lb-cube_b200/build.py [--force] [--verbose]
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "liblbcube_b200.so")
+
+NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off"]
+# Per-unit extra flags: exact (non-contracted) arithmetic for everything that
+# must reproduce the reference's rounding.
+UNITS = {
+    "fluid_step.cu": ["--fmad=false"],
+    "adr.cu": ["--fmad=false"],
+    "stats.cu": ["--fmad=false"],
+    "init.cu": ["--fmad=false"],
+}
+
+
+def _sources():
+    return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+
+
+def _headers():
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    hs += [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith((".h", ".cuh"))]
+    return hs
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _compile(src, verbose):
+    obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+    cmd = [NVCC, *COMMON, *ARCH, *UNITS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+    return obj, (res.stdout + res.stderr)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile (if stale) and link the engine library; returns its path."""
+    os.makedirs(BUILD, exist_ok=True)
+    headers = _headers()
+    todo, objs = [], []
+    for src in _sources():
+        obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(obj)
+        if force or _stale(obj, [os.path.join(CSRC, src), *headers, __file__]):
+            todo.append(src)
+    if todo:
+        with cf.ThreadPoolExecutor(max_workers=min(len(todo), os.cpu_count() or 4)) as ex:
+            for obj, log in ex.map(lambda s: _compile(s, verbose), todo):
+                if verbose and log.strip():
+                    print(log)
+    if force or todo or _stale(LIB, objs):
+        tmp = LIB + ".tmp"
+        cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+        os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, verbose=a.verbose))
+    sys.exit(0)

@@ -1,0 +1,371 @@
+// Advection-diffusion(-reaction) kernels for D2Q5 / D3Q7 scalars.
+//
+// scalar_step_kernel    replaces kernel_scalar_step  (src/lattice_cuda.cu:234-327)
+// reaction_ab_kernel    replaces kernel_reaction_AB  (src/lattice_cuda.cu:349-457)
+// fluid_reaction_kernel fuses launch_step_gpu + launch_reaction_AB_gpu the way
+//                       the reaction driver sequences them
+//                       (src/simulate_reaction.cpp:518-543), optionally with
+//                       the reactive-statistics partial sums of the new fields.
+#include "collide.cuh"
+#include "common.cuh"
+#include "reduce.cuh"
+#include "../../include/lbcube_b200.h"
+
+namespace lbcube {
+
+struct Neighbours {
+  int xm, xp, ym, yp, zm, zp;
+};
+
+__device__ __forceinline__ Neighbours neighbours(const Grid& g, int x, int y, int z) {
+  Neighbours n;
+  n.xm = x == 0 ? g.nx - 1 : x - 1;
+  n.xp = x == g.nx - 1 ? 0 : x + 1;
+  n.ym = y == 0 ? g.ny - 1 : y - 1;
+  n.yp = y == g.ny - 1 ? 0 : y + 1;
+  n.zm = z == 0 ? g.nz - 1 : z - 1;
+  n.zp = z == g.nz - 1 ? 0 : z + 1;
+  return n;
+}
+
+// Pull-gather of all Q populations of lattice L at (x, y, z) (lattice_core.hpp:70-78).
+template <class L, class Real>
+__device__ __forceinline__ void gather(const Real* __restrict__ cur, const Grid& g,
+                                       const Neighbours& n, int x, int y, int z,
+                                       Real (&f)[L::Q]) {
+  const size_t plane = (size_t)g.plane;
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    const int sx = cx == 0 ? x : (cx > 0 ? n.xm : n.xp);
+    const int sy = cy == 0 ? y : (cy > 0 ? n.ym : n.yp);
+    const int sz = cz == 0 ? z : (cz > 0 ? n.zm : n.zp);
+    f[i] = __ldg(cur + plane * i + ((sz * g.ny + sy) * g.nx + sx));
+  });
+}
+
+// All Q populations of the cell itself.
+template <class L, class Real>
+__device__ __forceinline__ void load_cell(const Real* __restrict__ cur, const Grid& g, int cell,
+                                          Real (&f)[L::Q]) {
+  const size_t plane = (size_t)g.plane;
+  static_for<L::Q>([&](auto I) { f[LB_I(I)] = __ldg(cur + plane * LB_I(I) + cell); });
+}
+
+template <class L, class Real>
+__device__ __forceinline__ void store_cell(Real* __restrict__ out, const Grid& g, int cell,
+                                           const Real (&f)[L::Q]) {
+  const size_t plane = (size_t)g.plane;
+  static_for<L::Q>([&](auto I) { out[plane * LB_I(I) + cell] = f[LB_I(I)]; });
+}
+
+// Fluid velocity at a cell from its populations (compute_macro_state).
+template <class FL, class Real>
+__device__ __forceinline__ void fluid_velocity(const Real (&f)[FL::Q], Real (&u)[FL::D]) {
+  Real rho;
+  macro_state<FL>(f, rho, u);
+}
+
+template <class FL, class Real>
+__global__ void __launch_bounds__(kThreads)
+    scalar_step_kernel(const Real* __restrict__ cur_s, Real* __restrict__ nxt_s,
+                       const Real* __restrict__ cur_f, Grid g, Real omega_c, Real source) {
+  using SL = typename ScalarOf<FL>::type;
+  int x, y, z;
+  if (!cell_of(g, x, y, z)) return;
+  const int cell = (z * g.ny + y) * g.nx + x;
+  Real f[FL::Q], u[FL::D], s[SL::Q];
+  load_cell<FL>(cur_f, g, cell, f);
+  fluid_velocity<FL>(f, u);
+  gather<SL>(cur_s, g, neighbours(g, x, y, z), x, y, z, s);
+  collide_scalar<SL>(s, u, omega_c, source);
+  store_cell<SL>(nxt_s, g, cell, s);
+}
+
+// Two species pulled, one exact A+B->C source applied to both
+// (lattice_core.hpp:403-411).
+template <class SL, class Real>
+__device__ __forceinline__ void react_pair(Real (&a)[SL::Q], Real (&b)[SL::Q],
+                                           const Real (&u)[SL::D], Real omega_c, Real k) {
+  const Real ca = concentration<SL>(a);
+  const Real cb = concentration<SL>(b);
+  const Real src = reaction_source<Real>(ca, cb, k);
+  collide_scalar<SL>(a, u, omega_c, src);
+  collide_scalar<SL>(b, u, omega_c, src);
+}
+
+template <class FL, class Real>
+__global__ void __launch_bounds__(kThreads)
+    reaction_ab_kernel(const Real* __restrict__ cur_a, Real* __restrict__ nxt_a,
+                       const Real* __restrict__ cur_b, Real* __restrict__ nxt_b,
+                       const Real* __restrict__ cur_f, Grid g, Real omega_c, Real k) {
+  using SL = typename ScalarOf<FL>::type;
+  int x, y, z;
+  if (!cell_of(g, x, y, z)) return;
+  const int cell = (z * g.ny + y) * g.nx + x;
+  Real f[FL::Q], u[FL::D], a[SL::Q], b[SL::Q];
+  load_cell<FL>(cur_f, g, cell, f);
+  fluid_velocity<FL>(f, u);
+  const Neighbours n = neighbours(g, x, y, z);
+  gather<SL>(cur_a, g, n, x, y, z, a);
+  gather<SL>(cur_b, g, n, x, y, z, b);
+  react_pair<SL>(a, b, u, omega_c, k);
+  store_cell<SL>(nxt_a, g, cell, a);
+  store_cell<SL>(nxt_b, g, cell, b);
+}
+
+// Fluid step + reaction step in one pass. The advecting velocity is
+// recomputed from the post-collision fluid populations: they are bit for bit
+// the values the reference's separate reaction launch reads back from the new
+// fluid buffer at this cell, so the result equals the two-launch sequence.
+template <class FL, class Real, int CT, bool STATS>
+__global__ void __launch_bounds__(kThreads)
+    fluid_reaction_kernel(const Real* __restrict__ cur_f, Real* __restrict__ nxt_f,
+                          const Real* __restrict__ cur_a, Real* __restrict__ nxt_a,
+                          const Real* __restrict__ cur_b, Real* __restrict__ nxt_b, Grid g,
+                          Real omega, Real omega_minus, Real omega_c, Real k,
+                          double* __restrict__ partials) {
+  using SL = typename ScalarOf<FL>::type;
+  int x, y, z;
+  const bool active = cell_of(g, x, y, z);
+  double sums[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (active) {
+    const int cell = (z * g.ny + y) * g.nx + x;
+    const Neighbours n = neighbours(g, x, y, z);
+    Real f[FL::Q], u[FL::D];
+    gather<FL>(cur_f, g, n, x, y, z, f);
+    collide<FL, Real, CT>(f, omega, omega_minus);
+    store_cell<FL>(nxt_f, g, cell, f);
+    fluid_velocity<FL>(f, u);
+    Real a[SL::Q], b[SL::Q];
+    gather<SL>(cur_a, g, n, x, y, z, a);
+    gather<SL>(cur_b, g, n, x, y, z, b);
+    react_pair<SL>(a, b, u, omega_c, k);
+    store_cell<SL>(nxt_a, g, cell, a);
+    store_cell<SL>(nxt_b, g, cell, b);
+    if constexpr (STATS) {
+      // concentration_at of the stored fields (lattice_io.hpp:125-133)
+      const double ca = (double)concentration<SL>(a);
+      const double cb = (double)concentration<SL>(b);
+      sums[0] = ca;
+      sums[1] = cb;
+      sums[2] = ca * ca;
+      sums[3] = cb * cb;
+      sums[4] = ca * cb;
+    }
+  }
+  if constexpr (STATS) block_sum_to<kStatSums>(sums, partials + block_linear() * kStatSums);
+}
+
+template <class FL, class Real>
+cudaError_t launch_scalar(const Real* cur_s, Real* nxt_s, const Real* cur_f, size_t nx, size_t ny,
+                          size_t nz, Real omega_c, Real source, unsigned bx, unsigned by,
+                          unsigned bz, cudaStream_t stream) {
+  using SL = typename ScalarOf<FL>::type;
+  Grid g;
+  cudaError_t err = validate_domain(cur_s == nullptr || nxt_s == nullptr || cur_f == nullptr, bx,
+                                    by, bz, FL::D, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  const size_t sb = (size_t)SL::Q * g.plane * sizeof(Real);
+  const size_t fb = (size_t)FL::Q * g.plane * sizeof(Real);
+  const Span reads[2] = {{cur_s, sb}, {cur_f, fb}};
+  const Span writes[1] = {{nxt_s, sb}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  scalar_step_kernel<FL, Real><<<grid_dims(g), kThreads, 0, stream>>>(cur_s, nxt_s, cur_f, g,
+                                                                       omega_c, source);
+  return cudaGetLastError();
+}
+
+template <class FL, class Real>
+cudaError_t launch_reaction(const Real* cur_a, Real* nxt_a, const Real* cur_b, Real* nxt_b,
+                            const Real* cur_f, size_t nx, size_t ny, size_t nz, Real omega_c,
+                            Real k, unsigned bx, unsigned by, unsigned bz, cudaStream_t stream) {
+  using SL = typename ScalarOf<FL>::type;
+  Grid g;
+  cudaError_t err =
+      validate_domain(cur_a == nullptr || nxt_a == nullptr || cur_b == nullptr ||
+                          nxt_b == nullptr || cur_f == nullptr,
+                      bx, by, bz, FL::D, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  const size_t sb = (size_t)SL::Q * g.plane * sizeof(Real);
+  const size_t fb = (size_t)FL::Q * g.plane * sizeof(Real);
+  const Span reads[3] = {{cur_a, sb}, {cur_b, sb}, {cur_f, fb}};
+  const Span writes[2] = {{nxt_a, sb}, {nxt_b, sb}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  reaction_ab_kernel<FL, Real><<<grid_dims(g), kThreads, 0, stream>>>(cur_a, nxt_a, cur_b, nxt_b,
+                                                                       cur_f, g, omega_c, k);
+  return cudaGetLastError();
+}
+
+template <class FL, class Real, int CT>
+cudaError_t launch_fluid_reaction(const Real* cur_f, Real* nxt_f, const Real* cur_a, Real* nxt_a,
+                                  const Real* cur_b, Real* nxt_b, size_t nx, size_t ny,
+                                  size_t nz, Real omega, Real omega_c, Real k, double* partials,
+                                  size_t partials_bytes, cudaStream_t stream) {
+  using SL = typename ScalarOf<FL>::type;
+  Grid g;
+  cudaError_t err = validate_domain(cur_f == nullptr || nxt_f == nullptr || cur_a == nullptr ||
+                                        nxt_a == nullptr || cur_b == nullptr || nxt_b == nullptr,
+                                    1, 1, 1, FL::D, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  const size_t sb = (size_t)SL::Q * g.plane * sizeof(Real);
+  const size_t fb = (size_t)FL::Q * g.plane * sizeof(Real);
+  const Span reads[3] = {{cur_f, fb}, {cur_a, sb}, {cur_b, sb}};
+  if (partials != nullptr) {
+    const size_t need = (size_t)g.blocks() * kStatSums * sizeof(double);
+    if (partials_bytes < need) return cudaErrorInvalidValue;
+    const Span writes[4] = {{nxt_f, fb}, {nxt_a, sb}, {nxt_b, sb}, {partials, need}};
+    if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  } else {
+    const Span writes[3] = {{nxt_f, fb}, {nxt_a, sb}, {nxt_b, sb}};
+    if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  }
+  const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
+  if (partials != nullptr) {
+    fluid_reaction_kernel<FL, Real, CT, true><<<grid_dims(g), kThreads, 0, stream>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, partials);
+  } else {
+    fluid_reaction_kernel<FL, Real, CT, false><<<grid_dims(g), kThreads, 0, stream>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, nullptr);
+  }
+  return cudaGetLastError();
+}
+
+template <class FL, class Real>
+cudaError_t fused_by_collision(int collision, const void* cf, void* nf, const void* ca, void* na,
+                               const void* cb, void* nb, size_t nx, size_t ny, size_t nz,
+                               double omega, double omega_c, double k, double* partials,
+                               size_t pbytes, cudaStream_t s) {
+  const Real* f0 = static_cast<const Real*>(cf);
+  Real* f1 = static_cast<Real*>(nf);
+  const Real* a0 = static_cast<const Real*>(ca);
+  Real* a1 = static_cast<Real*>(na);
+  const Real* b0 = static_cast<const Real*>(cb);
+  Real* b1 = static_cast<Real*>(nb);
+  switch (collision) {
+    case kBGK:
+      return launch_fluid_reaction<FL, Real, kBGK>(f0, f1, a0, a1, b0, b1, nx, ny, nz, Real(omega),
+                                                   Real(omega_c), Real(k), partials, pbytes, s);
+    case kTRT:
+      return launch_fluid_reaction<FL, Real, kTRT>(f0, f1, a0, a1, b0, b1, nx, ny, nz, Real(omega),
+                                                   Real(omega_c), Real(k), partials, pbytes, s);
+    case kMRT:
+      return launch_fluid_reaction<FL, Real, kMRT>(f0, f1, a0, a1, b0, b1, nx, ny, nz, Real(omega),
+                                                   Real(omega_c), Real(k), partials, pbytes, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace lbcube
+
+using namespace lbcube;
+
+#define LBCUBE_SCALAR_SYMBOL(fl, sl, FL, real)                                                   \
+  extern "C" int lbm_launch_scalar_step_gpu_##fl##_##sl##_##real(                              \
+      const real* current_scalar, real* next_scalar, const real* current_fluid,                \
+      size_t x_extent, size_t y_extent, size_t z_extent, real omega_c, real source_term,       \
+      unsigned block_x, unsigned block_y, unsigned block_z) {                                  \
+    return (int)launch_scalar<FL, real>(current_scalar, next_scalar, current_fluid, x_extent,  \
+                                        y_extent, z_extent, omega_c, source_term, block_x,     \
+                                        block_y, block_z, (cudaStream_t)0);                    \
+  }
+
+#define LBCUBE_REACTION_SYMBOL(fl, sl, FL, real)                                                 \
+  extern "C" int lbm_launch_reaction_ab_gpu_##fl##_##sl##_##real(                              \
+      const real* current_a, real* next_a, const real* current_b, real* next_b,                \
+      const real* current_fluid, size_t x_extent, size_t y_extent, size_t z_extent,            \
+      real omega_c, real k_react, unsigned block_x, unsigned block_y, unsigned block_z) {      \
+    return (int)launch_reaction<FL, real>(current_a, next_a, current_b, next_b, current_fluid, \
+                                          x_extent, y_extent, z_extent, omega_c, k_react,      \
+                                          block_x, block_y, block_z, (cudaStream_t)0);         \
+  }
+
+LBCUBE_SCALAR_SYMBOL(d2q9, d2q5, D2Q9, float)
+LBCUBE_SCALAR_SYMBOL(d2q9, d2q5, D2Q9, double)
+LBCUBE_SCALAR_SYMBOL(d3q19, d3q7, D3Q19, float)
+LBCUBE_SCALAR_SYMBOL(d3q19, d3q7, D3Q19, double)
+LBCUBE_SCALAR_SYMBOL(d3q27, d3q7, D3Q27, float)
+LBCUBE_SCALAR_SYMBOL(d3q27, d3q7, D3Q27, double)
+
+LBCUBE_REACTION_SYMBOL(d2q9, d2q5, D2Q9, float)
+LBCUBE_REACTION_SYMBOL(d2q9, d2q5, D2Q9, double)
+LBCUBE_REACTION_SYMBOL(d3q19, d3q7, D3Q19, float)
+LBCUBE_REACTION_SYMBOL(d3q19, d3q7, D3Q19, double)
+LBCUBE_REACTION_SYMBOL(d3q27, d3q7, D3Q27, float)
+LBCUBE_REACTION_SYMBOL(d3q27, d3q7, D3Q27, double)
+
+extern "C" int lbm_scalar_step_async(int fluid_lattice, int precision, const void* current_scalar,
+                                     void* next_scalar, const void* current_fluid,
+                                     size_t x_extent, size_t y_extent, size_t z_extent,
+                                     double omega_c, double source_term, void* stream) {
+  const cudaStream_t s = as_stream(stream);
+#define LBCUBE_CASE(FL, real)                                                                     \
+  return (int)launch_scalar<FL, real>(static_cast<const real*>(current_scalar),                  \
+                                      static_cast<real*>(next_scalar),                           \
+                                      static_cast<const real*>(current_fluid), x_extent,         \
+                                      y_extent, z_extent, real(omega_c), real(source_term), 1, 1, \
+                                      1, s)
+  if (precision == LBM_FLOAT) {
+    if (fluid_lattice == LBM_D2Q9) LBCUBE_CASE(D2Q9, float);
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_CASE(D3Q19, float);
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_CASE(D3Q27, float);
+  } else if (precision == LBM_DOUBLE) {
+    if (fluid_lattice == LBM_D2Q9) LBCUBE_CASE(D2Q9, double);
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_CASE(D3Q19, double);
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_CASE(D3Q27, double);
+  }
+#undef LBCUBE_CASE
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int lbm_reaction_ab_async(int fluid_lattice, int precision, const void* current_a,
+                                     void* next_a, const void* current_b, void* next_b,
+                                     const void* current_fluid, size_t x_extent, size_t y_extent,
+                                     size_t z_extent, double omega_c, double k_react,
+                                     void* stream) {
+  const cudaStream_t s = as_stream(stream);
+#define LBCUBE_CASE(FL, real)                                                                 \
+  return (int)launch_reaction<FL, real>(                                                     \
+      static_cast<const real*>(current_a), static_cast<real*>(next_a),                       \
+      static_cast<const real*>(current_b), static_cast<real*>(next_b),                       \
+      static_cast<const real*>(current_fluid), x_extent, y_extent, z_extent, real(omega_c),  \
+      real(k_react), 1, 1, 1, s)
+  if (precision == LBM_FLOAT) {
+    if (fluid_lattice == LBM_D2Q9) LBCUBE_CASE(D2Q9, float);
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_CASE(D3Q19, float);
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_CASE(D3Q27, float);
+  } else if (precision == LBM_DOUBLE) {
+    if (fluid_lattice == LBM_D2Q9) LBCUBE_CASE(D2Q9, double);
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_CASE(D3Q19, double);
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_CASE(D3Q27, double);
+  }
+#undef LBCUBE_CASE
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int lbm_fluid_reaction_ab_async(int fluid_lattice, int precision, int collision,
+                                           const void* current_fluid, void* next_fluid,
+                                           const void* current_a, void* next_a,
+                                           const void* current_b, void* next_b, size_t x_extent,
+                                           size_t y_extent, size_t z_extent, double omega,
+                                           double omega_c, double k_react,
+                                           double* stats_partials, size_t stats_partials_bytes,
+                                           void* stream) {
+  const cudaStream_t s = as_stream(stream);
+#define LBCUBE_CASE(FL, real)                                                                  \
+  return (int)fused_by_collision<FL, real>(collision, current_fluid, next_fluid, current_a,   \
+                                           next_a, current_b, next_b, x_extent, y_extent,     \
+                                           z_extent, omega, omega_c, k_react, stats_partials, \
+                                           stats_partials_bytes, s)
+  if (precision == LBM_FLOAT) {
+    if (fluid_lattice == LBM_D2Q9) LBCUBE_CASE(D2Q9, float);
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_CASE(D3Q19, float);
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_CASE(D3Q27, float);
+  } else if (precision == LBM_DOUBLE) {
+    if (fluid_lattice == LBM_D2Q9) LBCUBE_CASE(D2Q9, double);
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_CASE(D3Q19, double);
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_CASE(D3Q27, double);
+  }
+#undef LBCUBE_CASE
+  return (int)cudaErrorInvalidValue;
+}

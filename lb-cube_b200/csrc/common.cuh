@@ -1,0 +1,90 @@
+// Launch geometry and argument validation shared by every kernel family.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstddef>
+#include <cstdint>
+
+#include "lattices.cuh"
+
+namespace lbcube {
+
+// Threads per block along x. Each thread owns one cell of an x-row; a block
+// covers kThreads consecutive cells of one (y, z) row.
+constexpr int kThreads = 128;
+
+// Domain extents and the block decomposition: grid.x = xblocks * ny
+// (row-major over y, then x-block), grid.y = nz.
+struct Grid {
+  int nx, ny, nz;
+  int xblocks;
+  long long plane;  // cells per population plane, nx * ny * nz (< 2^31)
+
+  __host__ __device__ long long blocks() const { return (long long)xblocks * ny * nz; }
+};
+
+__device__ __forceinline__ bool cell_of(const Grid& g, int& x, int& y, int& z) {
+  const int row = blockIdx.x / g.xblocks;
+  const int xb = blockIdx.x - row * g.xblocks;
+  x = xb * kThreads + threadIdx.x;
+  y = row;
+  z = blockIdx.y;
+  return x < g.nx;
+}
+
+// Linear block index used to address per-block partial sums.
+__device__ __forceinline__ long long block_linear() {
+  return (long long)blockIdx.y * gridDim.x + blockIdx.x;
+}
+
+inline dim3 grid_dims(const Grid& g) { return dim3((unsigned)(g.xblocks * g.ny), (unsigned)g.nz, 1); }
+
+// Validation in the reference's order (src/lattice_cuda.cu:488-503), then the
+// engine's own limits. On success fills `g`.
+inline cudaError_t validate_domain(bool any_null, unsigned bx, unsigned by, unsigned bz, int dims,
+                                   size_t nx, size_t ny, size_t nz, Grid& g) {
+  if (any_null) return cudaErrorInvalidDevicePointer;
+  if (bx == 0 || by == 0 || bz == 0) return cudaErrorInvalidConfiguration;
+  if (dims == 2) nz = 1;
+  if (nx == 0 || ny == 0 || nz == 0) return cudaErrorInvalidValue;
+  if (nx > (size_t)INT_MAX || ny > (size_t)INT_MAX || nz > 65535) return cudaErrorInvalidValue;
+  const unsigned long long cells = (unsigned long long)nx * ny;
+  if (cells > (unsigned long long)INT_MAX || cells * nz > (unsigned long long)INT_MAX)
+    return cudaErrorInvalidValue;
+  g.nx = (int)nx;
+  g.ny = (int)ny;
+  g.nz = (int)nz;
+  g.xblocks = (int)((nx + kThreads - 1) / kThreads);
+  g.plane = (long long)(cells * nz);
+  if ((long long)g.xblocks * g.ny > (long long)INT_MAX) return cudaErrorInvalidValue;
+  return cudaSuccess;
+}
+
+struct Span {
+  const void* p;
+  size_t bytes;
+};
+
+inline bool overlaps(Span a, Span b) {
+  const uintptr_t a0 = (uintptr_t)a.p, a1 = a0 + a.bytes;
+  const uintptr_t b0 = (uintptr_t)b.p, b1 = b0 + b.bytes;
+  return a0 < b1 && b0 < a1;
+}
+
+// Every written buffer must be disjoint from every other buffer of the call.
+template <int NR, int NW>
+inline bool any_overlap(const Span (&reads)[NR], const Span (&writes)[NW]) {
+  for (int w = 0; w < NW; ++w) {
+    for (int r = 0; r < NR; ++r)
+      if (overlaps(writes[w], reads[r])) return true;
+    for (int v = w + 1; v < NW; ++v)
+      if (overlaps(writes[w], writes[v])) return true;
+  }
+  return false;
+}
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace lbcube

@@ -1,0 +1,131 @@
+// Fused pull-scheme collide-stream step for D2Q9 / D3Q19 / D3Q27 fluids.
+//
+// Replaces kernel_step and launch_step_gpu (src/lattice_cuda.cu:149-213,
+// :476-520). One thread owns one destination cell: it gathers the Q incoming
+// populations f_i(x - c_i) from the current buffer (periodic wrap by
+// compare-and-select on 32-bit coordinates instead of the reference's 64-bit
+// modulo), collides in registers and writes the Q results to the next buffer
+// at its own cell. A warp covers 32 consecutive x cells, so each of the Q
+// gathers and Q stores is one coalesced 128-byte row segment (shifted by at
+// most one element for c_x != 0, which the L1/L2 sector reuse absorbs).
+#include "collide.cuh"
+#include "common.cuh"
+#include "../../include/lbcube_b200.h"
+
+namespace lbcube {
+
+template <class L, class Real, int CT>
+__global__ void __launch_bounds__(kThreads)
+    fluid_step_kernel(const Real* __restrict__ cur, Real* __restrict__ nxt, Grid g, Real omega,
+                      Real omega_minus) {
+  int x, y, z;
+  if (!cell_of(g, x, y, z)) return;
+  const int xm = x == 0 ? g.nx - 1 : x - 1, xp = x == g.nx - 1 ? 0 : x + 1;
+  const int ym = y == 0 ? g.ny - 1 : y - 1, yp = y == g.ny - 1 ? 0 : y + 1;
+  const int zm = z == 0 ? g.nz - 1 : z - 1, zp = z == g.nz - 1 ? 0 : z + 1;
+  const size_t plane = (size_t)g.plane;
+
+  Real f[L::Q];
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    // pull: source = destination - c_i (lattice_core.hpp:70-78)
+    const int sx = cx == 0 ? x : (cx > 0 ? xm : xp);
+    const int sy = cy == 0 ? y : (cy > 0 ? ym : yp);
+    const int sz = cz == 0 ? z : (cz > 0 ? zm : zp);
+    f[i] = __ldg(cur + plane * i + ((sz * g.ny + sy) * g.nx + sx));
+  });
+
+  collide<L, Real, CT>(f, omega, omega_minus);
+
+  const int cell = (z * g.ny + y) * g.nx + x;
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    nxt[plane * i + cell] = f[i];
+  });
+}
+
+template <class L, class Real, int CT>
+cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, size_t nz,
+                              Real omega, unsigned bx, unsigned by, unsigned bz,
+                              cudaStream_t stream) {
+  Grid g;
+  cudaError_t err =
+      validate_domain(cur == nullptr || nxt == nullptr, bx, by, bz, L::D, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  const size_t bytes = (size_t)L::Q * (size_t)g.plane * sizeof(Real);
+  const Span reads[1] = {{cur, bytes}};
+  const Span writes[1] = {{nxt, bytes}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
+  fluid_step_kernel<L, Real, CT><<<grid_dims(g), kThreads, 0, stream>>>(cur, nxt, g, omega,
+                                                                         omega_minus);
+  return cudaGetLastError();
+}
+
+template <class Real, int CT>
+cudaError_t dispatch_lattice(int lattice, const void* cur, void* nxt, size_t nx, size_t ny,
+                             size_t nz, double omega, cudaStream_t s) {
+  const Real* c = static_cast<const Real*>(cur);
+  Real* n = static_cast<Real*>(nxt);
+  switch (lattice) {
+    case kD2Q9: return launch_fluid_step<D2Q9, Real, CT>(c, n, nx, ny, nz, Real(omega), 1, 1, 1, s);
+    case kD3Q19: return launch_fluid_step<D3Q19, Real, CT>(c, n, nx, ny, nz, Real(omega), 1, 1, 1, s);
+    case kD3Q27: return launch_fluid_step<D3Q27, Real, CT>(c, n, nx, ny, nz, Real(omega), 1, 1, 1, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <class Real>
+cudaError_t dispatch_collision(int lattice, int collision, const void* cur, void* nxt, size_t nx,
+                               size_t ny, size_t nz, double omega, cudaStream_t s) {
+  switch (collision) {
+    case kBGK: return dispatch_lattice<Real, kBGK>(lattice, cur, nxt, nx, ny, nz, omega, s);
+    case kTRT: return dispatch_lattice<Real, kTRT>(lattice, cur, nxt, nx, ny, nz, omega, s);
+    case kMRT: return dispatch_lattice<Real, kMRT>(lattice, cur, nxt, nx, ny, nz, omega, s);
+    case kRLBM: return dispatch_lattice<Real, kRLBM>(lattice, cur, nxt, nx, ny, nz, omega, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace lbcube
+
+using namespace lbcube;
+
+#define LBCUBE_STEP_SYMBOL(lat, LAT, real, op, OP)                                                \
+  extern "C" int lbm_launch_step_gpu_##lat##_##real##_##op(                                     \
+      const real* current_populations, real* next_populations, size_t x_extent,                 \
+      size_t y_extent, size_t z_extent, real omega, unsigned block_x, unsigned block_y,         \
+      unsigned block_z) {                                                                       \
+    return (int)launch_fluid_step<LAT, real, OP>(current_populations, next_populations,        \
+                                                 x_extent, y_extent, z_extent, omega, block_x, \
+                                                 block_y, block_z, (cudaStream_t)0);            \
+  }
+
+#define LBCUBE_STEP_OPS(lat, LAT, real)              \
+  LBCUBE_STEP_SYMBOL(lat, LAT, real, bgk, kBGK)      \
+  LBCUBE_STEP_SYMBOL(lat, LAT, real, trt, kTRT)      \
+  LBCUBE_STEP_SYMBOL(lat, LAT, real, mrt, kMRT)      \
+  LBCUBE_STEP_SYMBOL(lat, LAT, real, rlbm, kRLBM)
+
+LBCUBE_STEP_OPS(d2q9, D2Q9, float)
+LBCUBE_STEP_OPS(d2q9, D2Q9, double)
+LBCUBE_STEP_OPS(d3q19, D3Q19, float)
+LBCUBE_STEP_OPS(d3q19, D3Q19, double)
+LBCUBE_STEP_OPS(d3q27, D3Q27, float)
+LBCUBE_STEP_OPS(d3q27, D3Q27, double)
+
+extern "C" int lbm_step_async(int lattice, int precision, int collision,
+                              const void* current_populations, void* next_populations,
+                              size_t x_extent, size_t y_extent, size_t z_extent, double omega,
+                              void* stream) {
+  const cudaStream_t s = as_stream(stream);
+  if (precision == LBM_FLOAT)
+    return (int)dispatch_collision<float>(lattice, collision, current_populations,
+                                          next_populations, x_extent, y_extent, z_extent, omega, s);
+  if (precision == LBM_DOUBLE)
+    return (int)dispatch_collision<double>(lattice, collision, current_populations,
+                                           next_populations, x_extent, y_extent, z_extent, omega,
+                                           s);
+  return (int)cudaErrorInvalidValue;
+}

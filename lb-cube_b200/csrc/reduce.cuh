@@ -1,0 +1,44 @@
+// Deterministic FP64 block reductions for the statistics epilogues.
+//
+// Every block writes one partial per quantity; a single-block second pass sums
+// the partials in a fixed order. No atomics, so the result is identical from
+// run to run for a given domain.
+#pragma once
+
+#include "common.cuh"
+
+namespace lbcube {
+
+// Number of FP64 sums the reactive statistics carry per block:
+// sum C_A, sum C_B, sum C_A^2, sum C_B^2, sum C_A C_B (lattice_io.hpp:266-271).
+constexpr int kStatSums = 5;
+
+// Sums v[0..N) over the block (all kThreads threads must call it) and writes
+// the block's totals to out[0..N) from thread 0. Fixed reduction tree.
+template <int N>
+__device__ __forceinline__ void block_sum_to(double (&v)[N], double* out) {
+  constexpr int kWarps = kThreads / 32;
+  __shared__ double part[kWarps][N];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) part[warp][k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double s = part[0][k];
+#pragma unroll
+      for (int w = 1; w < kWarps; ++w) s += part[w][k];
+      out[k] = s;
+    }
+  }
+}
+
+}  // namespace lbcube

@@ -1,0 +1,159 @@
+// Reactive-mixing statistics on the device, replacing the host loop of
+// compute_reactive_stats (include/lattice_io.hpp:256-338).
+//
+// Pass 1 (stats_partials_kernel, or the epilogue of fluid_reaction_kernel)
+// writes per-block FP64 sums of C_A, C_B, C_A^2, C_B^2, C_A C_B. Pass 2
+// (stats_finalize_kernel, one block) adds the partials in a fixed order and
+// forms the eight ReactiveDiagnostics fields (lattice_io.hpp:148-166) with the
+// reference's formulas (:318-337), in FP64.
+#include "collide.cuh"
+#include "common.cuh"
+#include "reduce.cuh"
+#include "../../include/lbcube_b200.h"
+
+namespace lbcube {
+
+template <class SL, class Real>
+__global__ void __launch_bounds__(kThreads)
+    stats_partials_kernel(const Real* __restrict__ a, const Real* __restrict__ b, Grid g,
+                          double* __restrict__ partials) {
+  int x, y, z;
+  const bool active = cell_of(g, x, y, z);
+  double sums[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (active) {
+    const size_t plane = (size_t)g.plane;
+    const int cell = (z * g.ny + y) * g.nx + x;
+    Real ga[SL::Q], gb[SL::Q];
+    static_for<SL::Q>([&](auto I) {
+      ga[LB_I(I)] = __ldg(a + plane * LB_I(I) + cell);
+      gb[LB_I(I)] = __ldg(b + plane * LB_I(I) + cell);
+    });
+    const double ca = (double)concentration<SL>(ga);
+    const double cb = (double)concentration<SL>(gb);
+    sums[0] = ca;
+    sums[1] = cb;
+    sums[2] = ca * ca;
+    sums[3] = cb * cb;
+    sums[4] = ca * cb;
+  }
+  block_sum_to<kStatSums>(sums, partials + block_linear() * kStatSums);
+}
+
+constexpr int kFinalThreads = 1024;
+
+__global__ void __launch_bounds__(kFinalThreads)
+    stats_finalize_kernel(const double* __restrict__ partials, long long blocks, long long cells,
+                          double k, double* __restrict__ out) {
+  __shared__ double sh[kFinalThreads][kStatSums];
+  double s[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (long long blk = threadIdx.x; blk < blocks; blk += kFinalThreads) {
+#pragma unroll
+    for (int q = 0; q < kStatSums; ++q) s[q] += partials[blk * kStatSums + q];
+  }
+#pragma unroll
+  for (int q = 0; q < kStatSums; ++q) sh[threadIdx.x][q] = s[q];
+  __syncthreads();
+  for (int stride = kFinalThreads / 2; stride > 0; stride >>= 1) {
+    if ((int)threadIdx.x < stride) {
+#pragma unroll
+      for (int q = 0; q < kStatSums; ++q) sh[threadIdx.x][q] += sh[threadIdx.x + stride][q];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double inv = 1.0 / (double)cells;
+    const double ma = sh[0][0] * inv, mb = sh[0][1] * inv;
+    const double ma2 = sh[0][2] * inv, mb2 = sh[0][3] * inv, mab = sh[0][4] * inv;
+    const double cov = mab - ma * mb;
+    const double mp = ma * mb;
+    const double eps = 2.220446049250313080847e-16;
+    out[0] = ma;
+    out[1] = mb;
+    out[2] = ma2 - ma * ma;
+    out[3] = mb2 - mb * mb;
+    out[4] = cov;
+    out[5] = fabs(mp) > eps ? cov / mp : 0.0;
+    out[6] = k * mab;
+    out[7] = k * ma * mb;
+  }
+}
+
+cudaError_t launch_finalize(const Grid& g, double k, const double* partials, double* out,
+                            cudaStream_t s) {
+  stats_finalize_kernel<<<1, kFinalThreads, 0, s>>>(partials, g.blocks(), g.plane, k, out);
+  return cudaGetLastError();
+}
+
+template <class SL, class Real>
+cudaError_t launch_stats(const void* va, const void* vb, size_t nx, size_t ny, size_t nz, double k,
+                         double* partials, size_t pbytes, double* out, cudaStream_t s) {
+  const Real* a = static_cast<const Real*>(va);
+  const Real* b = static_cast<const Real*>(vb);
+  Grid g;
+  cudaError_t err = validate_domain(a == nullptr || b == nullptr || partials == nullptr ||
+                                        out == nullptr,
+                                    1, 1, 1, SL::D, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  const size_t need = (size_t)g.blocks() * kStatSums * sizeof(double);
+  if (pbytes < need) return cudaErrorInvalidValue;
+  const size_t sb = (size_t)SL::Q * g.plane * sizeof(Real);
+  const Span reads[2] = {{a, sb}, {b, sb}};
+  const Span writes[2] = {{partials, need}, {out, 8 * sizeof(double)}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  stats_partials_kernel<SL, Real><<<grid_dims(g), kThreads, 0, s>>>(a, b, g, partials);
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  return launch_finalize(g, k, partials, out, s);
+}
+
+}  // namespace lbcube
+
+using namespace lbcube;
+
+extern "C" size_t lbm_stats_partials_bytes(int fluid_lattice, size_t x_extent, size_t y_extent,
+                                           size_t z_extent) {
+  Grid g;
+  const int dims = fluid_lattice == LBM_D2Q9 || fluid_lattice == LBM_D2Q5 ? 2 : 3;
+  if (validate_domain(false, 1, 1, 1, dims, x_extent, y_extent, z_extent, g) != cudaSuccess)
+    return 0;
+  return (size_t)g.blocks() * kStatSums * sizeof(double);
+}
+
+extern "C" int lbm_reactive_stats_async(int scalar_lattice, int precision, const void* current_a,
+                                        const void* current_b, size_t x_extent, size_t y_extent,
+                                        size_t z_extent, double k_react, double* partials,
+                                        size_t partials_bytes, double* diagnostics,
+                                        void* stream) {
+  const cudaStream_t s = as_stream(stream);
+  if (scalar_lattice == LBM_D2Q5) {
+    if (precision == LBM_FLOAT)
+      return (int)launch_stats<D2Q5, float>(current_a, current_b, x_extent, y_extent, z_extent,
+                                            k_react, partials, partials_bytes, diagnostics, s);
+    if (precision == LBM_DOUBLE)
+      return (int)launch_stats<D2Q5, double>(current_a, current_b, x_extent, y_extent, z_extent,
+                                             k_react, partials, partials_bytes, diagnostics, s);
+  } else if (scalar_lattice == LBM_D3Q7) {
+    if (precision == LBM_FLOAT)
+      return (int)launch_stats<D3Q7, float>(current_a, current_b, x_extent, y_extent, z_extent,
+                                            k_react, partials, partials_bytes, diagnostics, s);
+    if (precision == LBM_DOUBLE)
+      return (int)launch_stats<D3Q7, double>(current_a, current_b, x_extent, y_extent, z_extent,
+                                             k_react, partials, partials_bytes, diagnostics, s);
+  }
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int lbm_reactive_stats_finalize_async(int fluid_lattice, size_t x_extent,
+                                                 size_t y_extent, size_t z_extent,
+                                                 double k_react, const double* partials,
+                                                 size_t partials_bytes, double* diagnostics,
+                                                 void* stream) {
+  Grid g;
+  const int dims = fluid_lattice == LBM_D2Q9 || fluid_lattice == LBM_D2Q5 ? 2 : 3;
+  cudaError_t err = validate_domain(partials == nullptr || diagnostics == nullptr, 1, 1, 1, dims,
+                                    x_extent, y_extent, z_extent, g);
+  if (err != cudaSuccess) return (int)err;
+  if (partials_bytes < (size_t)g.blocks() * kStatSums * sizeof(double))
+    return (int)cudaErrorInvalidValue;
+  return (int)launch_finalize(g, k_react, partials, diagnostics, as_stream(stream));
+}

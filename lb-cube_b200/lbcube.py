@@ -1,0 +1,243 @@
+"""Python front end of the B200 lattice Boltzmann engine (ctypes over the C ABI).
+
+The launchers mirror LB-Cube's CUDA launcher API (include/lattice_cuda.cuh:
+179-319): same names, same argument meaning (device buffers in the unpadded
+[Q, Z, Y, X] layout, element extents, relaxation frequencies), and the same
+``cudaError_t`` return codes, including the reference's validation order. Any
+object with ``data_ptr()`` (a torch CUDA tensor) or a plain integer address can
+be passed as a buffer; ``None`` is the null pointer.
+
+The engine library (``liblbcube_b200.so`` next to this file) must have been
+built (``python lb-cube_b200/build.py``); importing this module without it
+raises, there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbcube_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "lbcube_b200.h")
+
+LATTICES = {"D2Q9": 0, "D3Q19": 1, "D3Q27": 2, "D2Q5": 3, "D3Q7": 4}
+Q_OF = {"D2Q9": 9, "D3Q19": 19, "D3Q27": 27, "D2Q5": 5, "D3Q7": 7}
+D_OF = {"D2Q9": 2, "D3Q19": 3, "D3Q27": 3, "D2Q5": 2, "D3Q7": 3}
+SCALAR_OF = {"D2Q9": "D2Q5", "D3Q19": "D3Q7", "D3Q27": "D3Q7"}
+COLLISIONS = {"BGK": 0, "TRT": 1, "MRT": 2, "RLBM": 3}
+REALS = {"float": 0, "double": 1}
+
+# cudaError_t values returned by the launchers
+cudaSuccess = 0
+cudaErrorInvalidValue = 1
+cudaErrorInvalidConfiguration = 9
+cudaErrorInvalidDevicePointer = 17
+
+STATS_FIELDS = ("mean_A", "mean_B", "var_A", "var_B", "covariance", "segregation_intensity",
+                "true_reaction_rate", "mixed_reaction_rate")
+
+_lib = None
+
+
+class LbmCudaError(RuntimeError):
+    def __init__(self, what: str, code: int):
+        super().__init__(f"{what} failed with cudaError_t {code}")
+        self.code = code
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load() -> C.CDLL:
+    """The engine library, loaded once. Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"engine library {LIB_PATH} is missing: build it with "
+                "`python lb-cube_b200/build.py` (there is no CPU fallback)")
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+_sz, _vp, _u = C.c_size_t, C.c_void_p, C.c_uint
+
+
+def _declare(lib):
+    for lat in ("d2q9", "d3q19", "d3q27"):
+        for real, ct in (("float", C.c_float), ("double", C.c_double)):
+            for op in ("bgk", "trt", "mrt", "rlbm"):
+                fn = getattr(lib, f"lbm_launch_step_gpu_{lat}_{real}_{op}")
+                fn.restype = C.c_int
+                fn.argtypes = [_vp, _vp, _sz, _sz, _sz, ct, _u, _u, _u]
+    for fl, sl in (("d2q9", "d2q5"), ("d3q19", "d3q7"), ("d3q27", "d3q7")):
+        for real, ct in (("float", C.c_float), ("double", C.c_double)):
+            fn = getattr(lib, f"lbm_launch_scalar_step_gpu_{fl}_{sl}_{real}")
+            fn.restype = C.c_int
+            fn.argtypes = [_vp, _vp, _vp, _sz, _sz, _sz, ct, ct, _u, _u, _u]
+            fn = getattr(lib, f"lbm_launch_reaction_ab_gpu_{fl}_{sl}_{real}")
+            fn.restype = C.c_int
+            fn.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz, ct, ct, _u, _u, _u]
+    d = C.c_double
+    sig = {
+        "lbm_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, _vp],
+        "lbm_scalar_step_async": [C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, d, d, _vp],
+        "lbm_reaction_ab_async": [C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz, d, d, _vp],
+        "lbm_fluid_reaction_ab_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
+                                        _sz, _sz, _sz, d, d, d, _vp, _sz, _vp],
+        "lbm_reactive_stats_async": [C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
+        "lbm_reactive_stats_finalize_async": [C.c_int, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
+        "lbm_init_equilibrium_async": [C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, _vp],
+    }
+    for name, args in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = C.c_int
+        fn.argtypes = args
+    lib.lbm_stats_partials_bytes.restype = C.c_size_t
+    lib.lbm_stats_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
+
+
+def _ptr(buf):
+    if buf is None:
+        return None
+    if isinstance(buf, int):
+        return buf
+    return buf.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream  # torch.cuda.Stream
+
+
+def real_name(dtype) -> str:
+    s = str(dtype)
+    if "float32" in s or s == "float":
+        return "float"
+    if "float64" in s or s == "double":
+        return "double"
+    raise ValueError(f"unsupported precision {dtype}")
+
+
+def check(code: int, what: str = "launch") -> None:
+    if code != cudaSuccess:
+        raise LbmCudaError(what, code)
+
+
+# --------------------------------------------------------------------------
+# Reference-named launchers (return the cudaError_t code, like the reference)
+# --------------------------------------------------------------------------
+def launch_step_gpu(lattice, real, collision, current_populations, next_populations, x_extent,
+                    y_extent, z_extent, omega, block=(16, 8, 1)) -> int:
+    """lbm::launch_step_gpu<Lattice, Real, CT> (include/lattice_cuda.cuh:179-190)."""
+    fn = getattr(load(), f"lbm_launch_step_gpu_{lattice.lower()}_{real_name(real)}_{collision.lower()}")
+    return fn(_ptr(current_populations), _ptr(next_populations), x_extent, y_extent, z_extent,
+              omega, *block)
+
+
+def launch_step_gpu_mem(lattice, real, collision, mem_extents, current_populations,
+                        next_populations, omega, block=(16, 8, 1)) -> int:
+    """The LatticeMemory overload (include/lattice_cuda.cuh:310-319): extents from a memory object."""
+    nx, ny, nz = mem_extents
+    return launch_step_gpu(lattice, real, collision, current_populations, next_populations, nx, ny,
+                           nz, omega, block)
+
+
+def launch_scalar_step_gpu(fluid_lattice, real, current_scalar, next_scalar, current_fluid,
+                           x_extent, y_extent, z_extent, omega_c, source_term=0.0,
+                           block=(16, 8, 1)) -> int:
+    """lbm::launch_scalar_step_gpu<FL, SL, Real> (include/lattice_cuda.cuh:209-222)."""
+    sl = SCALAR_OF[fluid_lattice].lower()
+    fn = getattr(load(), f"lbm_launch_scalar_step_gpu_{fluid_lattice.lower()}_{sl}_{real_name(real)}")
+    return fn(_ptr(current_scalar), _ptr(next_scalar), _ptr(current_fluid), x_extent, y_extent,
+              z_extent, omega_c, source_term, *block)
+
+
+def launch_scalar_step_gpu_mem(fluid_lattice, real, scalar_extents, fluid_extents, current_scalar,
+                               next_scalar, current_fluid, omega_c, source_term=0.0,
+                               block=(16, 8, 1)) -> int:
+    """The LatticeMemory overload (include/lattice_cuda.cuh:243-255, src/lattice_cuda.cu:716-747):
+    mismatched scalar/fluid extents return cudaErrorInvalidValue."""
+    if tuple(scalar_extents) != tuple(fluid_extents):
+        return cudaErrorInvalidValue
+    nx, ny, nz = scalar_extents
+    return launch_scalar_step_gpu(fluid_lattice, real, current_scalar, next_scalar, current_fluid,
+                                  nx, ny, nz, omega_c, source_term, block)
+
+
+def launch_reaction_AB_gpu(fluid_lattice, real, current_a, next_a, current_b, next_b,
+                           current_fluid, x_extent, y_extent, z_extent, omega_c, k_react,
+                           block=(16, 8, 1)) -> int:
+    """lbm::launch_reaction_AB_gpu<FL, SL, Real> (include/lattice_cuda.cuh:276-291)."""
+    sl = SCALAR_OF[fluid_lattice].lower()
+    fn = getattr(load(), f"lbm_launch_reaction_ab_gpu_{fluid_lattice.lower()}_{sl}_{real_name(real)}")
+    return fn(_ptr(current_a), _ptr(next_a), _ptr(current_b), _ptr(next_b), _ptr(current_fluid),
+              x_extent, y_extent, z_extent, omega_c, k_react, *block)
+
+
+# --------------------------------------------------------------------------
+# Stream-ordered extensions
+# --------------------------------------------------------------------------
+def step_async(lattice, real, collision, cur, nxt, nx, ny, nz, omega, stream=None) -> int:
+    return load().lbm_step_async(LATTICES[lattice], REALS[real_name(real)], COLLISIONS[collision],
+                                 _ptr(cur), _ptr(nxt), nx, ny, nz, float(omega), _stream(stream))
+
+
+def scalar_step_async(fluid_lattice, real, cur_s, nxt_s, cur_f, nx, ny, nz, omega_c, source=0.0,
+                      stream=None) -> int:
+    return load().lbm_scalar_step_async(LATTICES[fluid_lattice], REALS[real_name(real)], _ptr(cur_s),
+                                        _ptr(nxt_s), _ptr(cur_f), nx, ny, nz, float(omega_c),
+                                        float(source), _stream(stream))
+
+
+def reaction_ab_async(fluid_lattice, real, cur_a, nxt_a, cur_b, nxt_b, cur_f, nx, ny, nz, omega_c,
+                      k_react, stream=None) -> int:
+    return load().lbm_reaction_ab_async(LATTICES[fluid_lattice], REALS[real_name(real)], _ptr(cur_a),
+                                        _ptr(nxt_a), _ptr(cur_b), _ptr(nxt_b), _ptr(cur_f), nx, ny,
+                                        nz, float(omega_c), float(k_react), _stream(stream))
+
+
+def stats_partials_bytes(fluid_lattice, nx, ny, nz) -> int:
+    return load().lbm_stats_partials_bytes(LATTICES[fluid_lattice], nx, ny, nz)
+
+
+def fluid_reaction_ab_async(fluid_lattice, real, collision, cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b,
+                            nx, ny, nz, omega, omega_c, k_react, partials=None, partials_bytes=0,
+                            stream=None) -> int:
+    return load().lbm_fluid_reaction_ab_async(
+        LATTICES[fluid_lattice], REALS[real_name(real)], COLLISIONS[collision], _ptr(cur_f),
+        _ptr(nxt_f), _ptr(cur_a), _ptr(nxt_a), _ptr(cur_b), _ptr(nxt_b), nx, ny, nz, float(omega),
+        float(omega_c), float(k_react), _ptr(partials), int(partials_bytes), _stream(stream))
+
+
+def reactive_stats_async(scalar_lattice, real, a, b, nx, ny, nz, k_react, partials, partials_bytes,
+                         diagnostics, stream=None) -> int:
+    return load().lbm_reactive_stats_async(LATTICES[scalar_lattice], REALS[real_name(real)], _ptr(a),
+                                           _ptr(b), nx, ny, nz, float(k_react), _ptr(partials),
+                                           int(partials_bytes), _ptr(diagnostics), _stream(stream))
+
+
+def reactive_stats_finalize_async(fluid_lattice, nx, ny, nz, k_react, partials, partials_bytes,
+                                  diagnostics, stream=None) -> int:
+    return load().lbm_reactive_stats_finalize_async(LATTICES[fluid_lattice], nx, ny, nz,
+                                                    float(k_react), _ptr(partials),
+                                                    int(partials_bytes), _ptr(diagnostics),
+                                                    _stream(stream))
+
+
+def init_equilibrium_async(lattice, real, rho, u, populations, nx, ny, nz, stream=None) -> int:
+    return load().lbm_init_equilibrium_async(LATTICES[lattice], REALS[real_name(real)], _ptr(rho),
+                                             _ptr(u), _ptr(populations), nx, ny, nz, _stream(stream))
+
+
+def declared_symbols(header: str = HEADER):
+    """Names of every function the C ABI header declares."""
+    import re
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^(?:int|size_t)\s+(lbm_\w+)\s*\(", text, flags=re.M)))

@@ -1,0 +1,105 @@
+"""CPU: the engine library loads, exports every symbol its C header declares,
+and its launchers reject bad arguments with the reference's error codes before
+touching the GPU (src/lattice_cuda.cu:488-503). Fake, never-dereferenced
+addresses stand in for device buffers: every case below returns before any
+CUDA call is made."""
+import ctypes as C
+
+import pytest
+
+import lbcube as E
+
+# Fake device addresses (never dereferenced: validation fails first).
+A0, A1, A2, A3, A4 = 0x10000000, 0x20000000, 0x30000000, 0x40000000, 0x50000000
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import os
+
+    if not os.path.exists(E.LIB_PATH):
+        import build
+
+        build.build()
+    return E.load()
+
+
+def test_exports_every_declared_symbol(lib):
+    declared = E.declared_symbols()
+    assert len(declared) >= 44
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_reference_launcher_set_is_complete():
+    """24 step + 6 scalar + 6 reaction instantiations (src/lattice_cuda.cu:756-1029)."""
+    declared = set(E.declared_symbols())
+    steps = [s for s in declared if s.startswith("lbm_launch_step_gpu_")]
+    scal = [s for s in declared if s.startswith("lbm_launch_scalar_step_gpu_")]
+    reac = [s for s in declared if s.startswith("lbm_launch_reaction_ab_gpu_")]
+    assert (len(steps), len(scal), len(reac)) == (24, 6, 6)
+
+
+@pytest.mark.parametrize("lat", ["D2Q9", "D3Q19", "D3Q27"])
+@pytest.mark.parametrize("real", ["float", "double"])
+@pytest.mark.parametrize("op", ["BGK", "TRT", "MRT", "RLBM"])
+def test_step_validation_order(lib, lat, real, op):
+    f = lambda *a, **k: E.launch_step_gpu(lat, real, op, *a, **k)  # noqa: E731
+    # null pointer first, even with a zero block and zero extents
+    assert f(None, A1, 0, 0, 0, 1.0, block=(0, 0, 0)) == E.cudaErrorInvalidDevicePointer
+    assert f(A0, None, 8, 8, 8, 1.0) == E.cudaErrorInvalidDevicePointer
+    # zero block dimension before extents
+    assert f(A0, A1, 0, 8, 8, 1.0, block=(16, 0, 1)) == E.cudaErrorInvalidConfiguration
+    assert f(A0, A1, 8, 8, 8, 1.0, block=(16, 8, 0)) == E.cudaErrorInvalidConfiguration
+    # zero extents
+    assert f(A0, A1, 0, 8, 8, 1.0) == E.cudaErrorInvalidValue
+    assert f(A0, A1, 8, 0, 8, 1.0) == E.cudaErrorInvalidValue
+    if lat != "D2Q9":
+        assert f(A0, A1, 8, 8, 0, 1.0) == E.cudaErrorInvalidValue
+    # overlapping read/write buffers (engine check)
+    assert f(A0, A0, 8, 8, 8, 1.0) == E.cudaErrorInvalidValue
+    assert f(A0, A0 + 64, 8, 8, 8, 1.0) == E.cudaErrorInvalidValue
+    # more than 2^31 - 1 cells (engine limit)
+    if lat != "D2Q9":
+        assert f(A0, A0 + (1 << 44), 2048, 2048, 1024, 1.0) == E.cudaErrorInvalidValue
+
+
+@pytest.mark.parametrize("fl", ["D2Q9", "D3Q19", "D3Q27"])
+@pytest.mark.parametrize("real", ["float", "double"])
+def test_scalar_and_reaction_validation(lib, fl, real):
+    s = E.launch_scalar_step_gpu
+    assert s(fl, real, A0, A1, None, 8, 8, 8, 1.2) == E.cudaErrorInvalidDevicePointer
+    assert s(fl, real, A0, A1, A2, 8, 8, 8, 1.2, block=(0, 8, 1)) == E.cudaErrorInvalidConfiguration
+    assert s(fl, real, A0, A1, A2, 0, 8, 8, 1.2) == E.cudaErrorInvalidValue
+    assert s(fl, real, A0, A0, A2, 8, 8, 8, 1.2) == E.cudaErrorInvalidValue
+    # LatticeMemory overload: mismatched scalar / fluid extents (src/lattice_cuda.cu:731-735)
+    assert E.launch_scalar_step_gpu_mem(fl, real, (8, 8, 8), (8, 8, 4), A0, A1, A2, 1.2) == \
+        E.cudaErrorInvalidValue
+    r = E.launch_reaction_AB_gpu
+    assert r(fl, real, A0, A1, A2, A3, None, 8, 8, 8, 1.2, 0.01) == E.cudaErrorInvalidDevicePointer
+    assert r(fl, real, A0, A1, A2, A3, A4, 8, 8, 8, 1.2, 0.01, block=(1, 1, 0)) == \
+        E.cudaErrorInvalidConfiguration
+    assert r(fl, real, A0, A1, A2, A3, A4, 8, 0, 8, 1.2, 0.01) == E.cudaErrorInvalidValue
+    # next_a aliasing current_b
+    assert r(fl, real, A0, A2, A2, A3, A4, 8, 8, 8, 1.2, 0.01) == E.cudaErrorInvalidValue
+
+
+def test_2d_block_z_checked_before_forcing(lib):
+    """For 2D lattices the reference checks block.z == 0 before forcing it to 1
+    (src/lattice_cuda.cu:492-499)."""
+    assert E.launch_step_gpu("D2Q9", "float", "BGK", A0, A1, 8, 8, 1, 1.0, block=(16, 8, 0)) == \
+        E.cudaErrorInvalidConfiguration
+
+
+def test_extension_enum_validation(lib):
+    assert E.load().lbm_step_async(7, 0, 0, A0, A1, 8, 8, 8, 1.0, None) == E.cudaErrorInvalidValue
+    assert E.load().lbm_step_async(1, 5, 0, A0, A1, 8, 8, 8, 1.0, None) == E.cudaErrorInvalidValue
+    assert E.load().lbm_step_async(1, 0, 9, A0, A1, 8, 8, 8, 1.0, None) == E.cudaErrorInvalidValue
+    # the fused fluid + reaction launch has no RLBM variant
+    assert E.fluid_reaction_ab_async("D3Q19", "float", "RLBM", A0, A1, A2, A3, A4, A4 + (1 << 30),
+                                     8, 8, 8, 1.6, 1.2, 0.01) == E.cudaErrorInvalidValue
+    assert E.stats_partials_bytes("D3Q19", 256, 256, 256) == 2 * 256 * 256 * 5 * 8
+    assert E.stats_partials_bytes("D2Q9", 1024, 1024, 7) == 8 * 1024 * 5 * 8
+    # a too-small partials buffer is rejected
+    assert E.reactive_stats_async("D3Q7", "float", A0, A1, 256, 256, 256, 0.1, A2, 16, A3) == \
+        E.cudaErrorInvalidValue
