@@ -274,15 +274,16 @@ size_t lbm_stats_partials_bytes(int fluid_lattice, size_t x_extent, size_t y_ext
  * scratch of lbm_stats_partials_bytes bytes. `diagnostics` (device, 8
  * doubles) receives mean_A, mean_B, var_A, var_B, covariance,
  * segregation_intensity, true_reaction_rate, mixed_reaction_rate
- * (ReactiveDiagnostics, include/lattice_io.hpp:148-166). */
+ * (ReactiveDiagnostics, include/lattice_io.hpp:148-166). As in the
+ * reference, k_react is taken in the population precision. */
 int lbm_reactive_stats_async(int scalar_lattice, int precision, const void* current_a,
     const void* current_b, size_t x_extent, size_t y_extent, size_t z_extent, double k_react,
     double* partials, size_t partials_bytes, double* diagnostics, void* stream);
 
 /* Second pass of the statistics over partials written by a fused launch. */
-int lbm_reactive_stats_finalize_async(int fluid_lattice, size_t x_extent, size_t y_extent,
-    size_t z_extent, double k_react, const double* partials, size_t partials_bytes,
-    double* diagnostics, void* stream);
+int lbm_reactive_stats_finalize_async(int fluid_lattice, int precision, size_t x_extent,
+    size_t y_extent, size_t z_extent, double k_react, const double* partials,
+    size_t partials_bytes, double* diagnostics, void* stream);
 
 /* Equilibrium initialisation from macroscopic fields (device, `precision`):
  * rho[N] (density, or concentration for D2Q5/D3Q7) and u[D*N] component-major.

@@ -15,10 +15,14 @@
 
 namespace lbcube {
 
+// exp for the reaction source. The float version is evaluated in double and
+// rounded once, which is (almost always) the correctly rounded single-precision
+// value that the host libm's expf returns, so the float reaction step tracks
+// the CPU path more closely than a single-precision device exp would.
 template <class Real>
 __device__ __forceinline__ Real rexp(Real x);
 template <>
-__device__ __forceinline__ float rexp<float>(float x) { return expf(x); }
+__device__ __forceinline__ float rexp<float>(float x) { return (float)exp((double)x); }
 template <>
 __device__ __forceinline__ double rexp<double>(double x) { return exp(x); }
 

@@ -103,7 +103,8 @@ cudaError_t launch_stats(const void* va, const void* vb, size_t nx, size_t ny, s
   stats_partials_kernel<SL, Real><<<grid_dims(g), kThreads, 0, s>>>(a, b, g, partials);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
-  return launch_finalize(g, k, partials, out, s);
+  // k_react has the population precision, as in compute_reactive_stats<SL, Real>.
+  return launch_finalize(g, (double)(Real)k, partials, out, s);
 }
 
 }  // namespace lbcube
@@ -143,9 +144,10 @@ extern "C" int lbm_reactive_stats_async(int scalar_lattice, int precision, const
   return (int)cudaErrorInvalidValue;
 }
 
-extern "C" int lbm_reactive_stats_finalize_async(int fluid_lattice, size_t x_extent,
-                                                 size_t y_extent, size_t z_extent,
-                                                 double k_react, const double* partials,
+extern "C" int lbm_reactive_stats_finalize_async(int fluid_lattice, int precision,
+                                                 size_t x_extent, size_t y_extent,
+                                                 size_t z_extent, double k_react,
+                                                 const double* partials,
                                                  size_t partials_bytes, double* diagnostics,
                                                  void* stream) {
   Grid g;
@@ -155,5 +157,7 @@ extern "C" int lbm_reactive_stats_finalize_async(int fluid_lattice, size_t x_ext
   if (err != cudaSuccess) return (int)err;
   if (partials_bytes < (size_t)g.blocks() * kStatSums * sizeof(double))
     return (int)cudaErrorInvalidValue;
-  return (int)launch_finalize(g, k_react, partials, diagnostics, as_stream(stream));
+  if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return (int)cudaErrorInvalidValue;
+  const double k = precision == LBM_FLOAT ? (double)(float)k_react : k_react;
+  return (int)launch_finalize(g, k, partials, diagnostics, as_stream(stream));
 }

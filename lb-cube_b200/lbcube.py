@@ -88,7 +88,7 @@ def _declare(lib):
         "lbm_fluid_reaction_ab_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp,
                                         _sz, _sz, _sz, d, d, d, _vp, _sz, _vp],
         "lbm_reactive_stats_async": [C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
-        "lbm_reactive_stats_finalize_async": [C.c_int, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
+        "lbm_reactive_stats_finalize_async": [C.c_int, C.c_int, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
         "lbm_init_equilibrium_async": [C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, _vp],
     }
     for name, args in sig.items():
@@ -222,9 +222,10 @@ def reactive_stats_async(scalar_lattice, real, a, b, nx, ny, nz, k_react, partia
                                            int(partials_bytes), _ptr(diagnostics), _stream(stream))
 
 
-def reactive_stats_finalize_async(fluid_lattice, nx, ny, nz, k_react, partials, partials_bytes,
+def reactive_stats_finalize_async(fluid_lattice, real, nx, ny, nz, k_react, partials, partials_bytes,
                                   diagnostics, stream=None) -> int:
-    return load().lbm_reactive_stats_finalize_async(LATTICES[fluid_lattice], nx, ny, nz,
+    return load().lbm_reactive_stats_finalize_async(LATTICES[fluid_lattice], REALS[real_name(real)],
+                                                    nx, ny, nz,
                                                     float(k_react), _ptr(partials),
                                                     int(partials_bytes), _ptr(diagnostics),
                                                     _stream(stream))
