@@ -280,6 +280,22 @@ int lbm_reactive_stats_async(int scalar_lattice, int precision, const void* curr
     const void* current_b, size_t x_extent, size_t y_extent, size_t z_extent, double k_react,
     double* partials, size_t partials_bytes, double* diagnostics, void* stream);
 
+/* Allocation-free form of lbm_reactive_stats_async. No counterpart in the
+ * reference. For callers that cannot allocate device memory, e.g. a plugin or
+ * FFI binding inside an application that owns every device allocation and
+ * passes this library only the two scalar fields: the FP64 partial sums go to
+ * a fixed array inside the library (5 MiB, reserved on every GPU that loads
+ * the library until the process exits) instead of caller scratch. Limit:
+ * ceil(x_extent / 128) * y_extent * z_extent <= LBM_STATS_NOALLOC_MAX_BLOCKS
+ * (e.g. 256^3 or 1024^2); larger domains return cudaErrorInvalidValue. The
+ * first call on a device looks up the array's device address for that device
+ * (make it before any stream capture). All calls share the array: calls that
+ * overlap on the GPU (other streams, other threads) race, so serialise them. */
+#define LBM_STATS_NOALLOC_MAX_BLOCKS 131072
+int lbm_reactive_stats_noalloc_async(int scalar_lattice, int precision, const void* current_a,
+    const void* current_b, size_t x_extent, size_t y_extent, size_t z_extent, double k_react,
+    double* diagnostics, void* stream);
+
 /* Second pass of the statistics over partials written by a fused launch. */
 int lbm_reactive_stats_finalize_async(int fluid_lattice, int precision, size_t x_extent,
     size_t y_extent, size_t z_extent, double k_react, const double* partials,

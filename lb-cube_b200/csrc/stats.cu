@@ -161,3 +161,66 @@ extern "C" int lbm_reactive_stats_finalize_async(int fluid_lattice, int precisio
   const double k = precision == LBM_FLOAT ? (double)(float)k_react : k_react;
   return (int)launch_finalize(g, k, partials, diagnostics, as_stream(stream));
 }
+
+// ----------------------------------------------------------------------------
+// Allocation-free statistics.
+//
+// For callers that cannot allocate device memory: for example a solver plugin
+// or an FFI binding inside a host application that owns every device
+// allocation through its own pool and hands this library only the scalar
+// fields, so it has no way to obtain the partial-sum scratch that
+// lbm_reactive_stats_async needs. Here the scratch is a file-scope device
+// array of fixed size, reserved on every GPU that loads the library until the
+// process exits; nothing is allocated per call.
+// ----------------------------------------------------------------------------
+#include <mutex>
+
+namespace lbcube {
+
+// Partial sums for up to this many 128-cell row segments (blocks):
+// ceil(nx / 128) * ny * nz <= 131072, e.g. 256^3 or 1024^2. 5 MiB per GPU.
+constexpr long long kNoAllocMaxBlocks = 131072;
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxBlocks * kStatSums];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mutex;
+static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_partials on the current device. In host code
+// the array's name only stands in for the symbol, so the address is looked up
+// once per device (with that device current) and cached.
+static cudaError_t noalloc_scratch(double** out) {
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    err = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (err != cudaSuccess) return err;
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace lbcube
+
+extern "C" int lbm_reactive_stats_noalloc_async(int scalar_lattice, int precision,
+                                                const void* current_a, const void* current_b,
+                                                size_t x_extent, size_t y_extent,
+                                                size_t z_extent, double k_react,
+                                                double* diagnostics, void* stream) {
+  double* scratch = nullptr;
+  const cudaError_t err = noalloc_scratch(&scratch);
+  if (err != cudaSuccess) return (int)err;
+  // Every block overwrites its own partial slots and the second pass reads
+  // only those, so nothing left in the array by an earlier call is used and
+  // nothing needs clearing. A domain with more blocks than the array holds is
+  // rejected with cudaErrorInvalidValue by the capacity check.
+  const size_t capacity = (size_t)kNoAllocMaxBlocks * kStatSums * sizeof(double);
+  return lbm_reactive_stats_async(scalar_lattice, precision, current_a, current_b, x_extent,
+                                  y_extent, z_extent, k_react, scratch, capacity, diagnostics,
+                                  stream);
+}
