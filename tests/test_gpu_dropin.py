@@ -47,7 +47,7 @@ def test_lbm_reaction_sim_gpu_matches_cpu(tmp_path):
     g = _run(tmp_path, "lbm_reaction_sim", "gpu", args)
     rc = list(csv.reader(open(c / "reaction_diagnostics.csv")))
     rg = list(csv.reader(open(g / "reaction_diagnostics.csv")))
-    assert rc[0] == rg[0] and len(rc) == len(rg) == 6
+    assert rc[0] == rg[0] and len(rc) == len(rg) == 7  # header, step 0, 5 outputs
     for a, b in zip(rc[1:], rg[1:]):
         assert a[0] == b[0]
         for x, y in zip(map(float, a[1:]), map(float, b[1:])):
