@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the other storage/lattice variants and the 2000-step accuracy run")
+    ap.add_argument("--storage", choices=["fp32", "f16s", "bf16s", "e3m12s", "q15s"], default="fp32",
+                    help="population storage of the timed run (16-bit ones are shifted)")
     ap.add_argument("--size", type=int, default=256,
                     help="cube edge; smaller sizes are for profiling captures only")
     a = ap.parse_args()
@@ -153,6 +157,13 @@ def committed_traffic(kernel_key):
 # ----------------------------------------------------------------------------
 # engine arm
 # ----------------------------------------------------------------------------
+C_D3Q19 = [[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
+           [1, 1, 0], [-1, 1, 0], [1, -1, 0], [-1, -1, 0], [1, 0, 1], [-1, 0, 1], [1, 0, -1],
+           [-1, 0, -1], [0, 1, 1], [0, -1, 1], [0, 1, -1], [0, -1, -1]]
+FORMAT_NOTE = {"q15s": "Q15 shifted (16-bit fixed point, |f/w - rho0| < 1)",
+               "e3m12s": "E3M12 shifted (sign, 3-bit exponent, 12-bit mantissa)",
+               "f16s": "IEEE FP16 shifted (x 4096)", "bf16s": "BF16 shifted"}
+FORMATS16 = ("q15s", "e3m12s", "f16s", "bf16s")
 def make_initial_state(torch, E, dev):
     """Taylor-Green + seeded noise, rho = 1, built on the device and turned into
     equilibrium populations by the engine's own init kernel."""
@@ -176,6 +187,125 @@ def make_initial_state(torch, E, dev):
     return f
 
 
+def _time_steps(torch, launch, a, b, steps, warmup):
+    """Mean ms per step of `launch(cur, nxt)` with ping-pong buffers (CUDA events)."""
+    import lbcube as E
+
+    for _ in range(warmup):
+        E.check(launch(a, b))
+        a, b = b, a
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream()
+    t0.record(stream)
+    for _ in range(steps):
+        rc = launch(a, b)
+        a, b = b, a
+    t1.record(stream)
+    torch.cuda.synchronize()
+    E.check(rc)
+    return t0.elapsed_time(t1) / steps
+
+
+def run_variants(torch, E, dev, f32, peak, fp32_ms):
+    """Single-GPU characterisation at the same size: other operators, 16-bit
+    shifted storage, D3Q27 and FP64. Each: 10 warm-up + 200 timed steps."""
+    omega = 1.0 / TAU
+    cells = NX * NY * NZ
+    out = []
+
+    def rec(name, ms, bytes_per_lu, **kw):
+        gbs = bytes_per_lu * cells / (ms * 1e-3) / 1e9
+        d = {"variant": name, "mlups": round(cells / (ms * 1e-3) / 1e6, 1), "ms_per_step": round(ms, 5),
+             "bytes_per_lu": bytes_per_lu, "achieved_gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 4)}
+        d.update(kw)
+        out.append(d)
+        return d
+
+    g = torch.empty_like(f32)
+    for op in ("MRT", "BGK"):
+        ms = _time_steps(torch, lambda a, b, op=op: E.launch_step_gpu("D3Q19", "float", op, a, b, NX, NY, NZ, omega),
+                         f32.clone(), g, 200, 10)
+        rec(f"D3Q19 {op} fp32", ms, 152)
+    h = torch.empty(f32.shape, dtype=torch.int16, device=dev)
+    hg = torch.empty_like(h)
+    for fmt in FORMATS16:
+        E.check(E.encode_shifted_async("D3Q19", fmt, "float", f32, h, NX, NY, NZ, 1.0))
+        for op in ("TRT", "MRT"):
+            ms = _time_steps(torch, lambda a, b, op=op, fmt=fmt: E.step_shifted_async("D3Q19", fmt, op, a, b, NX, NY, NZ, omega, 1.0),
+                             h, hg, 200, 10)
+            ref = fp32_ms if op == "TRT" else out[0]["ms_per_step"]
+            rec(f"D3Q19 {op} {fmt}", ms, 76, format=FORMAT_NOTE[fmt], speedup_vs_fp32=round(ref / ms, 3))
+    del h, hg, g
+    # FP64 (the reference drivers' precision) and the 27-velocity bandwidth case
+    f64 = f32.double()
+    g64 = torch.empty_like(f64)
+    ms = _time_steps(torch, lambda a, b: E.launch_step_gpu("D3Q19", "double", "BGK", a, b, NX, NY, NZ, omega),
+                     f64, g64, 200, 10)
+    rec("D3Q19 BGK fp64", ms, 304)
+    del f64, g64
+    f27 = torch.empty((27, NZ, NY, NX), dtype=torch.float32, device=dev)
+    rho = torch.ones((NZ, NY, NX), dtype=torch.float32, device=dev)
+    u = torch.zeros((3, NZ, NY, NX), dtype=torch.float32, device=dev)
+    E.check(E.init_equilibrium_async("D3Q27", "float", rho, u, f27, NX, NY, NZ))
+    g27 = torch.empty_like(f27)
+    ms = _time_steps(torch, lambda a, b: E.launch_step_gpu("D3Q27", "float", "BGK", a, b, NX, NY, NZ, omega),
+                     f27, g27, 200, 10)
+    rec("D3Q27 BGK fp32", ms, 216)
+    del f27, g27, rho, u
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_accuracy(torch, E, dev, steps=2000):
+    """Velocity rel-L2 after `steps` steps of the benchmark case against the FP64
+    run (the FP64 kernel is bit-identical to the reference CPU path)."""
+    omega = 1.0 / TAU
+    c = torch.tensor(C_D3Q19, dtype=torch.float64, device=dev)
+
+    def vel(f):
+        f = f.double()
+        return torch.einsum("qd,q...->d...", c, f) / f.sum(0)
+
+    res = {}
+    for op in ("TRT", "MRT"):
+        f32 = make_initial_state(torch, E, dev)
+        f64 = f32.double()  # same initial bits in both precisions
+        runs = {"fp64": [f64, torch.empty_like(f64)], "fp32": [f32, torch.empty_like(f32)]}
+        for fmt in FORMATS16:
+            h = torch.empty(f32.shape, dtype=torch.int16, device=dev)
+            E.check(E.encode_shifted_async("D3Q19", fmt, "float", f32, h, NX, NY, NZ, 1.0))
+            runs[fmt] = [h, torch.empty_like(h)]
+        for _ in range(steps):
+            for k, (a, b) in runs.items():
+                if k == "fp64":
+                    rc = E.launch_step_gpu("D3Q19", "double", op, a, b, NX, NY, NZ, omega)
+                elif k == "fp32":
+                    rc = E.launch_step_gpu("D3Q19", "float", op, a, b, NX, NY, NZ, omega)
+                else:
+                    rc = E.step_shifted_async("D3Q19", k, op, a, b, NX, NY, NZ, omega, 1.0)
+                E.check(rc)
+                runs[k] = [b, a]
+        u_ref = vel(runs["fp64"][0])
+        nref = torch.linalg.vector_norm(u_ref)
+        errs = {}
+        for k, (a, _) in runs.items():
+            if k == "fp64":
+                continue
+            if k == "fp32":
+                fk = a
+            else:
+                fk = torch.empty((19, NZ, NY, NX), dtype=torch.float64, device=dev)
+                E.check(E.decode_shifted_async("D3Q19", k, "double", a, fk, NX, NY, NZ, 1.0))
+            errs[k] = float(torch.linalg.vector_norm(vel(fk) - u_ref) / nref)
+            del fk
+        res[op] = {k: float(f"{v:.4g}") for k, v in errs.items()}
+        del runs, u_ref
+        torch.cuda.empty_cache()
+    return {"steps": steps, "quantity": "velocity relative L2 vs the FP64 run", "tau": TAU, "by_collision": res}
+
+
 def run_engine(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -189,10 +319,20 @@ def run_engine(args, rank, world, local_rank):
     cells = NX * NY * NZ
 
     f = make_initial_state(torch, E, dev)
-    g = torch.empty_like(f)
+    storage = args.storage
+    bytes_per_lu = BYTES_PER_LU if storage == "fp32" else BYTES_PER_LU // 2
+    if storage == "fp32":
+        def step(cur, nxt):
+            return E.launch_step_gpu("D3Q19", "float", "TRT", cur, nxt, NX, NY, NZ, omega)
+    else:
+        h = torch.empty(f.shape, dtype=torch.int16, device=dev)
+        E.check(E.encode_shifted_async("D3Q19", storage, "float", f, h, NX, NY, NZ, 1.0))
+        torch.cuda.synchronize()
+        f = h
 
-    def step(cur, nxt):
-        return E.launch_step_gpu("D3Q19", "float", "TRT", cur, nxt, NX, NY, NZ, omega)
+        def step(cur, nxt):
+            return E.step_shifted_async("D3Q19", storage, "TRT", cur, nxt, NX, NY, NZ, omega, 1.0)
+    g = torch.empty_like(f)
 
     for _ in range(args.warmup):
         E.check(step(f, g))
@@ -225,7 +365,7 @@ def run_engine(args, rank, world, local_rank):
         ms = float(t.item())
     ms_per_step = ms / args.steps
     value = cells * world * args.steps / (ms * 1e-3) / 1e6
-    achieved_gbs = BYTES_PER_LU * cells / (ms_per_step * 1e-3) / 1e9
+    achieved_gbs = bytes_per_lu * cells / (ms_per_step * 1e-3) / 1e9
 
     # end to end through the C ABI with host buffers
     e2e = None
@@ -256,22 +396,42 @@ def run_engine(args, rank, world, local_rank):
                "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
                "note": "pinned host field copied in, K steps via lbm_launch_step_gpu_d3q19_float_trt, "
                        "field copied back; copies amortised over K"}
+        if storage != "fp32":
+            e2e["note"] = e2e["note"].replace("lbm_launch_step_gpu_d3q19_float_trt", "lbm_step_shifted_async")
         del host
 
     if rank != 0:
         return None
     peak, peak_kind = measured_hbm_peak()
-    traffic = committed_traffic(f"d3q19_float_trt_{NX}")
+    traffic = committed_traffic(f"d3q19_float_trt_{NX}") if storage == "fp32" else None
+    variants = accuracy = fp16_store = None
+    if world == 1 and not args.no_variants and storage == "fp32":
+        variants = run_variants(torch, E, dev, f, peak, ms_per_step)
+        del f, g
+        torch.cuda.empty_cache()
+        accuracy = run_accuracy(torch, E, dev)
+        # the fastest 16-bit format meeting the 1e-3 velocity error bar for TRT
+        ok = [v for v in variants if v["variant"].startswith("D3Q19 TRT ") and v["variant"][10:] in FORMATS16
+              and accuracy["by_collision"]["TRT"][v["variant"][10:]] <= 1e-3]
+        if ok:
+            best = max(ok, key=lambda v: v["mlups"])
+            fmt = best["variant"][10:]
+            fp16_store = {"format": FORMAT_NOTE[fmt], "mlups": best["mlups"], "hbm_frac": best["hbm_frac"],
+                          "speedup_vs_fp32": best["speedup_vs_fp32"],
+                          "velocity_rel_l2_2000_steps": accuracy["by_collision"]["TRT"][fmt],
+                          "velocity_rel_l2_2000_steps_mrt": accuracy["by_collision"]["MRT"][fmt]}
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": config_dict(),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if storage == "fp32" else f"{storage} storage, f32 compute",
+        "data": "synthetic", "config": dict(config_dict(), storage=storage),
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved_gbs / peak, 4),
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": BYTES_PER_LU * cells},
+                     "algorithmic_bytes_per_launch": bytes_per_lu * cells},
         "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps,
+        "fp16_store": fp16_store, "variants": variants, "accuracy": accuracy,
     }
     return line
 

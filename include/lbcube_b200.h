@@ -29,6 +29,7 @@
  *   lattice   LBM_D2Q9 0, LBM_D3Q19 1, LBM_D3Q27 2, LBM_D2Q5 3, LBM_D3Q7 4
  *   precision LBM_FLOAT 0, LBM_DOUBLE 1
  *   collision LBM_BGK 0, LBM_TRT 1, LBM_MRT 2, LBM_RLBM 3
+ *   16-bit storage format LBM_F16S 2, LBM_BF16S 3, LBM_E3M12S 4, LBM_Q15S 5
  */
 #ifndef LBCUBE_B200_H
 #define LBCUBE_B200_H
@@ -43,6 +44,7 @@ extern "C" {
 enum { LBM_D2Q9 = 0, LBM_D3Q19 = 1, LBM_D3Q27 = 2, LBM_D2Q5 = 3, LBM_D3Q7 = 4 };
 enum { LBM_FLOAT = 0, LBM_DOUBLE = 1 };
 enum { LBM_BGK = 0, LBM_TRT = 1, LBM_MRT = 2, LBM_RLBM = 3 };
+enum { LBM_F16S = 2, LBM_BF16S = 3, LBM_E3M12S = 4, LBM_Q15S = 5 };
 
 /* ---------------------------------------------------------------------------
  * Fused pull collide-stream step, one symbol per instantiation. Each replaces
@@ -279,6 +281,40 @@ size_t lbm_stats_partials_bytes(int fluid_lattice, size_t x_extent, size_t y_ext
 int lbm_reactive_stats_async(int scalar_lattice, int precision, const void* current_a,
     const void* current_b, size_t x_extent, size_t y_extent, size_t z_extent, double k_react,
     double* partials, size_t partials_bytes, double* diagnostics, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Shifted 16-bit population storage (no reference counterpart). A population
+ * is stored as a 16-bit code of v_i = S (f_i / w_i - rho0), round to nearest,
+ * and read back as f_i = w_i (rho0 + v_i / S):
+ *   LBM_F16S   IEEE binary16, S = 4096
+ *   LBM_BF16S  bfloat16, S = 1
+ *   LBM_E3M12S sign | 3-bit exponent E | 12-bit mantissa m, S = 1, standing
+ *              for |v| = 2^(E-6) (1 + m/4096) - 2^-6: uniform 2^-18 grid near
+ *              zero, 13-bit relative precision above ~1/64, |v| < 3.98,
+ *              saturating
+ *   LBM_Q15S   16-bit two's-complement fixed point (code = round(v)),
+ *              S = 32768: uniform 2^-15 grid over |f/w - rho0| < 1,
+ *              saturating (NaN gives 0)
+ * Half the bytes of FP32 storage; collision in FP32 registers (BGK and TRT on
+ * the deviations v, MRT and RLBM on the decoded f with the FP32 operator
+ * code). Buffers are uint16 [Q, Z, Y, X]; x_extent must be a multiple of 4
+ * and buffers 8-byte aligned (else cudaErrorInvalidValue). rho0 is the
+ * reference density of the shift.
+ * ------------------------------------------------------------------------- */
+int lbm_step_shifted_async(int lattice, int format, int collision,
+    const void* current_populations, void* next_populations, size_t x_extent,
+    size_t y_extent, size_t z_extent, float omega, float rho0, void* stream);
+
+/* FP32/FP64 populations (`precision`) -> shifted 16-bit form, any lattice
+ * (fluid or scalar; scalars shift by w_i * rho0 with rho0 a reference
+ * concentration). */
+int lbm_encode_shifted_async(int lattice, int format, int precision, const void* populations,
+    void* shifted, size_t x_extent, size_t y_extent, size_t z_extent, float rho0, void* stream);
+
+/* Shifted 16-bit form -> FP32/FP64 populations. */
+int lbm_decode_shifted_async(int lattice, int format, int precision, const void* shifted,
+    void* populations, size_t x_extent, size_t y_extent, size_t z_extent, float rho0,
+    void* stream);
 
 /* Allocation-free form of lbm_reactive_stats_async. No counterpart in the
  * reference. For callers that cannot allocate device memory, e.g. a plugin or

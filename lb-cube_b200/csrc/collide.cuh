@@ -83,16 +83,44 @@ __device__ __forceinline__ Real feq(Real rho, const Real (&u)[L::D], Real usq) {
           Real(0.5) * inv_cs2 * usq);
 }
 
+// All Q equilibria of a cell, bit-identical to feq<L, i> for every i but
+// computed once per opposite pair: with c_o = -c_i, cu_o = -cu_i exactly, so
+// 3 cu_o = -(3 cu_i), 1 + 3 cu_o == 1 - 3 cu_i, and (4.5 cu_o) cu_o ==
+// (4.5 cu_i) cu_i, all without rounding differences.
+template <class L, class Real>
+__device__ __forceinline__ void equilibria(Real rho, const Real (&u)[L::D], Real usq,
+                                           Real (&eq)[L::Q]) {
+  const Real inv_cs2 = Real(1.0) / Real(L::cs2);
+  const Real a = Real(0.5) * inv_cs2 * inv_cs2;  // 4.5, exact
+  const Real b = Real(0.5) * inv_cs2;            // 1.5, exact
+  const Real tail = b * usq;
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr int o = L::opp[i];
+    constexpr double wd = L::w[i];
+    const Real wr = Real(wd) * rho;
+    if constexpr (i == o) {
+      eq[i] = wr * (Real(1.0) - tail);  // c_i = 0: 1 + 3*0 + (4.5*0)*0 == 1
+    } else if constexpr (i < o) {
+      const Real cu = c_dot<L, i>(u);
+      const Real p = inv_cs2 * cu;
+      const Real t2 = a * cu * cu;
+      eq[i] = wr * (Real(1.0) + p + t2 - tail);
+      eq[o] = wr * (Real(1.0) - p + t2 - tail);
+    }
+  });
+}
+
 // collide_bgk (lattice_physics.hpp:307-318).
 template <class L, class Real>
 __device__ __forceinline__ void collide_bgk(Real (&f)[L::Q], Real omega) {
-  Real rho, u[L::D];
+  Real rho, u[L::D], eq[L::Q];
   macro_state<L>(f, rho, u);
   const Real usq = u_dot_u<L>(u);
+  equilibria<L>(rho, u, usq, eq);
   static_for<L::Q>([&](auto I) {
     constexpr int i = LB_I(I);
-    const Real eq = feq<L, i>(rho, u, usq);
-    f[i] = f[i] + omega * (eq - f[i]);
+    f[i] = f[i] + omega * (eq[i] - f[i]);
   });
 }
 
@@ -107,22 +135,35 @@ __host__ __device__ inline Real trt_omega_minus(Real omega_plus) {
 
 // collide_trt (lattice_physics.hpp:366-398) after compute_macro_state
 // (lattice_core.hpp:96-100). omega_minus is precomputed once per launch.
+// Evaluated once per opposite pair (i, o): the reference's even parts for i
+// and o are the same values, its odd parts exact negatives, so
+//   post_i = (f_i - A) - B,  post_o = (f_o - A) + B
+// with A = w+ (even - eq_even), B = w- (odd_i - eq_odd_i) reproduces both of
+// its results bit for bit. The rest population has odd part +0.
 template <class L, class Real>
 __device__ __forceinline__ void collide_trt(Real (&f)[L::Q], Real omega_plus, Real omega_minus) {
-  Real rho, u[L::D], eq[L::Q], post[L::Q];
+  Real rho, u[L::D], eq[L::Q];
   macro_state<L>(f, rho, u);
   const Real usq = u_dot_u<L>(u);
-  static_for<L::Q>([&](auto I) { eq[LB_I(I)] = feq<L, LB_I(I)>(rho, u, usq); });
+  equilibria<L>(rho, u, usq, eq);
   static_for<L::Q>([&](auto I) {
     constexpr int i = LB_I(I);
     constexpr int o = L::opp[i];
-    const Real even = Real{0.5} * (f[i] + f[o]);
-    const Real eq_even = Real{0.5} * (eq[i] + eq[o]);
-    const Real odd = Real{0.5} * (f[i] - f[o]);
-    const Real eq_odd = Real{0.5} * (eq[i] - eq[o]);
-    post[i] = f[i] - omega_plus * (even - eq_even) - omega_minus * (odd - eq_odd);
+    if constexpr (i == o) {
+      f[i] = f[i] - omega_plus * (f[i] - eq[i]);
+    } else if constexpr (i < o) {
+      const Real even = Real{0.5} * (f[i] + f[o]);
+      const Real eq_even = Real{0.5} * (eq[i] + eq[o]);
+      const Real odd = Real{0.5} * (f[i] - f[o]);
+      const Real eq_odd = Real{0.5} * (eq[i] - eq[o]);
+      const Real A = omega_plus * (even - eq_even);
+      const Real B = omega_minus * (odd - eq_odd);
+      const Real fi = f[i] - A - B;
+      const Real fo = f[o] - A + B;
+      f[i] = fi;
+      f[o] = fo;
+    }
   });
-  static_for<L::Q>([&](auto I) { f[LB_I(I)] = post[LB_I(I)]; });
 }
 
 // ----------------------------------------------------------------------------
@@ -478,7 +519,7 @@ __device__ __forceinline__ void collide_rlbm(Real (&f)[L::Q], Real omega) {
   Real rho, u[L::D], fe[L::Q];
   macro_state<L>(f, rho, u);
   const Real usq = u_dot_u<L>(u);
-  static_for<L::Q>([&](auto I) { fe[LB_I(I)] = feq<L, LB_I(I)>(rho, u, usq); });
+  equilibria<L>(rho, u, usq, fe);
   const Real hp = Real{9} / Real{2};
   const Real cs2 = Real(L::cs2);
   // Pi_neq = sum_i (f_i - feq_i) c_i c_i, accumulated from zero in ascending i.
@@ -488,6 +529,7 @@ __device__ __forceinline__ void collide_rlbm(Real (&f)[L::Q], Real omega) {
     const Real fn = f[i] - fe[i];
     constexpr int ix = L::c[i][0], iy = L::c[i][1], iz = L::c[i][2];
     const Real cx = Real(ix), cy = Real(iy), cz = Real(iz);
+    (void)cz;
     pxx += fn * cx * cx;
     pyy += fn * cy * cy;
     pxy += fn * cx * cy;
@@ -557,6 +599,7 @@ __device__ __forceinline__ void collide_rlbm(Real (&f)[L::Q], Real omega) {
       const Real h_xzz = cx * cz * cz - cs2 * cx;
       const Real h_yzz = cy * cz * cz - cs2 * cy;
       const Real h_xyz = cx * cy * cz;
+      (void)h_xxx, (void)h_yyy, (void)h_zzz, (void)h_xyz;  // unused by the D3Q19 branch
       Real third;
       if constexpr (L::id == kD3Q19) {
         third = Real{3} * (h_xxy + h_yzz) * (a_xxy + a_yzz) + (h_xxy - h_yzz) * (a_xxy - a_yzz) +

@@ -10,6 +10,7 @@
 // most one element for c_x != 0, which the L1/L2 sector reuse absorbs).
 #include "collide.cuh"
 #include "common.cuh"
+#include "stream_vec.cuh"
 #include "../../include/lbcube_b200.h"
 
 namespace lbcube {
@@ -45,6 +46,16 @@ __global__ void __launch_bounds__(kThreads)
   });
 }
 
+// Cells per thread of the vectorised kernel: 2 FP32 cells (8-byte words) or 1
+// FP64 cell per thread measured fastest on B200 at 256^3 (D3Q19 TRT FP32: 0.99
+// of the copy bandwidth at V = 2 against 0.80 at V = 4 and 0.76 at V = 1;
+// FP64 best at V = 1). Operators whose register footprint would spill use the
+// one-cell kernel.
+template <class Real>
+constexpr int kVecCells = sizeof(Real) == 4 ? 2 : 1;
+template <class L, class Real, int CT>
+constexpr bool kUseVec = !(L::Q == 27 && sizeof(Real) == 8 && (CT == kMRT || CT == kRLBM));
+
 template <class L, class Real, int CT>
 cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, size_t nz,
                               Real omega, unsigned bx, unsigned by, unsigned bz,
@@ -58,8 +69,15 @@ cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, 
   const Span writes[1] = {{nxt, bytes}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
-  fluid_step_kernel<L, Real, CT><<<grid_dims(g), kThreads, 0, stream>>>(cur, nxt, g, omega,
-                                                                         omega_minus);
+  using S = NativeStorage<Real, kVecCells<Real>>;
+  if (kUseVec<L, Real, CT> && vec_eligible<S>(g, cur, nxt)) {
+    const VecGrid vg = make_vec_grid(g, S::V);
+    fluid_step_vec_kernel<L, S, CT><<<vec_grid_dims(vg), kThreads, 0, stream>>>(
+        cur, nxt, vg, omega, omega_minus, typename S::Params{});
+  } else {
+    fluid_step_kernel<L, Real, CT><<<grid_dims(g), kThreads, 0, stream>>>(cur, nxt, g, omega,
+                                                                           omega_minus);
+  }
   return cudaGetLastError();
 }
 

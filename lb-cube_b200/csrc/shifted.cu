@@ -1,0 +1,198 @@
+// Shifted 16-bit population storage (FP16, BF16, E3M12 or Q15) with FP32
+// collision.
+//
+// An extension with no reference counterpart. Populations are stored as codes
+// of v_i = S (f_i / w_i - rho0) in 16 bits (collide_dev.cuh), halving the bytes
+// per lattice update (D3Q19: 76 B instead of 152 B). BGK and TRT collide on
+// the deviations v directly (DevStorage); MRT and RLBM decode to f, run the
+// reference operator and re-encode (ShiftedStorage). Rounding to 16 bits is to
+// nearest. Encode/decode kernels convert between FP32/FP64 populations and the
+// 16-bit form.
+#include <algorithm>
+#include <type_traits>
+
+#include "collide.cuh"
+#include "common.cuh"
+#include "stream_vec.cuh"
+#include "../../include/lbcube_b200.h"
+
+namespace lbcube {
+
+// Cells per thread of the 16-bit kernels (8-byte words).
+constexpr int kShiftedCells = 4;
+
+// BGK and TRT collide on the stored deviations; MRT and RLBM decode to f.
+template <int FMT, int CT>
+using ShiftedPolicy = std::conditional_t<CT == kBGK || CT == kTRT, DevStorage<FMT, kShiftedCells>,
+                                         ShiftedStorage<FMT, kShiftedCells>>;
+
+template <class L, int FMT, int CT>
+cudaError_t launch_shifted_step(const void* cur, void* nxt, size_t nx, size_t ny, size_t nz,
+                                float omega, float rho0, cudaStream_t stream) {
+  using S = ShiftedPolicy<FMT, CT>;
+  Grid g;
+  cudaError_t err = validate_domain(cur == nullptr || nxt == nullptr, 1, 1, 1, L::D, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  const size_t bytes = (size_t)L::Q * g.plane * sizeof(typename S::elem);
+  const Span reads[1] = {{cur, bytes}};
+  const Span writes[1] = {{nxt, bytes}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  if (!vec_eligible<S>(g, cur, nxt)) return cudaErrorInvalidValue;  // nx % V, word alignment
+  const float omega_minus = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
+  const VecGrid vg = make_vec_grid(g, S::V);
+  fluid_step_vec_kernel<L, S, CT><<<vec_grid_dims(vg), kThreads, 0, stream>>>(
+      static_cast<const unsigned short*>(cur), static_cast<unsigned short*>(nxt), vg, omega,
+      omega_minus, typename S::Params{rho0});
+  return cudaGetLastError();
+}
+
+template <class L, int FMT>
+cudaError_t shifted_by_collision(int collision, const void* cur, void* nxt, size_t nx, size_t ny,
+                                 size_t nz, float omega, float rho0, cudaStream_t s) {
+  switch (collision) {
+    case kBGK: return launch_shifted_step<L, FMT, kBGK>(cur, nxt, nx, ny, nz, omega, rho0, s);
+    case kTRT: return launch_shifted_step<L, FMT, kTRT>(cur, nxt, nx, ny, nz, omega, rho0, s);
+    case kMRT: return launch_shifted_step<L, FMT, kMRT>(cur, nxt, nx, ny, nz, omega, rho0, s);
+    case kRLBM: return launch_shifted_step<L, FMT, kRLBM>(cur, nxt, nx, ny, nz, omega, rho0, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int FMT>
+cudaError_t shifted_by_lattice(int lattice, int collision, const void* cur, void* nxt, size_t nx,
+                               size_t ny, size_t nz, float omega, float rho0, cudaStream_t s) {
+  switch (lattice) {
+    case kD2Q9: return shifted_by_collision<D2Q9, FMT>(collision, cur, nxt, nx, ny, nz, omega, rho0, s);
+    case kD3Q19: return shifted_by_collision<D3Q19, FMT>(collision, cur, nxt, nx, ny, nz, omega, rho0, s);
+    case kD3Q27: return shifted_by_collision<D3Q27, FMT>(collision, cur, nxt, nx, ny, nz, omega, rho0, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// ---- conversions --------------------------------------------------------------
+// One thread per (population, cell) element; plane i uses weight w_i.
+template <class L, int FMT, class Real, bool ENCODE>
+__global__ void __launch_bounds__(256)
+    convert_kernel(const void* __restrict__ in, void* __restrict__ out, long long plane,
+                   float rho0) {
+  using S = ShiftedStorage<FMT>;
+  const long long n = plane * L::Q;
+  const typename S::Params p{rho0};
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / plane);
+    static_for<L::Q>([&](auto I) {
+      constexpr int q = LB_I(I);
+      if (q != i) return;
+      if constexpr (ENCODE) {
+        const float f = (float)static_cast<const Real*>(in)[e];
+        static_cast<unsigned short*>(out)[e] = S::template encode<L, q>(f, p);
+      } else {
+        const float f = S::template decode<L, q>(static_cast<const unsigned short*>(in)[e], p);
+        static_cast<Real*>(out)[e] = (Real)f;
+      }
+    });
+  }
+}
+
+template <class L, int FMT, bool ENCODE>
+cudaError_t launch_convert(int precision, const void* in, void* out, size_t nx, size_t ny,
+                           size_t nz, float rho0, cudaStream_t s) {
+  Grid g;
+  cudaError_t err = validate_domain(in == nullptr || out == nullptr, 1, 1, 1, L::D, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return cudaErrorInvalidValue;
+  const size_t wide = (size_t)L::Q * g.plane * (precision == LBM_FLOAT ? 4 : 8);
+  const size_t narrow = (size_t)L::Q * g.plane * 2;
+  const Span reads[1] = {{in, ENCODE ? wide : narrow}};
+  const Span writes[1] = {{out, ENCODE ? narrow : wide}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  const long long n = (long long)L::Q * g.plane;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 32);
+  if (precision == LBM_FLOAT)
+    convert_kernel<L, FMT, float, ENCODE><<<blocks, 256, 0, s>>>(in, out, g.plane, rho0);
+  else
+    convert_kernel<L, FMT, double, ENCODE><<<blocks, 256, 0, s>>>(in, out, g.plane, rho0);
+  return cudaGetLastError();
+}
+
+template <int FMT, bool ENCODE>
+cudaError_t convert_by_lattice(int lattice, int precision, const void* in, void* out, size_t nx,
+                               size_t ny, size_t nz, float rho0, cudaStream_t s) {
+  switch (lattice) {
+    case kD2Q9: return launch_convert<D2Q9, FMT, ENCODE>(precision, in, out, nx, ny, nz, rho0, s);
+    case kD3Q19: return launch_convert<D3Q19, FMT, ENCODE>(precision, in, out, nx, ny, nz, rho0, s);
+    case kD3Q27: return launch_convert<D3Q27, FMT, ENCODE>(precision, in, out, nx, ny, nz, rho0, s);
+    case kD2Q5: return launch_convert<D2Q5, FMT, ENCODE>(precision, in, out, nx, ny, nz, rho0, s);
+    case kD3Q7: return launch_convert<D3Q7, FMT, ENCODE>(precision, in, out, nx, ny, nz, rho0, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace lbcube
+
+using namespace lbcube;
+
+extern "C" int lbm_step_shifted_async(int lattice, int format, int collision,
+                                      const void* current_populations, void* next_populations,
+                                      size_t x_extent, size_t y_extent, size_t z_extent,
+                                      float omega, float rho0, void* stream) {
+  const cudaStream_t s = as_stream(stream);
+  if (format == LBM_F16S)
+    return (int)shifted_by_lattice<kF16S>(lattice, collision, current_populations,
+                                          next_populations, x_extent, y_extent, z_extent, omega,
+                                          rho0, s);
+  if (format == LBM_BF16S)
+    return (int)shifted_by_lattice<kBF16S>(lattice, collision, current_populations,
+                                           next_populations, x_extent, y_extent, z_extent, omega,
+                                           rho0, s);
+  if (format == LBM_E3M12S)
+    return (int)shifted_by_lattice<kE3M12S>(lattice, collision, current_populations,
+                                            next_populations, x_extent, y_extent, z_extent, omega,
+                                            rho0, s);
+  if (format == LBM_Q15S)
+    return (int)shifted_by_lattice<kQ15S>(lattice, collision, current_populations,
+                                          next_populations, x_extent, y_extent, z_extent, omega,
+                                          rho0, s);
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int lbm_encode_shifted_async(int lattice, int format, int precision,
+                                        const void* populations, void* shifted, size_t x_extent,
+                                        size_t y_extent, size_t z_extent, float rho0,
+                                        void* stream) {
+  const cudaStream_t s = as_stream(stream);
+  if (format == LBM_F16S)
+    return (int)convert_by_lattice<kF16S, true>(lattice, precision, populations, shifted,
+                                                x_extent, y_extent, z_extent, rho0, s);
+  if (format == LBM_BF16S)
+    return (int)convert_by_lattice<kBF16S, true>(lattice, precision, populations, shifted,
+                                                 x_extent, y_extent, z_extent, rho0, s);
+  if (format == LBM_E3M12S)
+    return (int)convert_by_lattice<kE3M12S, true>(lattice, precision, populations, shifted,
+                                                  x_extent, y_extent, z_extent, rho0, s);
+  if (format == LBM_Q15S)
+    return (int)convert_by_lattice<kQ15S, true>(lattice, precision, populations, shifted,
+                                                x_extent, y_extent, z_extent, rho0, s);
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int lbm_decode_shifted_async(int lattice, int format, int precision,
+                                        const void* shifted, void* populations, size_t x_extent,
+                                        size_t y_extent, size_t z_extent, float rho0,
+                                        void* stream) {
+  const cudaStream_t s = as_stream(stream);
+  if (format == LBM_F16S)
+    return (int)convert_by_lattice<kF16S, false>(lattice, precision, shifted, populations,
+                                                 x_extent, y_extent, z_extent, rho0, s);
+  if (format == LBM_BF16S)
+    return (int)convert_by_lattice<kBF16S, false>(lattice, precision, shifted, populations,
+                                                  x_extent, y_extent, z_extent, rho0, s);
+  if (format == LBM_E3M12S)
+    return (int)convert_by_lattice<kE3M12S, false>(lattice, precision, shifted, populations,
+                                                   x_extent, y_extent, z_extent, rho0, s);
+  if (format == LBM_Q15S)
+    return (int)convert_by_lattice<kQ15S, false>(lattice, precision, shifted, populations,
+                                                 x_extent, y_extent, z_extent, rho0, s);
+  return (int)cudaErrorInvalidValue;
+}

@@ -26,6 +26,7 @@ D_OF = {"D2Q9": 2, "D3Q19": 3, "D3Q27": 3, "D2Q5": 2, "D3Q7": 3}
 SCALAR_OF = {"D2Q9": "D2Q5", "D3Q19": "D3Q7", "D3Q27": "D3Q7"}
 COLLISIONS = {"BGK": 0, "TRT": 1, "MRT": 2, "RLBM": 3}
 REALS = {"float": 0, "double": 1}
+FORMATS = {"f16s": 2, "bf16s": 3, "e3m12s": 4, "q15s": 5}  # shifted 16-bit population storage
 
 # cudaError_t values returned by the launchers
 cudaSuccess = 0
@@ -90,6 +91,10 @@ def _declare(lib):
         "lbm_reactive_stats_async": [C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
         "lbm_reactive_stats_finalize_async": [C.c_int, C.c_int, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
         "lbm_init_equilibrium_async": [C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, _vp],
+        "lbm_step_shifted_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, C.c_float,
+                                   C.c_float, _vp],
+        "lbm_encode_shifted_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, C.c_float, _vp],
+        "lbm_decode_shifted_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, C.c_float, _vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -234,6 +239,28 @@ def reactive_stats_finalize_async(fluid_lattice, real, nx, ny, nz, k_react, part
 def init_equilibrium_async(lattice, real, rho, u, populations, nx, ny, nz, stream=None) -> int:
     return load().lbm_init_equilibrium_async(LATTICES[lattice], REALS[real_name(real)], _ptr(rho),
                                              _ptr(u), _ptr(populations), nx, ny, nz, _stream(stream))
+
+
+def step_shifted_async(lattice, fmt, collision, cur, nxt, nx, ny, nz, omega, rho0=1.0,
+                       stream=None) -> int:
+    """One collide-stream step on shifted 16-bit populations (fmt in FORMATS)."""
+    return load().lbm_step_shifted_async(LATTICES[lattice], FORMATS[fmt], COLLISIONS[collision],
+                                         _ptr(cur), _ptr(nxt), nx, ny, nz, float(omega),
+                                         float(rho0), _stream(stream))
+
+
+def encode_shifted_async(lattice, fmt, real, populations, shifted, nx, ny, nz, rho0=1.0,
+                         stream=None) -> int:
+    return load().lbm_encode_shifted_async(LATTICES[lattice], FORMATS[fmt], REALS[real_name(real)],
+                                           _ptr(populations), _ptr(shifted), nx, ny, nz,
+                                           float(rho0), _stream(stream))
+
+
+def decode_shifted_async(lattice, fmt, real, shifted, populations, nx, ny, nz, rho0=1.0,
+                         stream=None) -> int:
+    return load().lbm_decode_shifted_async(LATTICES[lattice], FORMATS[fmt], REALS[real_name(real)],
+                                           _ptr(shifted), _ptr(populations), nx, ny, nz,
+                                           float(rho0), _stream(stream))
 
 
 def declared_symbols(header: str = HEADER):

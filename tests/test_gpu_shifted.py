@@ -1,0 +1,154 @@
+"""GPU: shifted 16-bit population storage (FP16 / BF16 / E3M12 / Q15) with FP32 collision.
+
+* encode/decode round trip: the error of every population is within half a
+  16-bit ulp of its stored deviation (f/w - rho0);
+* one 16-bit step against encode(FP32 step(decode(h))): the two differ only in
+  FP32 rounding before the final 16-bit rounding (BGK/TRT collide on the
+  deviations; the FP32 path works on f ~ w and carries a few FP32 ulps of 1 of
+  absolute error in f/w after cancelling rho0, more for D3Q27's 1/216 weights
+  and 27-term MRT sums), so every value is within one 16-bit step plus 2e-6
+  of the other and at least 95 % of the codes agree;
+* Q15 covers |f/w - rho0| < 1 only, so its round trip uses a state inside
+  that range (|u| ~ 0.03) and out-of-range values saturate;
+* 2000 steps of the D3Q19 256^3 Taylor-Green + noise case (tau 0.55): the
+  velocity rel-L2 against the FP64 run (the FP64 kernel is bit-identical to
+  the reference CPU path, tests/test_gpu_parity.py). Bars: E3M12 <= 1e-3 for
+  TRT and MRT; IEEE FP16 <= 1e-3 for MRT and <= 3e-3 for TRT (1.9e-3 measured:
+  TRT's odd modes relax at omega- ~ 0.18 at tau 0.55 and keep the rounding
+  noise); Q15 <= 1e-3 for TRT and <= 3e-3 for MRT (2.6e-4 and 1.4e-3
+  measured); BF16 <= 0.15 (8-bit significand: ~8e-2 measured, not usable at
+  this tolerance).
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import _util as U
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FMTS = ("f16s", "bf16s", "e3m12s", "q15s")
+ULP = {"f16s": 2.0 ** -10, "bf16s": 2.0 ** -7, "e3m12s": 2.0 ** -12, "q15s": 0.0}  # relative spacing
+ABS_FLOOR = {"f16s": 0.0, "bf16s": 0.0, "e3m12s": 2.0 ** -18, "q15s": 2.0 ** -16}  # half the uniform grid
+BARS = {("e3m12s", "TRT"): 1e-3, ("e3m12s", "MRT"): 1e-3, ("f16s", "MRT"): 1e-3,
+        ("f16s", "TRT"): 3e-3, ("bf16s", "TRT"): 0.15, ("bf16s", "MRT"): 0.15,
+        ("q15s", "TRT"): 1e-3, ("q15s", "MRT"): 3e-3}
+
+
+def _w(lat):
+    import lbcube  # noqa: F401
+
+    return torch.tensor({"D2Q9": [4 / 9] + [1 / 9] * 4 + [1 / 36] * 4,
+                         "D3Q19": [1 / 3] + [1 / 18] * 6 + [1 / 36] * 12,
+                         "D3Q27": [8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8}[lat],
+                        dtype=torch.float64)
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("lat", ["D2Q9", "D3Q19", "D3Q27"])
+def test_encode_decode_round_trip(engine, dev, fmt, lat):
+    nx, ny, nz = (64, 12, 1) if lat == "D2Q9" else (32, 6, 5)
+    u_amp = 0.03 if fmt == "q15s" else 0.08
+    f = torch.from_numpy(U.random_state(lat, nx, ny, nz, np.float32, seed=5, u_amp=u_amp)).to(dev)
+    h = torch.empty(f.shape, dtype=torch.int16, device=dev)
+    back = torch.empty_like(f)
+    engine.check(engine.encode_shifted_async(lat, fmt, "float", f, h, nx, ny, nz, 1.0))
+    engine.check(engine.decode_shifted_async(lat, fmt, "float", h, back, nx, ny, nz, 1.0))
+    torch.cuda.synchronize()
+    w = _w(lat).to(dev).view(-1, 1)
+    dev_in = f.double() / w - 1.0
+    err = (back.double() - f.double()).abs() / w
+    # half an ulp of the stored deviation (x2 for the binade), the E3M12 uniform-grid floor, FP32 arithmetic
+    bound = 0.5 * ULP[fmt] * dev_in.abs() * 2 + ABS_FLOOR[fmt] + 1e-7
+    assert bool((err <= bound).all()), float((err - bound).max())
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("lat", ["D2Q9", "D3Q19", "D3Q27"])
+@pytest.mark.parametrize("op", ["BGK", "TRT", "MRT", "RLBM"])
+def test_shifted_step_is_rounded_fp32_step(engine, dev, fmt, lat, op):
+    nx, ny, nz = (64, 12, 1) if lat == "D2Q9" else (32, 6, 5)
+    f = torch.from_numpy(U.random_state(lat, nx, ny, nz, np.float32, seed=6)).to(dev)
+    h0 = torch.empty(f.shape, dtype=torch.int16, device=dev)
+    engine.check(engine.encode_shifted_async(lat, fmt, "float", f, h0, nx, ny, nz, 1.0))
+    f0 = torch.empty_like(f)
+    engine.check(engine.decode_shifted_async(lat, fmt, "float", h0, f0, nx, ny, nz, 1.0))
+    f1 = torch.empty_like(f)
+    engine.check(engine.launch_step_gpu(lat, "float", op, f0, f1, nx, ny, nz, 1 / 0.6))
+    want = torch.empty_like(h0)
+    engine.check(engine.encode_shifted_async(lat, fmt, "float", f1, want, nx, ny, nz, 1.0))
+    h1 = torch.empty_like(h0)
+    engine.check(engine.step_shifted_async(lat, fmt, op, h0, h1, nx, ny, nz, 1 / 0.6, 1.0))
+    got_f, want_f = torch.empty_like(f), torch.empty_like(f)
+    engine.check(engine.decode_shifted_async(lat, fmt, "float", h1, got_f, nx, ny, nz, 1.0))
+    engine.check(engine.decode_shifted_async(lat, fmt, "float", want, want_f, nx, ny, nz, 1.0))
+    torch.cuda.synchronize()
+    w = _w(lat).to(dev).view(-1, 1)
+    dv = (got_f.double() - want_f.double()).abs() / w
+    step = ULP[fmt] * (want_f.double() / w - 1.0).abs() * 2 + 2 * ABS_FLOOR[fmt] + 2e-6
+    assert bool((dv <= step).all()), float((dv - step).max())
+    assert float((h1 == want).double().mean()) >= 0.95
+
+
+def test_shifted_rejects_unaligned_extent(engine, dev):
+    h = torch.zeros((19, 4, 4, 30), dtype=torch.int16, device=dev)
+    g = torch.empty_like(h)
+    assert engine.step_shifted_async("D3Q19", "f16s", "TRT", h, g, 30, 4, 4, 1.5) == engine.cudaErrorInvalidValue
+
+
+def _velocity(f, lat):
+    c = torch.tensor(_CV[lat], dtype=f.dtype, device=f.device)
+    rho = f.sum(0)
+    u = torch.einsum("qd,q...->d...", c, f) / rho
+    return rho, u
+
+
+_CV = {"D3Q19": [[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
+                 [1, 1, 0], [-1, 1, 0], [1, -1, 0], [-1, -1, 0], [1, 0, 1], [-1, 0, 1], [1, 0, -1],
+                 [-1, 0, -1], [0, 1, 1], [0, -1, 1], [0, 1, -1], [0, -1, -1]]}
+
+
+def tgv_noise_init(engine, dev, n, dtype):
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(20261203)
+    k = 2 * math.pi / n
+    ax = torch.arange(n, device=dev, dtype=torch.float64) * k
+    z, y, x = torch.meshgrid(ax, ax, ax, indexing="ij")
+    u = torch.stack([0.05 * torch.sin(x) * torch.cos(y) * torch.cos(z),
+                     -0.05 * torch.cos(x) * torch.sin(y) * torch.cos(z), torch.zeros_like(x)])
+    u += 1e-3 * torch.randn(u.shape, generator=gen, device=dev, dtype=torch.float64)
+    rho = torch.ones((n, n, n), device=dev, dtype=torch.float64)
+    f = torch.empty((19, n, n, n), device=dev, dtype=dtype)
+    real = "double" if dtype == torch.float64 else "float"
+    engine.check(engine.init_equilibrium_async("D3Q19", real, rho.to(dtype), u.to(dtype).contiguous(), f, n, n, n))
+    return f
+
+
+@pytest.mark.parametrize("fmt", FMTS)
+@pytest.mark.parametrize("op", ["TRT", "MRT"])
+def test_shifted_2000_steps_vs_fp64(engine, dev, fmt, op):
+    n, steps, tau = 256, 2000, 0.55
+    f64 = tgv_noise_init(engine, dev, n, torch.float64)
+    g64 = torch.empty_like(f64)
+    f32 = f64.float()
+    h = torch.empty(f32.shape, dtype=torch.int16, device=dev)
+    engine.check(engine.encode_shifted_async("D3Q19", fmt, "float", f32, h, n, n, n, 1.0))
+    del f32
+    hg = torch.empty_like(h)
+    for _ in range(steps):
+        engine.check(engine.launch_step_gpu("D3Q19", "double", op, f64, g64, n, n, n, 1 / tau))
+        f64, g64 = g64, f64
+        engine.check(engine.step_shifted_async("D3Q19", fmt, op, h, hg, n, n, n, 1 / tau, 1.0))
+        h, hg = hg, h
+    del g64, hg
+    fh = torch.empty((19, n, n, n), dtype=torch.float64, device=dev)
+    engine.check(engine.decode_shifted_async("D3Q19", fmt, "double", h, fh, n, n, n, 1.0))
+    torch.cuda.synchronize()
+    _, u_ref = _velocity(f64, "D3Q19")
+    _, u_h = _velocity(fh, "D3Q19")
+    err = float(torch.linalg.vector_norm(u_h - u_ref) / torch.linalg.vector_norm(u_ref))
+    print(f"{fmt} {op} velocity rel-L2 after {steps} steps: {err:.3e}")
+    assert err <= BARS[(fmt, op)]
