@@ -316,6 +316,35 @@ int lbm_decode_shifted_async(int lattice, int format, int precision, const void*
     void* populations, size_t x_extent, size_t y_extent, size_t z_extent, float rho0,
     void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Discrete reverse-mode adjoint (no reference counterpart). Objective:
+ * J = sum_x 0.5 rho |u|^2 of the state after `steps` collide-stream steps
+ * (BGK or TRT) started from f^0 = f_eq(rho0, u0). The gradient driver runs
+ * the forward pass storing a checkpoint every `checkpoint_interval` steps,
+ * then for each segment, last first, recomputes the segment's states from
+ * its checkpoint and runs the adjoint steps back through it. Outputs (device):
+ * objective_and_dtau[0] = J, [1] = dJ/dtau (FP64, deterministic), and
+ * grad_u0 = dJ/du0 [D, Z, Y, X] in the population precision. The workspace
+ * (checkpoints, one segment, two adjoint fields, FP64 slots) is caller-owned
+ * device memory of lbm_ke_gradient_workspace_bytes bytes; rho0, u0 and
+ * grad_u0 must not overlap it. Cost: about 2 forward runs + 1 adjoint run.
+ * ------------------------------------------------------------------------- */
+size_t lbm_ke_gradient_workspace_bytes(int lattice, int precision, size_t x_extent,
+    size_t y_extent, size_t z_extent, int steps, int checkpoint_interval);
+
+int lbm_ke_gradient_async(int lattice, int precision, int collision, const void* rho0,
+    const void* u0, size_t x_extent, size_t y_extent, size_t z_extent, double tau, int steps,
+    int checkpoint_interval, void* workspace, size_t workspace_bytes, double* objective_and_dtau,
+    void* grad_u0, void* stream);
+
+/* One adjoint step: lambda = J_step(f^n)^T lambda_next, where f^n is the state
+ * the forward step started from (pull formulation; the adjoint scatters). If
+ * dtau_slots is non-null, each block adds lambda_next . dC/dtau over its cells
+ * to its own FP64 slot (lbm_stats_partials_bytes / 5 slots). */
+int lbm_adjoint_step_async(int lattice, int precision, int collision, const void* populations,
+    const void* lambda_next, void* lambda, size_t x_extent, size_t y_extent, size_t z_extent,
+    double tau, double* dtau_slots, void* stream);
+
 /* Allocation-free form of lbm_reactive_stats_async. No counterpart in the
  * reference. For callers that cannot allocate device memory, e.g. a plugin or
  * FFI binding inside an application that owns every device allocation and

@@ -95,6 +95,9 @@ def _declare(lib):
                                    C.c_float, _vp],
         "lbm_encode_shifted_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, C.c_float, _vp],
         "lbm_decode_shifted_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, C.c_float, _vp],
+        "lbm_ke_gradient_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, C.c_int, C.c_int,
+                                  _vp, _sz, _vp, _vp, _vp],
+        "lbm_adjoint_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -102,6 +105,8 @@ def _declare(lib):
         fn.argtypes = args
     lib.lbm_stats_partials_bytes.restype = C.c_size_t
     lib.lbm_stats_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
+    lib.lbm_ke_gradient_workspace_bytes.restype = C.c_size_t
+    lib.lbm_ke_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, _sz, _sz, _sz, C.c_int, C.c_int]
 
 
 def _ptr(buf):
@@ -261,6 +266,28 @@ def decode_shifted_async(lattice, fmt, real, shifted, populations, nx, ny, nz, r
     return load().lbm_decode_shifted_async(LATTICES[lattice], FORMATS[fmt], REALS[real_name(real)],
                                            _ptr(shifted), _ptr(populations), nx, ny, nz,
                                            float(rho0), _stream(stream))
+
+
+def ke_gradient_workspace_bytes(lattice, real, nx, ny, nz, steps, interval) -> int:
+    return load().lbm_ke_gradient_workspace_bytes(LATTICES[lattice], REALS[real_name(real)], nx, ny,
+                                                  nz, int(steps), int(interval))
+
+
+def ke_gradient_async(lattice, real, collision, rho0, u0, nx, ny, nz, tau, steps, interval,
+                      workspace, workspace_bytes, out2, grad_u0, stream=None) -> int:
+    """Checkpointed adjoint of J = sum 0.5 rho |u|^2 after `steps` steps from
+    f_eq(rho0, u0): out2 = [J, dJ/dtau] (device FP64), grad_u0 = dJ/du0."""
+    return load().lbm_ke_gradient_async(LATTICES[lattice], REALS[real_name(real)], COLLISIONS[collision],
+                                        _ptr(rho0), _ptr(u0), nx, ny, nz, float(tau), int(steps),
+                                        int(interval), _ptr(workspace), int(workspace_bytes),
+                                        _ptr(out2), _ptr(grad_u0), _stream(stream))
+
+
+def adjoint_step_async(lattice, real, collision, populations, lambda_next, lam, nx, ny, nz, tau,
+                       dtau_slots=None, stream=None) -> int:
+    return load().lbm_adjoint_step_async(LATTICES[lattice], REALS[real_name(real)], COLLISIONS[collision],
+                                         _ptr(populations), _ptr(lambda_next), _ptr(lam), nx, ny, nz,
+                                         float(tau), _ptr(dtau_slots), _stream(stream))
 
 
 def declared_symbols(header: str = HEADER):
