@@ -306,6 +306,71 @@ def run_accuracy(torch, E, dev, steps=2000):
     return {"steps": steps, "quantity": "velocity relative L2 vs the FP64 run", "tau": TAU, "by_collision": res}
 
 
+def solenoidal_field(torch, dev, n, amp, k_peak, seed):
+    """Seeded random solenoidal velocity: curl of a random-phase vector potential
+    whose spectrum peaks at |k| = k_peak, rescaled to max |u| = amp."""
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    k1 = torch.fft.fftfreq(n, d=1.0 / n, device=dev)
+    kz, ky, kx = torch.meshgrid(k1, k1, k1, indexing="ij")
+    kk = torch.sqrt(kx * kx + ky * ky + kz * kz)
+    env = (kk / k_peak) ** 2 * torch.exp(-(kk / k_peak) ** 2)
+    A = [torch.fft.fftn(torch.randn((n, n, n), generator=gen, device=dev, dtype=torch.float64)) * env
+         for _ in range(3)]
+    Ax, Ay, Az = A
+    uh = [1j * (ky * Az - kz * Ay), 1j * (kz * Ax - kx * Az), 1j * (kx * Ay - ky * Ax)]
+    u = torch.stack([torch.fft.ifftn(c).real for c in uh])
+    return (u * (amp / u.abs().max())).contiguous()
+
+
+def run_adjoint_cost(torch, E, dev, n=128, steps=2000, interval=100, tau=0.56):
+    """Adjoint cost: full gradient (forward with checkpoints, segment
+    recomputation, adjoint sweep) over one forward run, D3Q19 BGK FP32."""
+    u0 = solenoidal_field(torch, dev, n, 0.03, 4.0, SEED).float()
+    rho0 = torch.ones((n, n, n), dtype=torch.float32, device=dev)
+    f = torch.empty((19, n, n, n), dtype=torch.float32, device=dev)
+    g = torch.empty_like(f)
+    omega = 1.0 / tau
+
+    def forward():
+        E.check(E.init_equilibrium_async("D3Q19", "float", rho0, u0, f, n, n, n))
+        a, b = f, g
+        for _ in range(steps):
+            E.check(E.launch_step_gpu("D3Q19", "float", "BGK", a, b, n, n, n, omega))
+            a, b = b, a
+
+    nbytes = E.ke_gradient_workspace_bytes("D3Q19", "float", n, n, n, steps, interval)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    out = torch.zeros(2, dtype=torch.float64, device=dev)
+    grad = torch.empty_like(u0)
+
+    def gradient():
+        E.check(E.ke_gradient_async("D3Q19", "float", "BGK", rho0, u0, n, n, n, tau, steps, interval,
+                                    ws, nbytes, out, grad))
+
+    def timed(fn):
+        fn()  # warm-up
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        fn()
+        t1.record()
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1)
+
+    fwd_ms = timed(forward)
+    grad_ms = timed(gradient)
+    res = {"config": f"D3Q19 BGK FP32 {n}^3, tau {tau}, {steps} steps, solenoidal u0 (amplitude 0.03, "
+                     f"spectrum peak |k| = 4), objective final total kinetic energy, checkpoint every {interval}",
+           "forward_ms": round(fwd_ms, 2), "gradient_ms": round(grad_ms, 2),
+           "cost_ratio": round(grad_ms / fwd_ms, 3), "objective": float(out[0]), "dJ_dtau": float(out[1]),
+           "workspace_gb": round(nbytes / 1e9, 2)}
+    del ws, f, g, grad
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_engine(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -404,12 +469,13 @@ def run_engine(args, rank, world, local_rank):
         return None
     peak, peak_kind = measured_hbm_peak()
     traffic = committed_traffic(f"d3q19_float_trt_{NX}") if storage == "fp32" else None
-    variants = accuracy = fp16_store = None
+    variants = accuracy = fp16_store = adjoint = None
     if world == 1 and not args.no_variants and storage == "fp32":
         variants = run_variants(torch, E, dev, f, peak, ms_per_step)
         del f, g
         torch.cuda.empty_cache()
         accuracy = run_accuracy(torch, E, dev)
+        adjoint = run_adjoint_cost(torch, E, dev)
         # the fastest 16-bit format meeting the 1e-3 velocity error bar for TRT
         ok = [v for v in variants if v["variant"].startswith("D3Q19 TRT ") and v["variant"][10:] in FORMATS16
               and accuracy["by_collision"]["TRT"][v["variant"][10:]] <= 1e-3]
@@ -431,7 +497,7 @@ def run_engine(args, rank, world, local_rank):
                      "traffic": traffic, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_per_lu * cells},
         "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps,
-        "fp16_store": fp16_store, "variants": variants, "accuracy": accuracy,
+        "fp16_store": fp16_store, "adjoint": adjoint, "variants": variants, "accuracy": accuracy,
     }
     return line
 

@@ -71,39 +71,48 @@ __global__ void __launch_bounds__(kThreads)
     Real eq[L::Q];
     equilibria<L>(rho, u, usq, eq);
     const Real om = Real(ap.omega), omm = Real(ap.omega_minus);
-    // weights of f_eq in C, and the tau-derivative of the step
+    // weights of f_eq in C, and the tau-derivative of the step (per cell in the
+    // population precision, accumulated over cells in FP64)
     Real Lam[L::Q];
+    Real dt1 = Real(0), dt2 = Real(0);
     static_for<L::Q>([&](auto I) {
       constexpr int i = LB_I(I);
       constexpr int o = L::opp[i];
       if constexpr (CT == kBGK) {
         Lam[i] = om * lv[i];
-        dtau += (double)lv[i] * (double)(eq[i] - gv[i]) * ap.domega_dtau;
+        dt1 += lv[i] * (eq[i] - gv[i]);
       } else {
         const Real lp = Real(0.5) * (lv[i] + lv[o]), lm = Real(0.5) * (lv[i] - lv[o]);
         Lam[i] = om * lp + omm * lm;
-        const Real dp = Real(0.5) * ((gv[i] + gv[o]) - (eq[i] + eq[o]));  // g+ - f_eq+
-        const Real dm = Real(0.5) * ((gv[i] - gv[o]) - (eq[i] - eq[o]));  // g- - f_eq-
-        dtau -= (double)lv[i] * ((double)dp * ap.domega_dtau + (double)dm * ap.domega_minus_dtau);
+        dt1 += lv[i] * (Real(0.5) * ((gv[i] + gv[o]) - (eq[i] + eq[o])));  // g+ - f_eq+
+        dt2 += lv[i] * (Real(0.5) * ((gv[i] - gv[o]) - (eq[i] - eq[o])));  // g- - f_eq-
       }
     });
-    Real A = Real(0), B[L::D];
+    if constexpr (CT == kBGK) {
+      dtau = (double)dt1 * ap.domega_dtau;
+    } else {
+      dtau = -((double)dt1 * ap.domega_dtau + (double)dt2 * ap.domega_minus_dtau);
+    }
+    // A = sum_i w_i Lam_i (1 + 1.5 u.u) - 4.5 sum_i w_i Lam_i (c_i.u)^2
+    // B = sum_i w_i Lam_i (3 + 9 c_i.u) c_i - 3 u sum_i w_i Lam_i
+    Real W = Real(0), Aq = Real(0), B[L::D];
     static_for<L::D>([&](auto D) { B[LB_I(D)] = Real(0); });
-    const Real h15 = Real(1.5) * usq;
     static_for<L::Q>([&](auto I) {
       constexpr int i = LB_I(I);
       constexpr double wd = L::w[i];
       const Real cu = c_dot<L, i>(u);
       const Real wl = Real(wd) * Lam[i];
-      A += wl * (Real(1) - Real(4.5) * cu * cu + h15);
+      W += wl;
+      Aq += wl * cu * cu;
       const Real s = wl * (Real(3) + Real(9) * cu);
       static_for<L::D>([&](auto D) {
         constexpr int c = L::c[i][LB_I(D)];
         if constexpr (c > 0) B[LB_I(D)] += s;
         if constexpr (c < 0) B[LB_I(D)] -= s;
-        B[LB_I(D)] -= Real(3) * wl * u[LB_I(D)];
       });
     });
+    const Real A = W * (Real(1) + Real(1.5) * usq) - Real(4.5) * Aq;
+    static_for<L::D>([&](auto D) { B[LB_I(D)] -= Real(3) * W * u[LB_I(D)]; });
     const Real a = CT == kBGK ? Real(1) - om : Real(1) - Real(0.5) * (om + omm);
     const Real b = CT == kBGK ? Real(0) : Real(0.5) * (omm - om);
     // scatter mu_j to lambda^n(x - c_j, j)
@@ -278,11 +287,21 @@ cudaError_t ke_gradient(int collision, const Real* rho0, const Real* u0, const G
   err = (cudaError_t)lbm_init_equilibrium_async(L::id, sizeof(Real) == 4 ? LBM_FLOAT : LBM_DOUBLE,
                                                 rho0, u0, ckpt(0), g.nx, g.ny, g.nz, s);
   if (err != cudaSuccess) return err;
+  // Intermediate states ping-pong in two segment slots, except in the last
+  // segment, whose states go straight to their segment slots so the backward
+  // sweep need not recompute it.
+  const long long nseg = (steps + interval - 1) / interval;
+  const int last0 = (int)((nseg - 1) * interval);
   const Real* cur = ckpt(0);
   for (int n = 0; n < steps; ++n) {
-    const bool at_ckpt = (n + 1) % interval == 0 || n + 1 == steps;
-    Real* nxt = at_ckpt ? ckpt((n + 1 + interval - 1) / interval) : seg(n % interval % 2);
-    if ((n + 1) % interval == 0) nxt = ckpt((n + 1) / interval);
+    Real* nxt;
+    if (n + 1 == steps || (n + 1) % interval == 0) {
+      nxt = ckpt((n + 1 + interval - 1) / interval);
+    } else if (n + 1 > last0) {
+      nxt = seg(n + 1 - last0);
+    } else {
+      nxt = seg(n % 2);
+    }
     err = forward_step<Real>(L::id, collision, cur, nxt, g, omega, s);
     if (err != cudaSuccess) return err;
     cur = nxt;
@@ -293,13 +312,13 @@ cudaError_t ke_gradient(int collision, const Real* rho0, const Real* u0, const G
   if ((err = cudaMemsetAsync(dtau_slots, 0, lay.slots * sizeof(double), s)) != cudaSuccess) return err;
   const AdjointParams ap = make_params<Real>(collision, tau);
   // backward over segments [k*interval, min((k+1)*interval, steps))
-  const long long nseg = (steps + interval - 1) / interval;
   for (long long k = nseg - 1; k >= 0; --k) {
     const int n0 = (int)(k * interval);
     const int n1 = (int)std::min<long long>((long long)steps, (k + 1) * interval);
     // recompute f^{n0+1} .. f^{n1-1} into the segment store from checkpoint k
+    // (the last segment's states are already there)
     const Real* src = ckpt(k);
-    for (int n = n0 + 1; n < n1; ++n) {
+    for (int n = n0 + 1; n < n1 && k < nseg - 1; ++n) {
       err = forward_step<Real>(L::id, collision, src, seg(n - n0), g, omega, s);
       if (err != cudaSuccess) return err;
       src = seg(n - n0);
