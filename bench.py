@@ -59,6 +59,9 @@ def parse():
                     help="population storage of the timed run (16-bit ones are shifted)")
     ap.add_argument("--size", type=int, default=256,
                     help="cube edge; smaller sizes are for profiling captures only")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the adjoint cost measurement (D3Q19 BGK FP32, --size cube, --steps "
+                         "steps, checkpoint every min(100, steps)) and print it; for profiling captures")
     a = ap.parse_args()
     global NX, NY, NZ
     NX = NY = NZ = a.size
@@ -582,6 +585,17 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
+        return
+    if args.adjoint_only:
+        import torch
+
+        import lbcube as E
+
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        E.load()
+        res = run_adjoint_cost(torch, E, dev, n=args.size, steps=args.steps, interval=min(100, args.steps))
+        print(json.dumps({"adjoint": res}), flush=True)
         return
     if world > 1:
         import datetime

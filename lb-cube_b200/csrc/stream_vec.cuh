@@ -311,4 +311,7 @@ inline dim3 vec_grid_dims(const VecGrid& v) {
   return dim3((unsigned)(v.xblocks * v.yblocks), (unsigned)v.g.nz, 1);
 }
 
+// Threads per block of the vectorised kernel: exactly tx * ty (<= kThreads).
+inline unsigned vec_block_threads(const VecGrid& v) { return (unsigned)(v.tx * v.ty); }
+
 }  // namespace lbcube

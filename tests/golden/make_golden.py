@@ -22,6 +22,37 @@ SIZES = {"D2Q9": (7, 5, 1), "D3Q19": (6, 5, 4), "D3Q27": (5, 4, 3)}
 OMEGA, OMEGA_C, K, STEPS = 1 / 0.6, 1 / 0.8, 0.07, 3
 
 
+def tgv_c1(n=64, u0=0.05):
+    """The C1 initial field: D3Q19 Taylor-Green u = u0 (sin kx cos ky cos kz,
+    -cos kx sin ky cos kz, 0), rho = 1, k = 2 pi / n. Built from 1-D tables of
+    glibc sin/cos (math module) and IEEE products, so every machine running
+    this image reproduces the same bits."""
+    import math
+
+    k = 2 * math.pi / n
+    s1 = np.array([math.sin(k * i) for i in range(n)])
+    c1 = np.array([math.cos(k * i) for i in range(n)])
+    ux = u0 * s1[None, None, :] * c1[None, :, None] * c1[:, None, None]
+    uy = -u0 * c1[None, None, :] * s1[None, :, None] * c1[:, None, None]
+    u = np.stack([ux, uy, np.zeros_like(ux)]).reshape(3, -1)
+    return O.init_equilibrium("D3Q19", np.ones(n ** 3), u, n, n, n)
+
+
+def c1_fingerprint(steps=1000, every=100, tau=0.6):
+    """C1 run on the reference CPU path: SHA-256 of the final populations and
+    the (mass, KE, max |u|) series every `every` steps."""
+    import hashlib
+
+    f = tgv_c1()
+    series = [O.fluid_diagnostics(f, "D3Q19", 64, 64, 64).tolist()]
+    for _ in range(steps // every):
+        f = O.step(f, "D3Q19", "BGK", 64, 64, 64, 1 / tau, steps=every, lib=O.REF)
+        series.append(O.fluid_diagnostics(f, "D3Q19", 64, 64, 64).tolist())
+    return {"workload": "D3Q19 BGK FP64 64^3 Taylor-Green u0 0.05 rho 1, tau 0.6",
+            "steps": steps, "sha256_final": hashlib.sha256(f.tobytes()).hexdigest(),
+            "diagnostics_every_100": series}
+
+
 def main():
     if not O.REF.available:
         raise SystemExit("reference build oracle/_ref/libref.so missing: run make -C oracle ref")
@@ -42,6 +73,11 @@ def main():
             out[f"{lat}_{dn}_stats"] = O.reactive_stats(a, b, sl, nx, ny, nz, K, lib=O.REF)
     np.savez_compressed(os.path.join(HERE, "reference_steps.npz"), **out)
     print(f"wrote {len(out)} arrays")
+    import json
+
+    with open(os.path.join(HERE, "c1_tgv64_fp64_bgk.json"), "w") as fh:
+        json.dump(c1_fingerprint(), fh, indent=1)
+    print("wrote the C1 fingerprint")
 
 
 if __name__ == "__main__":

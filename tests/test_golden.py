@@ -55,3 +55,49 @@ def test_engine_matches_reference_fixtures(engine, dev, lat, dn):
     for got, key in ((ta, "react_a"), (tb, "react_b")):
         want = G[f"{lat}_{dn}_{key}"]
         assert np.linalg.norm(got.cpu().numpy() - want) / np.linalg.norm(want) <= tol
+
+
+C1 = os.path.join(os.path.dirname(__file__), "golden", "c1_tgv64_fp64_bgk.json")
+
+
+def _c1_initial():
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+
+    return make_golden.tgv_c1()
+
+
+def test_oracle_c1_first_100_steps():
+    """C1 (D3Q19 BGK FP64 64^3 Taylor-Green): the oracle's (mass, KE, max|u|)
+    after 0 and 100 steps equal the reference build's, bit for bit."""
+    import json
+
+    want = json.load(open(C1))["diagnostics_every_100"]
+    f = _c1_initial()
+    assert O.fluid_diagnostics(f, "D3Q19", 64, 64, 64).tolist() == want[0]
+    f = O.step(f, "D3Q19", "BGK", 64, 64, 64, 1 / 0.6, steps=100)
+    assert O.fluid_diagnostics(f, "D3Q19", 64, 64, 64).tolist() == want[1]
+
+
+@pytest.mark.gpu
+def test_engine_c1_fingerprint(engine, dev):
+    """C1 on the engine: 1000 steps through the drop-in launcher; every 100
+    steps the diagnostics equal the reference build's and the final
+    populations have the reference's SHA-256."""
+    import hashlib
+    import json
+
+    import torch
+
+    ref = json.load(open(C1))
+    cur = torch.from_numpy(_c1_initial()).to(dev)
+    nxt = torch.empty_like(cur)
+    for block in range(1, ref["steps"] // 100 + 1):
+        for _ in range(100):
+            engine.check(engine.launch_step_gpu("D3Q19", "double", "BGK", cur, nxt, 64, 64, 64, 1 / 0.6))
+            cur, nxt = nxt, cur
+        f = cur.cpu().numpy()
+        assert O.fluid_diagnostics(f, "D3Q19", 64, 64, 64).tolist() == ref["diagnostics_every_100"][block], block
+    assert hashlib.sha256(f.tobytes()).hexdigest() == ref["sha256_final"]
