@@ -374,6 +374,36 @@ int lbm_reactive_stats_finalize_async(int fluid_lattice, int precision, size_t x
 int lbm_init_equilibrium_async(int lattice, int precision, const void* rho, const void* u,
     void* populations, size_t x_extent, size_t y_extent, size_t z_extent, void* stream);
 
+/* ---- fluid diagnostics and blow-up guard ---------------------------------
+ * Replace the host loops of lbm::log_diagnostics (lattice_io.hpp:182-234) and
+ * of compute_max_velocity with its crash test (turbulent_tgv_3d.cpp:150-173,
+ * :302-316), which need the whole field on the host (main.cpp:595-606).
+ * diagnostics (device, 5 doubles):
+ *   [0] total mass           sum of rho          (FP64 sum of Real terms)
+ *   [1] total kinetic energy sum of 0.5 rho |u|^2 (FP64 sum of Real terms)
+ *   [2] max |u| over the cells whose |u| is not NaN (log_diagnostics' max)
+ *   [3] number of cells whose |u| is not finite
+ *   [4] 1.0 if [3] > 0 or [2] > speed_limit (the driver's crash test), else 0.0
+ * Per-cell rho, |u|^2, 0.5 rho |u|^2 and |u| are computed in the population
+ * precision as the reference computes them; the reference's Real accumulators
+ * become FP64 ones added in a fixed order (run-to-run identical).
+ * partials: device scratch of lbm_diagnostics_partials_bytes() bytes. */
+size_t lbm_diagnostics_partials_bytes(int lattice, size_t x_extent, size_t y_extent,
+    size_t z_extent);
+int lbm_fluid_diagnostics_async(int lattice, int precision, const void* populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, double speed_limit, double* partials,
+    size_t partials_bytes, double* diagnostics, void* stream);
+/* One collide-stream step (as lbm_step_async) that also reduces the
+ * diagnostics of the state it writes, at no extra memory traffic: the
+ * populations a thread writes in the pull scheme are the next buffer's
+ * populations of its own cells. Same five values as lbm_fluid_diagnostics_async
+ * on next_populations (the FP64 sums may differ in the last bits: the cells are
+ * grouped into other blocks). */
+int lbm_step_diagnostics_async(int lattice, int precision, int collision,
+    const void* current_populations, void* next_populations, size_t x_extent, size_t y_extent,
+    size_t z_extent, double omega, double speed_limit, double* partials, size_t partials_bytes,
+    double* diagnostics, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -33,6 +33,7 @@ UNITS = {
     "adr.cu": ["--fmad=false"],
     "stats.cu": ["--fmad=false"],
     "init.cu": ["--fmad=false"],
+    "diag.cu": ["--fmad=false"],
 }
 
 

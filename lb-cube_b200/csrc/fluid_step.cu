@@ -10,23 +10,21 @@
 // most one element for c_x != 0, which the L1/L2 sector reuse absorbs).
 #include "collide.cuh"
 #include "common.cuh"
+#include "diag.cuh"
 #include "stream_vec.cuh"
 #include "../../include/lbcube_b200.h"
 
 namespace lbcube {
 
 template <class L, class Real, int CT>
-__global__ void __launch_bounds__(kThreads)
-    fluid_step_kernel(const Real* __restrict__ cur, Real* __restrict__ nxt, Grid g, Real omega,
-                      Real omega_minus) {
-  int x, y, z;
-  if (!cell_of(g, x, y, z)) return;
+__device__ __forceinline__ void step_cell(const Real* __restrict__ cur, Real* __restrict__ nxt,
+                                          const Grid& g, int x, int y, int z, Real omega,
+                                          Real omega_minus, Real (&f)[L::Q]) {
   const int xm = x == 0 ? g.nx - 1 : x - 1, xp = x == g.nx - 1 ? 0 : x + 1;
   const int ym = y == 0 ? g.ny - 1 : y - 1, yp = y == g.ny - 1 ? 0 : y + 1;
   const int zm = z == 0 ? g.nz - 1 : z - 1, zp = z == g.nz - 1 ? 0 : z + 1;
   const size_t plane = (size_t)g.plane;
 
-  Real f[L::Q];
   static_for<L::Q>([&](auto I) {
     constexpr int i = LB_I(I);
     constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
@@ -44,6 +42,28 @@ __global__ void __launch_bounds__(kThreads)
     constexpr int i = LB_I(I);
     nxt[plane * i + cell] = f[i];
   });
+}
+
+// DIAG: also reduce the diagnostics of the written state over the block
+// (diag.cuh), as in fluid_step_vec_kernel.
+template <class L, class Real, int CT, bool DIAG = false>
+__global__ void __launch_bounds__(kThreads)
+    fluid_step_kernel(const Real* __restrict__ cur, Real* __restrict__ nxt, Grid g, Real omega,
+                      Real omega_minus, double* __restrict__ partials = nullptr) {
+  int x, y, z;
+  const bool active = cell_of(g, x, y, z);
+  Real f[L::Q];
+  if constexpr (DIAG) {
+    DiagAcc acc;
+    if (active) {
+      step_cell<L, Real, CT>(cur, nxt, g, x, y, z, omega, omega_minus, f);
+      diag_cell<L>(f, acc);
+    }
+    diag_block_to(acc, partials + block_linear() * kDiagPartials);
+  } else {
+    if (!active) return;
+    step_cell<L, Real, CT>(cur, nxt, g, x, y, z, omega, omega_minus, f);
+  }
 }
 
 // Cells per thread of the vectorised kernel: 2 FP32 cells (8-byte words) or 1
@@ -79,6 +99,71 @@ cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, 
                                                                            omega_minus);
   }
   return cudaGetLastError();
+}
+
+// One step plus the diagnostics of the state it writes (diag.cuh): the
+// kernel writes one partial per block, the finalize pass reduces them.
+template <class L, class Real, int CT>
+cudaError_t launch_fluid_step_diag(const Real* cur, Real* nxt, size_t nx, size_t ny, size_t nz,
+                                   Real omega, double speed_limit, double* partials,
+                                   size_t pbytes, double* out, cudaStream_t stream) {
+  Grid g;
+  cudaError_t err = validate_domain(cur == nullptr || nxt == nullptr || partials == nullptr ||
+                                        out == nullptr,
+                                    1, 1, 1, L::D, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  const size_t need = (size_t)g.blocks() * kDiagPartials * sizeof(double);
+  if (pbytes < need) return cudaErrorInvalidValue;
+  const size_t bytes = (size_t)L::Q * (size_t)g.plane * sizeof(Real);
+  const Span reads[1] = {{cur, bytes}};
+  const Span writes[3] = {{nxt, bytes}, {partials, need}, {out, kDiagOut * sizeof(double)}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
+  using S = NativeStorage<Real, kVecCells<Real>>;
+  long long count;
+  if (kUseVec<L, Real, CT> && vec_eligible<S>(g, cur, nxt)) {
+    const VecGrid vg = make_vec_grid(g, S::V);
+    const dim3 grid = vec_grid_dims(vg);
+    count = (long long)grid.x * grid.y;  // <= g.blocks(): a block covers >= kThreads cells
+    fluid_step_vec_kernel<L, S, CT, true><<<grid, vec_block_threads(vg), 0, stream>>>(
+        cur, nxt, vg, omega, omega_minus, typename S::Params{}, partials);
+  } else {
+    count = g.blocks();
+    fluid_step_kernel<L, Real, CT, true><<<grid_dims(g), kThreads, 0, stream>>>(
+        cur, nxt, g, omega, omega_minus, partials);
+  }
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  return launch_diag_finalize(partials, count, speed_limit, out, stream);
+}
+
+template <class Real, int CT>
+cudaError_t diag_dispatch_lattice(int lattice, const void* cur, void* nxt, size_t nx, size_t ny,
+                                  size_t nz, double omega, double speed_limit, double* partials,
+                                  size_t pbytes, double* out, cudaStream_t s) {
+  const Real* c = static_cast<const Real*>(cur);
+  Real* n = static_cast<Real*>(nxt);
+  const Real w = Real(omega);
+  switch (lattice) {
+    case kD2Q9: return launch_fluid_step_diag<D2Q9, Real, CT>(c, n, nx, ny, nz, w, speed_limit, partials, pbytes, out, s);
+    case kD3Q19: return launch_fluid_step_diag<D3Q19, Real, CT>(c, n, nx, ny, nz, w, speed_limit, partials, pbytes, out, s);
+    case kD3Q27: return launch_fluid_step_diag<D3Q27, Real, CT>(c, n, nx, ny, nz, w, speed_limit, partials, pbytes, out, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <class Real>
+cudaError_t diag_dispatch_collision(int lattice, int collision, const void* cur, void* nxt,
+                                    size_t nx, size_t ny, size_t nz, double omega,
+                                    double speed_limit, double* partials, size_t pbytes,
+                                    double* out, cudaStream_t s) {
+  switch (collision) {
+    case kBGK: return diag_dispatch_lattice<Real, kBGK>(lattice, cur, nxt, nx, ny, nz, omega, speed_limit, partials, pbytes, out, s);
+    case kTRT: return diag_dispatch_lattice<Real, kTRT>(lattice, cur, nxt, nx, ny, nz, omega, speed_limit, partials, pbytes, out, s);
+    case kMRT: return diag_dispatch_lattice<Real, kMRT>(lattice, cur, nxt, nx, ny, nz, omega, speed_limit, partials, pbytes, out, s);
+    case kRLBM: return diag_dispatch_lattice<Real, kRLBM>(lattice, cur, nxt, nx, ny, nz, omega, speed_limit, partials, pbytes, out, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template <class Real, int CT>
@@ -145,5 +230,26 @@ extern "C" int lbm_step_async(int lattice, int precision, int collision,
     return (int)dispatch_collision<double>(lattice, collision, current_populations,
                                            next_populations, x_extent, y_extent, z_extent, omega,
                                            s);
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int lbm_step_diagnostics_async(int lattice, int precision, int collision,
+                                          const void* current_populations,
+                                          void* next_populations, size_t x_extent,
+                                          size_t y_extent, size_t z_extent, double omega,
+                                          double speed_limit, double* partials,
+                                          size_t partials_bytes, double* diagnostics,
+                                          void* stream) {
+  const cudaStream_t s = as_stream(stream);
+  if (precision == LBM_FLOAT)
+    return (int)diag_dispatch_collision<float>(lattice, collision, current_populations,
+                                               next_populations, x_extent, y_extent, z_extent,
+                                               omega, speed_limit, partials, partials_bytes,
+                                               diagnostics, s);
+  if (precision == LBM_DOUBLE)
+    return (int)diag_dispatch_collision<double>(lattice, collision, current_populations,
+                                                next_populations, x_extent, y_extent, z_extent,
+                                                omega, speed_limit, partials, partials_bytes,
+                                                diagnostics, s);
   return (int)cudaErrorInvalidValue;
 }

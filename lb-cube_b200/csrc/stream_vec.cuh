@@ -24,10 +24,12 @@
 #include <cuda_fp16.h>
 
 #include <cstring>
+#include <type_traits>
 
 #include "collide.cuh"
 #include "collide_dev.cuh"
 #include "common.cuh"
+#include "diag.cuh"
 
 namespace lbcube {
 
@@ -278,12 +280,16 @@ __device__ __forceinline__ void store_vec(typename S::elem* __restrict__ nxt, co
   });
 }
 
-template <class L, class S, int CT>
+// DIAG: also reduce the diagnostics of the new state (diag.cuh) over the
+// block into partials[block_linear() * kDiagPartials ..]. In the pull scheme
+// the populations a thread writes are exactly the next buffer's populations of
+// its own cells, so this costs no memory traffic. Native storage only.
+template <class L, class S, int CT, bool DIAG = false>
 __global__ void __launch_bounds__(kThreads)
     fluid_step_vec_kernel(const typename S::elem* __restrict__ cur,
                           typename S::elem* __restrict__ nxt, VecGrid vg,
                           typename S::compute omega, typename S::compute omega_minus,
-                          typename S::Params p) {
+                          typename S::Params p, double* __restrict__ partials = nullptr) {
   using R = typename S::compute;
   constexpr int V = S::V;
   const Grid& g = vg.g;
@@ -295,10 +301,23 @@ __global__ void __launch_bounds__(kThreads)
   const bool active = x0 < g.nx && y < g.ny;
   R f[V][L::Q];
   gather_vec<L, S>(cur, g, x0, y < g.ny ? y : 0, z, active, p, f);
-  if (!active) return;
+  if constexpr (DIAG) {
+    static_assert(std::is_same_v<typename S::elem, R>, "diagnostics need native storage");
+    DiagAcc acc;
+    if (active) {
 #pragma unroll
-  for (int j = 0; j < V; ++j) S::template collide_cell<L, CT>(f[j], omega, omega_minus, p);
-  store_vec<L, S>(nxt, g, x0, y, z, p, f);
+      for (int j = 0; j < V; ++j) S::template collide_cell<L, CT>(f[j], omega, omega_minus, p);
+      store_vec<L, S>(nxt, g, x0, y, z, p, f);
+#pragma unroll
+      for (int j = 0; j < V; ++j) diag_cell<L>(f[j], acc);
+    }
+    diag_block_to(acc, partials + block_linear() * kDiagPartials);
+  } else {
+    if (!active) return;
+#pragma unroll
+    for (int j = 0; j < V; ++j) S::template collide_cell<L, CT>(f[j], omega, omega_minus, p);
+    store_vec<L, S>(nxt, g, x0, y, z, p, f);
+  }
 }
 
 template <class S>

@@ -14,6 +14,7 @@ raises, there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -98,6 +99,9 @@ def _declare(lib):
         "lbm_ke_gradient_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, C.c_int, C.c_int,
                                   _vp, _sz, _vp, _vp, _vp],
         "lbm_adjoint_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp],
+        "lbm_fluid_diagnostics_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
+        "lbm_step_diagnostics_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, d, _vp, _sz,
+                                       _vp, _vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -105,6 +109,8 @@ def _declare(lib):
         fn.argtypes = args
     lib.lbm_stats_partials_bytes.restype = C.c_size_t
     lib.lbm_stats_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
+    lib.lbm_diagnostics_partials_bytes.restype = C.c_size_t
+    lib.lbm_diagnostics_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
     lib.lbm_ke_gradient_workspace_bytes.restype = C.c_size_t
     lib.lbm_ke_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, _sz, _sz, _sz, C.c_int, C.c_int]
 
@@ -288,6 +294,29 @@ def adjoint_step_async(lattice, real, collision, populations, lambda_next, lam, 
     return load().lbm_adjoint_step_async(LATTICES[lattice], REALS[real_name(real)], COLLISIONS[collision],
                                          _ptr(populations), _ptr(lambda_next), _ptr(lam), nx, ny, nz,
                                          float(tau), _ptr(dtau_slots), _stream(stream))
+
+
+def diagnostics_partials_bytes(lattice, nx, ny, nz) -> int:
+    return load().lbm_diagnostics_partials_bytes(LATTICES[lattice], nx, ny, nz)
+
+
+def fluid_diagnostics_async(lattice, real, populations, nx, ny, nz, partials, partials_bytes,
+                            diagnostics, speed_limit=math.inf, stream=None) -> int:
+    """diagnostics (device FP64[5]) = total mass, total kinetic energy, max |u|,
+    non-finite cells, blow-up flag (non-finite |u| or max |u| > speed_limit)."""
+    return load().lbm_fluid_diagnostics_async(LATTICES[lattice], REALS[real_name(real)],
+                                              _ptr(populations), nx, ny, nz, float(speed_limit),
+                                              _ptr(partials), int(partials_bytes),
+                                              _ptr(diagnostics), _stream(stream))
+
+
+def step_diagnostics_async(lattice, real, collision, cur, nxt, nx, ny, nz, omega, partials,
+                           partials_bytes, diagnostics, speed_limit=math.inf, stream=None) -> int:
+    """One collide-stream step plus the diagnostics of the state it writes."""
+    return load().lbm_step_diagnostics_async(LATTICES[lattice], REALS[real_name(real)],
+                                             COLLISIONS[collision], _ptr(cur), _ptr(nxt), nx, ny, nz,
+                                             float(omega), float(speed_limit), _ptr(partials),
+                                             int(partials_bytes), _ptr(diagnostics), _stream(stream))
 
 
 def declared_symbols(header: str = HEADER):

@@ -234,6 +234,16 @@ int oracle_fluid_diagnostics(int lattice, int precision, const void* f, size_t n
   return -1;
 }
 
+int oracle_fluid_diagnostics64(int lattice, int precision, const void* f, size_t nx, size_t ny,
+                               size_t nz, double speed_limit, double* out) {
+  if (!fluid_ok(lattice)) return -1;
+  const lattice_t* L = &LATTICES[lattice];
+  if (L->D == 2) nz = 1;
+  if (precision == 0) return fluid_diagnostics64_f32(L, f, nx, ny, nz, speed_limit, out);
+  if (precision == 1) return fluid_diagnostics64_f64(L, f, nx, ny, nz, speed_limit, out);
+  return -1;
+}
+
 int oracle_macro_fields(int lattice, int precision, const void* f, size_t nx, size_t ny,
                         size_t nz, double* rho, double* u) {
   if (lattice < 0 || lattice > 4) return -1;

@@ -59,6 +59,14 @@ int oracle_reactive_stats(int scalar_lattice, int precision, const void* a, cons
 int oracle_fluid_diagnostics(int lattice, int precision, const void* f, size_t nx, size_t ny,
                              size_t nz, double* out);
 
+/* The engine's device diagnostics restated: log_diagnostics' per-cell terms in
+ * the population precision, summed in double; out[5] = total mass, total
+ * kinetic energy, max |u| (NaN speeds skipped, as std::max skips them),
+ * number of non-finite |u|, crash flag (non-finite |u| or max |u| >
+ * speed_limit, turbulent_tgv_3d.cpp:302-316). */
+int oracle_fluid_diagnostics64(int lattice, int precision, const void* f, size_t nx, size_t ny,
+                               size_t nz, double speed_limit, double* out);
+
 /* Per-cell density and velocity (compute_macro_state, lattice_physics.hpp:227-249)
  * widened to double: rho[N], u[D*N] (component-major). */
 int oracle_macro_fields(int lattice, int precision, const void* f, size_t nx, size_t ny,

@@ -812,6 +812,36 @@ static int F(fluid_diagnostics)(const lattice_t* L, const void* vf, size_t nx, s
   return 0;
 }
 
+/* The engine's diagnostics: the per-cell terms of log_diagnostics in REAL,
+ * accumulated in double, plus the non-finite count and the crash flag of
+ * turbulent_tgv_3d.cpp:150-173, :302-316 (compute_max_velocity returns +inf
+ * on a non-finite speed; the driver stops on !isfinite(max) || max > limit). */
+static int F(fluid_diagnostics64)(const lattice_t* L, const void* vf, size_t nx, size_t ny,
+                                  size_t nz, double speed_limit, double* out) {
+  const REAL* fl = (const REAL*)vf;
+  REAL f[27], rho, u[3];
+  double mass = 0.0, ke = 0.0, umax = 0.0, nonfinite = 0.0;
+  for (size_t z = 0; z < nz; ++z)
+    for (size_t y = 0; y < ny; ++y)
+      for (size_t x = 0; x < nx; ++x) {
+        for (int i = 0; i < L->Q; ++i) f[i] = fl[pidx(i, x, y, z, nx, ny, nz)];
+        F(macro)(L, f, &rho, u);
+        const REAL s2 = F(dot)(u, u, L->D);
+        const REAL k = R(0.5) * rho * s2;
+        const REAL sp = SQRTR(s2);
+        mass += (double)rho;
+        ke += (double)k;
+        if (!isfinite(sp)) nonfinite += 1.0;
+        umax = umax < (double)sp ? (double)sp : umax;
+      }
+  out[0] = mass;
+  out[1] = ke;
+  out[2] = umax;
+  out[3] = nonfinite;
+  out[4] = (nonfinite > 0.0 || umax > speed_limit) ? 1.0 : 0.0;
+  return 0;
+}
+
 static int F(macro_fields)(const lattice_t* L, const void* vf, size_t nx, size_t ny, size_t nz,
                            double* rho_out, double* u_out) {
   const REAL* fl = (const REAL*)vf;

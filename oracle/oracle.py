@@ -12,6 +12,7 @@ this module. The engine never does.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -52,6 +53,7 @@ def _bind(lib, prefix):
     if prefix == "oracle_":
         sig["reactive_stats"] = (C.c_int, [C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, C.c_double, C.c_int, _dp])
         sig["fluid_diagnostics"] = (C.c_int, [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _dp])
+        sig["fluid_diagnostics64"] = (C.c_int, [C.c_int, C.c_int, _vp, _sz, _sz, _sz, C.c_double, _dp])
         sig["macro_fields"] = (C.c_int, [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _dp, _dp])
         sig["init_equilibrium"] = (C.c_int, [C.c_int, C.c_int, _dp, _dp, _vp, _sz, _sz, _sz])
     else:
@@ -170,6 +172,16 @@ def fluid_diagnostics(f, lattice, nx, ny, nz):
     out = np.zeros(3, np.float64)
     _check(ORACLE.fluid_diagnostics(LATTICES[lattice], _prec(f.dtype), _ptr(f), nx, ny, nz, _dptr(out)),
            "fluid_diagnostics")
+    return out
+
+
+def fluid_diagnostics64(f, lattice, nx, ny, nz, speed_limit=math.inf):
+    """The engine's diagnostics (FP64 sums): mass, KE, max |u|, non-finite
+    cells, crash flag."""
+    f = np.ascontiguousarray(f)
+    out = np.zeros(5, np.float64)
+    _check(ORACLE.fluid_diagnostics64(LATTICES[lattice], _prec(f.dtype), _ptr(f), nx, ny, nz,
+                                      float(speed_limit), _dptr(out)), "fluid_diagnostics64")
     return out
 
 

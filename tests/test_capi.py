@@ -103,3 +103,52 @@ def test_extension_enum_validation(lib):
     # a too-small partials buffer is rejected
     assert E.reactive_stats_async("D3Q7", "float", A0, A1, 256, 256, 256, 0.1, A2, 16, A3) == \
         E.cudaErrorInvalidValue
+
+
+def test_diagnostics_validation(lib):
+    assert E.diagnostics_partials_bytes("D3Q19", 256, 256, 256) == 2 * 256 * 256 * 4 * 8
+    assert E.diagnostics_partials_bytes("D2Q9", 1024, 1024, 7) == 8 * 1024 * 4 * 8
+    assert E.diagnostics_partials_bytes("D3Q19", 0, 4, 4) == 0
+    need = E.diagnostics_partials_bytes("D3Q19", 8, 8, 8)
+    # null populations, partials or output
+    assert E.fluid_diagnostics_async("D3Q19", "float", None, 8, 8, 8, A1, need, A2) == \
+        E.cudaErrorInvalidDevicePointer
+    assert E.fluid_diagnostics_async("D3Q19", "float", A0, 8, 8, 8, None, need, A2) == \
+        E.cudaErrorInvalidDevicePointer
+    assert E.step_diagnostics_async("D3Q19", "float", "TRT", A0, A1, 8, 8, 8, 1.6, A2, need, None) == \
+        E.cudaErrorInvalidDevicePointer
+    # zero extent, too-small scratch, scratch overlapping the populations, bad enums
+    assert E.fluid_diagnostics_async("D3Q19", "float", A0, 8, 0, 8, A1, need, A2) == E.cudaErrorInvalidValue
+    assert E.fluid_diagnostics_async("D3Q19", "float", A0, 8, 8, 8, A1, need - 8, A2) == E.cudaErrorInvalidValue
+    assert E.fluid_diagnostics_async("D3Q19", "float", A0, 8, 8, 8, A0 + 64, need, A2) == \
+        E.cudaErrorInvalidValue
+    assert E.step_diagnostics_async("D3Q19", "double", "BGK", A0, A1, 8, 8, 8, 1.6, A2, need, A1 + 8) == \
+        E.cudaErrorInvalidValue
+    assert E.fluid_diagnostics_async("D2Q5", "float", A0, 8, 8, 1, A1, need, A2) == E.cudaErrorInvalidValue
+    assert E.load().lbm_step_diagnostics_async(1, 0, 9, A0, A1, 8, 8, 8, 1.6, 1.0, A2, need, A3, None) == \
+        E.cudaErrorInvalidValue
+
+
+def test_oracle_diagnostics_semantics():
+    """The oracle's FP64-accumulated diagnostics: sums and max of the per-cell
+    terms, NaN speeds skipped by the max but counted, the crash flag."""
+    import numpy as np
+
+    import _util as U
+    import oracle as O
+
+    f = U.random_state("D3Q19", 6, 5, 4, np.float64, seed=3)
+    d = O.fluid_diagnostics64(f, "D3Q19", 6, 5, 4, speed_limit=1.0)
+    rho, u = O.macro_fields(f, "D3Q19", 6, 5, 4)
+    s2 = (u * u).sum(0)
+    assert d[0] == pytest.approx(rho.sum(), rel=1e-14)
+    assert d[1] == pytest.approx((0.5 * rho * s2).sum(), rel=1e-12)
+    assert d[2] == np.sqrt(s2).max() and d[3] == 0 and d[4] == 0
+    ref = O.fluid_diagnostics(f, "D3Q19", 6, 5, 4)
+    assert d[2] == ref[2]
+    assert O.fluid_diagnostics64(f, "D3Q19", 6, 5, 4, speed_limit=0.5 * d[2])[4] == 1
+    g = f.copy()
+    g[3, 7] = np.nan  # one cell with a NaN population
+    dn = O.fluid_diagnostics64(g, "D3Q19", 6, 5, 4, speed_limit=1.0)
+    assert np.isnan(dn[0]) and dn[3] == 1 and dn[4] == 1
+    assert dn[2] == np.sqrt(np.delete(s2, 7)).max()
