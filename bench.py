@@ -231,6 +231,15 @@ def run_variants(torch, E, dev, f32, peak, fp32_ms):
         ms = _time_steps(torch, lambda a, b, op=op: E.launch_step_gpu("D3Q19", "float", op, a, b, NX, NY, NZ, omega),
                          f32.clone(), g, 200, 10)
         rec(f"D3Q19 {op} fp32", ms, 152)
+    # every step also reduces mass, kinetic energy, max |u| and the blow-up flag
+    nb = E.diagnostics_partials_bytes("D3Q19", NX, NY, NZ)
+    part = torch.empty(nb, dtype=torch.uint8, device=dev)
+    diag = torch.empty(5, dtype=torch.float64, device=dev)
+    ms = _time_steps(torch, lambda a, b: E.step_diagnostics_async("D3Q19", "float", "TRT", a, b, NX, NY, NZ, omega,
+                                                                    part, nb, diag, speed_limit=0.2),
+                     f32.clone(), g, 200, 10)
+    rec("D3Q19 TRT fp32 + diagnostics every step", ms, 152, vs_plain_step=round(fp32_ms / ms, 3))
+    del part, diag
     h = torch.empty(f32.shape, dtype=torch.int16, device=dev)
     hg = torch.empty_like(h)
     for fmt in FORMATS16:
@@ -374,6 +383,78 @@ def run_adjoint_cost(torch, E, dev, n=128, steps=2000, interval=100, tau=0.56):
     return res
 
 
+def blob_fields(torch, dev, n, block, seed):
+    """A and B in {0, 1} on interleaved block^3 cubes (a 3-D checkerboard) with a
+    seeded random phase per axis; B = 1 - A."""
+    gen = torch.Generator().manual_seed(seed)
+    off = torch.randint(0, block, (3,), generator=gen).tolist()
+    ax = torch.arange(n, device=dev)
+    z, y, x = torch.meshgrid(ax, ax, ax, indexing="ij")
+    parity = ((x + off[2]) // block + (y + off[1]) // block + (z + off[0]) // block) % 2
+    a = (parity == 0).float()
+    return a.contiguous(), (1.0 - a).contiguous()
+
+
+def run_reactive_adjoint_cost(torch, E, dev, n=192, steps=3000, interval=60, tau=0.56, tau_c=0.55,
+                              k=0.03 / 16):
+    """Reactive adjoint cost: D3Q19 TRT + two D3Q7 scalars (A + B -> C), FP32,
+    objective final mean C; gradient w.r.t. k, tau, tau_c and the initial A
+    and B fields, over one forward run of the same fused coupled step."""
+    u0 = solenoidal_field(torch, dev, n, 0.03, 4.0, SEED).float()
+    rho0 = torch.ones((n, n, n), dtype=torch.float32, device=dev)
+    a0, b0 = blob_fields(torch, dev, n, 16, SEED)
+    nbytes = E.reactive_gradient_workspace_bytes("D3Q19", "float", n, n, n, steps, interval)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    res = torch.zeros(4, dtype=torch.float64, device=dev)
+    ga, gb = torch.empty_like(a0), torch.empty_like(b0)
+    omega, omega_c = 1.0 / tau, 1.0 / tau_c
+    # forward-only run of the same coupled step, in buffers of the workspace
+    f = [ws[:19 * n ** 3 * 4].view(torch.float32).view(19, n, n, n),
+         ws[19 * n ** 3 * 4:38 * n ** 3 * 4].view(torch.float32).view(19, n, n, n)]
+    base = 38 * n ** 3 * 4
+    sc = [ws[base + i * 7 * n ** 3 * 4: base + (i + 1) * 7 * n ** 3 * 4].view(torch.float32).view(7, n, n, n)
+          for i in range(4)]
+
+    def forward(nsteps):
+        E.check(E.init_equilibrium_async("D3Q19", "float", rho0, u0, f[0], n, n, n))
+        E.check(E.init_equilibrium_async("D3Q7", "float", a0, u0, sc[0], n, n, n))
+        E.check(E.init_equilibrium_async("D3Q7", "float", b0, u0, sc[2], n, n, n))
+        for s in range(nsteps):
+            i, j = s % 2, (s + 1) % 2
+            E.check(E.fluid_reaction_ab_async("D3Q19", "float", "TRT", f[i], f[j], sc[i], sc[j], sc[2 + i],
+                                              sc[2 + j], n, n, n, omega, omega_c, k))
+
+    def gradient(nsteps, nint):
+        E.check(E.reactive_gradient_async("D3Q19", "float", "TRT", "mean_product", rho0, u0, a0, b0, n, n, n,
+                                          tau, tau_c, k, nsteps, nint, ws, nbytes, res, ga, gb))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        fn()
+        t1.record()
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1)
+
+    forward(4)  # warm-up (kernels, clocks)
+    gradient(4, 2)
+    fwd_ms = timed(lambda: forward(steps))
+    grad_ms = timed(lambda: gradient(steps, interval))
+    r = res.tolist()
+    out = {"config": f"D3Q19 TRT + 2 x D3Q7 (A + B -> C) FP32 {n}^3, tau {tau}, tau_c {tau_c}, k {k:.6g}, "
+                     f"{steps} steps, solenoidal u0 (amplitude 0.03, spectrum peak |k| = 4), A, B in {{0, 1}} "
+                     f"on interleaved 16^3 blocks, objective final mean C, checkpoint every {interval}",
+           "forward_ms": round(fwd_ms, 2), "gradient_ms": round(grad_ms, 2),
+           "cost_ratio": round(grad_ms / fwd_ms, 3), "objective": r[0], "dJ_dk": r[1], "dJ_dtau": r[2],
+           "dJ_dtau_c": r[3], "grad_a0_l2": float(torch.linalg.vector_norm(ga.double())),
+           "workspace_gb": round(nbytes / 1e9, 2)}
+    del ws, ga, gb, f, sc
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_engine(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -472,13 +553,14 @@ def run_engine(args, rank, world, local_rank):
         return None
     peak, peak_kind = measured_hbm_peak()
     traffic = committed_traffic(f"d3q19_float_trt_{NX}") if storage == "fp32" else None
-    variants = accuracy = fp16_store = adjoint = None
+    variants = accuracy = fp16_store = adjoint = adjoint_reactive = None
     if world == 1 and not args.no_variants and storage == "fp32":
         variants = run_variants(torch, E, dev, f, peak, ms_per_step)
         del f, g
         torch.cuda.empty_cache()
         accuracy = run_accuracy(torch, E, dev)
         adjoint = run_adjoint_cost(torch, E, dev)
+        adjoint_reactive = run_reactive_adjoint_cost(torch, E, dev)
         # the fastest 16-bit format meeting the 1e-3 velocity error bar for TRT
         ok = [v for v in variants if v["variant"].startswith("D3Q19 TRT ") and v["variant"][10:] in FORMATS16
               and accuracy["by_collision"]["TRT"][v["variant"][10:]] <= 1e-3]
@@ -500,7 +582,8 @@ def run_engine(args, rank, world, local_rank):
                      "traffic": traffic, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_per_lu * cells},
         "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps,
-        "fp16_store": fp16_store, "adjoint": adjoint, "variants": variants, "accuracy": accuracy,
+        "fp16_store": fp16_store, "adjoint": adjoint, "adjoint_reactive": adjoint_reactive,
+        "variants": variants, "accuracy": accuracy,
     }
     return line
 
@@ -595,7 +678,9 @@ def main():
         torch.cuda.set_device(dev)
         E.load()
         res = run_adjoint_cost(torch, E, dev, n=args.size, steps=args.steps, interval=min(100, args.steps))
-        print(json.dumps({"adjoint": res}), flush=True)
+        rres = run_reactive_adjoint_cost(torch, E, dev, n=args.size, steps=args.steps,
+                                         interval=min(60, args.steps))
+        print(json.dumps({"adjoint": res, "adjoint_reactive": rres}), flush=True)
         return
     if world > 1:
         import datetime

@@ -345,6 +345,30 @@ int lbm_adjoint_step_async(int lattice, int precision, int collision, const void
     const void* lambda_next, void* lambda, size_t x_extent, size_t y_extent, size_t z_extent,
     double tau, double* dtau_slots, void* stream);
 
+/* Reactive-mixing gradients (no reference counterpart): the checkpointed
+ * discrete adjoint of the coupled step of lbm_fluid_reaction_ab_async (fluid
+ * BGK or TRT, then the A + B -> C reaction step of launch_reaction_AB_gpu on
+ * the post-step fluid, src/simulate_reaction.cpp:518-543). Initial state:
+ * f^0 = f_eq(rho0, u0), A^0 = g_eq(a0, u0), B^0 = g_eq(b0, u0) (fields [Z,Y,X],
+ * u0 [D,Z,Y,X], population precision). Objective of the state after `steps`:
+ *   LBM_OBJECTIVE_MEAN_PRODUCT  <C> = <a0> - <C_A>   (mean product formed)
+ *   LBM_OBJECTIVE_SEGREGATION   I_s = cov(C_A, C_B) / (<C_A> <C_B>), as
+ *                               compute_reactive_stats (lattice_io.hpp:318-337)
+ * result (device, 4 doubles): J, dJ/dk, dJ/dtau, dJ/dtau_c (omega = 1/tau,
+ * omega_c = 1/tau_c rounded to the population precision, as the launchers
+ * take them); grad_a0 = dJ/da0 and, if non-null, grad_b0 = dJ/db0 ([Z,Y,X]).
+ * Workspace of lbm_reactive_gradient_workspace_bytes bytes, not overlapping
+ * the inputs or outputs. Cost: about 2 forward runs + 1 adjoint run. */
+#define LBM_OBJECTIVE_MEAN_PRODUCT 0
+#define LBM_OBJECTIVE_SEGREGATION 1
+size_t lbm_reactive_gradient_workspace_bytes(int fluid_lattice, int precision, size_t x_extent,
+    size_t y_extent, size_t z_extent, int steps, int checkpoint_interval);
+int lbm_reactive_gradient_async(int fluid_lattice, int precision, int collision, int objective,
+    const void* rho0, const void* u0, const void* a0, const void* b0, size_t x_extent,
+    size_t y_extent, size_t z_extent, double tau, double tau_c, double k_react, int steps,
+    int checkpoint_interval, void* workspace, size_t workspace_bytes, double* result,
+    void* grad_a0, void* grad_b0, void* stream);
+
 /* Allocation-free form of lbm_reactive_stats_async. No counterpart in the
  * reference. For callers that cannot allocate device memory, e.g. a plugin or
  * FFI binding inside an application that owns every device allocation and

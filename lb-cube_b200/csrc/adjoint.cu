@@ -1,44 +1,21 @@
 // Discrete reverse-mode adjoint of the collide-stream step (BGK, TRT) and the
 // checkpointed gradient of the final kinetic energy. No reference counterpart.
 //
-// Forward step (lattice_core.hpp:146-216): f^{n+1}(x, i) = C_i(g(x)), with the
-// pulled state g_j(x) = f^n(x - c_j, j). For an objective J(f^N), the adjoint
-// lambda^n = dJ/df^n obeys
-//   lambda^n(x - c_j, j) = mu_j(x),   mu(x) = J_C(g(x))^T lambda^{n+1}(x, .),
-// a scatter that is a bijection for every j (race-free with ping-pong buffers).
-// For f_eq = w rho (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u.u) as a function of
-// rho = sum g and j = sum g c:
-//   d f_eq_i / d rho = w_i (1 - 4.5 (c_i.u)^2 + 1.5 u.u)
-//   d f_eq_i / d j_a = w_i (3 c_ia + 9 (c_i.u) c_ia - 3 u_a)
-// so with Lambda_i the weights of f_eq_i in C (BGK: omega lambda_i; TRT:
-// omega+ (lambda_i + lambda_o)/2 + omega- (lambda_i - lambda_o)/2),
-//   mu_j = a lambda_j + b lambda_opp(j) + A + B . c_j,
-//   A = sum_i Lambda_i d f_eq_i / d rho,   B_a = sum_i Lambda_i d f_eq_i / d j_a,
-// with a = 1 - omega, b = 0 (BGK) or a = 1 - (omega+ + omega-)/2,
-// b = (omega- - omega+)/2 (TRT): O(Q) work per cell. The tau-derivative of
-// the step, sum_x lambda^{n+1} . dC/dtau, is accumulated per block in FP64
-// into slots the block owns (deterministic over steps).
+// adjoint_step_kernel applies the transposed step Jacobian of adjoint.cuh at
+// every cell and scatters to the pull sources. The tau-derivative of the step,
+// sum_x lambda^{n+1} . dC/dtau, is accumulated per block in FP64 into slots
+// the block owns (deterministic over steps).
 #include <algorithm>
 #include <climits>
 
+#include "adjoint.cuh"
+#include "cells.cuh"
 #include "collide.cuh"
 #include "common.cuh"
 #include "reduce.cuh"
 #include "../../include/lbcube_b200.h"
 
 namespace lbcube {
-
-template <class L, class Real>
-__device__ __forceinline__ void load_local(const Real* __restrict__ p, const Grid& g, int cell,
-                                           Real (&v)[L::Q]) {
-  const size_t plane = (size_t)g.plane;
-  static_for<L::Q>([&](auto I) { v[LB_I(I)] = __ldg(p + plane * LB_I(I) + cell); });
-}
-
-struct AdjointParams {
-  double omega, omega_minus;
-  double domega_dtau, domega_minus_dtau;  // derivatives of the rates w.r.t. tau
-};
 
 template <class L, class Real, int CT>
 __global__ void __launch_bounds__(kThreads)
@@ -49,84 +26,15 @@ __global__ void __launch_bounds__(kThreads)
   const bool active = cell_of(g, x, y, z);
   double dtau = 0.0;
   if (active) {
-    const int xm = x == 0 ? g.nx - 1 : x - 1, xp = x == g.nx - 1 ? 0 : x + 1;
-    const int ym = y == 0 ? g.ny - 1 : y - 1, yp = y == g.ny - 1 ? 0 : y + 1;
-    const int zm = z == 0 ? g.nz - 1 : z - 1, zp = z == g.nz - 1 ? 0 : z + 1;
-    const size_t plane = (size_t)g.plane;
+    const Neighbours n = neighbours(g, x, y, z);
     const int cell = (z * g.ny + y) * g.nx + x;
-    Real gv[L::Q], lv[L::Q];
-    // pulled pre-collision state, as in the forward step
-    static_for<L::Q>([&](auto I) {
-      constexpr int i = LB_I(I);
-      constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-      const int sx = cx == 0 ? x : (cx > 0 ? xm : xp);
-      const int sy = cy == 0 ? y : (cy > 0 ? ym : yp);
-      const int sz = cz == 0 ? z : (cz > 0 ? zm : zp);
-      gv[i] = __ldg(fn + plane * i + ((sz * g.ny + sy) * g.nx + sx));
-    });
-    load_local<L>(lam_next, g, cell, lv);
+    Real gv[L::Q], lv[L::Q], mu[L::Q];
+    gather<L>(fn, g, n, x, y, z, gv);  // pulled pre-collision state, as in the forward step
+    load_cell<L>(lam_next, g, cell, lv);
     Real rho, u[L::D];
     macro_state<L>(gv, rho, u);
-    const Real usq = u_dot_u<L>(u);
-    Real eq[L::Q];
-    equilibria<L>(rho, u, usq, eq);
-    const Real om = Real(ap.omega), omm = Real(ap.omega_minus);
-    // weights of f_eq in C, and the tau-derivative of the step (per cell in the
-    // population precision, accumulated over cells in FP64)
-    Real Lam[L::Q];
-    Real dt1 = Real(0), dt2 = Real(0);
-    static_for<L::Q>([&](auto I) {
-      constexpr int i = LB_I(I);
-      constexpr int o = L::opp[i];
-      if constexpr (CT == kBGK) {
-        Lam[i] = om * lv[i];
-        dt1 += lv[i] * (eq[i] - gv[i]);
-      } else {
-        const Real lp = Real(0.5) * (lv[i] + lv[o]), lm = Real(0.5) * (lv[i] - lv[o]);
-        Lam[i] = om * lp + omm * lm;
-        dt1 += lv[i] * (Real(0.5) * ((gv[i] + gv[o]) - (eq[i] + eq[o])));  // g+ - f_eq+
-        dt2 += lv[i] * (Real(0.5) * ((gv[i] - gv[o]) - (eq[i] - eq[o])));  // g- - f_eq-
-      }
-    });
-    if constexpr (CT == kBGK) {
-      dtau = (double)dt1 * ap.domega_dtau;
-    } else {
-      dtau = -((double)dt1 * ap.domega_dtau + (double)dt2 * ap.domega_minus_dtau);
-    }
-    // A = sum_i w_i Lam_i (1 + 1.5 u.u) - 4.5 sum_i w_i Lam_i (c_i.u)^2
-    // B = sum_i w_i Lam_i (3 + 9 c_i.u) c_i - 3 u sum_i w_i Lam_i
-    Real W = Real(0), Aq = Real(0), B[L::D];
-    static_for<L::D>([&](auto D) { B[LB_I(D)] = Real(0); });
-    static_for<L::Q>([&](auto I) {
-      constexpr int i = LB_I(I);
-      constexpr double wd = L::w[i];
-      const Real cu = c_dot<L, i>(u);
-      const Real wl = Real(wd) * Lam[i];
-      W += wl;
-      Aq += wl * cu * cu;
-      const Real s = wl * (Real(3) + Real(9) * cu);
-      static_for<L::D>([&](auto D) {
-        constexpr int c = L::c[i][LB_I(D)];
-        if constexpr (c > 0) B[LB_I(D)] += s;
-        if constexpr (c < 0) B[LB_I(D)] -= s;
-      });
-    });
-    const Real A = W * (Real(1) + Real(1.5) * usq) - Real(4.5) * Aq;
-    static_for<L::D>([&](auto D) { B[LB_I(D)] -= Real(3) * W * u[LB_I(D)]; });
-    const Real a = CT == kBGK ? Real(1) - om : Real(1) - Real(0.5) * (om + omm);
-    const Real b = CT == kBGK ? Real(0) : Real(0.5) * (omm - om);
-    // scatter mu_j to lambda^n(x - c_j, j)
-    static_for<L::Q>([&](auto I) {
-      constexpr int j = LB_I(I);
-      constexpr int o = L::opp[j];
-      constexpr int cx = L::c[j][0], cy = L::c[j][1], cz = L::c[j][2];
-      Real mu = a * lv[j] + A + c_dot<L, j>(B);
-      if constexpr (CT != kBGK) mu += b * lv[o];
-      const int tx = cx == 0 ? x : (cx > 0 ? xm : xp);
-      const int ty = cy == 0 ? y : (cy > 0 ? ym : yp);
-      const int tz = cz == 0 ? z : (cz > 0 ? zm : zp);
-      lam[plane * j + ((tz * g.ny + ty) * g.nx + tx)] = mu;
-    });
+    dtau = fluid_adjoint_cell<L, Real, CT>(gv, lv, rho, u, ap, mu);
+    scatter<L>(lam, g, n, x, y, z, mu);
   }
   if (dtau_slots != nullptr) {
     double v[1] = {dtau};
@@ -151,7 +59,7 @@ __global__ void __launch_bounds__(kThreads)
     const int cell = (z * g.ny + y) * g.nx + x;
     const size_t plane = (size_t)g.plane;
     Real fv[L::Q], rho, u[L::D];
-    load_local<L>(f, g, cell, fv);
+    load_cell<L>(f, g, cell, fv);
     macro_state<L>(fv, rho, u);
     const Real usq = u_dot_u<L>(u);
     ke = 0.5 * (double)rho * (double)usq;
@@ -176,7 +84,7 @@ __global__ void __launch_bounds__(kThreads)
   const size_t plane = (size_t)g.plane;
   Real u[L::D], lv[L::Q];
   static_for<L::D>([&](auto D) { u[LB_I(D)] = u0[plane * LB_I(D) + cell]; });
-  load_local<L>(lam0, g, cell, lv);
+  load_cell<L>(lam0, g, cell, lv);
   const Real r = rho0[cell];
   Real gr[L::D];
   static_for<L::D>([&](auto D) { gr[LB_I(D)] = Real(0); });
@@ -193,37 +101,6 @@ __global__ void __launch_bounds__(kThreads)
     });
   });
   static_for<L::D>([&](auto D) { grad[plane * LB_I(D) + cell] = gr[LB_I(D)]; });
-}
-
-// Fixed-order sum of n doubles into out[0] (one block).
-__global__ void __launch_bounds__(1024) sum_slots_kernel(const double* __restrict__ s, long long n,
-                                                         double scale, double* __restrict__ out) {
-  __shared__ double sh[1024];
-  double acc = 0.0;
-  for (long long k = threadIdx.x; k < n; k += 1024) acc += s[k];
-  sh[threadIdx.x] = acc;
-  __syncthreads();
-  for (int st = 512; st > 0; st >>= 1) {
-    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) out[0] = sh[0] * scale;
-}
-
-template <class Real>
-AdjointParams make_params(int collision, double tau) {
-  AdjointParams ap{};
-  const Real omega = Real(1) / Real(tau);
-  ap.omega = omega;
-  ap.domega_dtau = -(double)omega * (double)omega;
-  if (collision == kTRT) {
-    const Real omm = trt_omega_minus<Real>(omega);
-    ap.omega_minus = omm;
-    // tau- = Lambda / (tau - 1/2) + 1/2  =>  d omega- / d tau = omega-^2 Lambda / (tau - 1/2)^2
-    const double t = (double)tau - 0.5;
-    ap.domega_minus_dtau = (double)omm * (double)omm * 0.25 / (t * t);
-  }
-  return ap;
 }
 
 template <class L, class Real>
@@ -332,8 +209,8 @@ cudaError_t ke_gradient(int collision, const Real* rho0, const Real* u0, const G
   }
   velocity_gradient_kernel<L, Real><<<grid_dims(g), kThreads, 0, s>>>(rho0, u0, lam[0], grad_u0, g);
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
-  sum_slots_kernel<<<1, 1024, 0, s>>>(ke_slots, lay.slots, 1.0, out);
-  sum_slots_kernel<<<1, 1024, 0, s>>>(dtau_slots, lay.slots, 1.0, out + 1);
+  sum_slots_kernel<<<1, 1024, 0, s>>>(ke_slots, lay.slots, 1, 1.0, out);
+  sum_slots_kernel<<<1, 1024, 0, s>>>(dtau_slots, lay.slots, 1, 1.0, out + 1);
   return cudaGetLastError();
 }
 

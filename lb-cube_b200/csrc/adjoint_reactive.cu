@@ -1,0 +1,480 @@
+// Checkpointed discrete adjoint of the coupled fluid + A + B -> C step, and
+// the gradients of a reactive-mixing objective with respect to the reaction
+// rate k, the fluid relaxation time tau, the scalar relaxation time tau_c and
+// the initial concentration fields A0, B0. No reference counterpart.
+//
+// Forward step n (src/simulate_reaction.cpp:518-543, one fused launch here):
+//   f^{n+1} = S(f^n)                            fluid collide-stream
+//   A^{n+1}_i(x) = a_i + w_c (g_eq_i(C_A, u) - a_i) + w_i S(C_A, C_B, k)
+//   B^{n+1}_i(x) = b_i + w_c (g_eq_i(C_B, u) - b_i) + w_i S(C_A, C_B, k)
+// with a_j = A^n(x - c_j, j), C_A = sum a (likewise b, C_B), u the fluid
+// velocity of f^{n+1}(x), g_eq_i(C, u) = w_i C (1 + c_i.u / cs2)
+// (lattice_physics.hpp:643-694) and S the exact batch source (:712-743).
+//
+// Adjoint step n, per cell x, with (lf, la, lb) = lambda^{n+1} at x:
+//   sigma = sum_i w_i (la_i + lb_i)
+//   abar_j = (1 - w_c) la_j + w_c sum_i la_i w_i (1 + c_i.u / cs2) + sigma dS/dC_A
+//   bbar_j = (1 - w_c) lb_j + w_c sum_i lb_i w_i (1 + c_i.u / cs2) + sigma dS/dC_B
+//   ubar   = (w_c / cs2) sum_i w_i c_i (C_A la_i + C_B lb_i)
+//   lf_k  += (c_k - u) . ubar / rho            (u = j / rho of f^{n+1}(x))
+// then the fluid adjoint (adjoint.cuh) on the updated lf; abar, bbar and the
+// fluid mu scatter to the pull sources. dJ/dk gathers sigma dS/dk, dJ/dw_c
+// gathers sum_i la_i (g_eq_i(C_A) - a_i) + lb_i (g_eq_i(C_B) - b_i). The
+// linearisation point uses the cell's pre-collision (rho, u), equal to the
+// post-collision ones up to rounding (BGK and TRT conserve mass and momentum).
+// The source derivatives are evaluated in FP64 at the step's inputs on the
+// branch the forward step took.
+//
+// Objectives (final state N, means over the N_c cells):
+//   LBM_OBJECTIVE_MEAN_PRODUCT  <C> = <A0> - <C_A^N>   (C = A0 - A; transport
+//                               conserves A, so this is the product formed)
+//   LBM_OBJECTIVE_SEGREGATION   I_s = cov(C_A, C_B) / (<C_A> <C_B>) of
+//                               compute_reactive_stats (lattice_io.hpp:318-337)
+#include <algorithm>
+
+#include "adjoint.cuh"
+#include "cells.cuh"
+#include "collide.cuh"
+#include "common.cuh"
+#include "reduce.cuh"
+#include "../../include/lbcube_b200.h"
+
+namespace lbcube {
+
+// dS/da, dS/db, dS/dk of reaction_source (collide.cuh) on the branch the
+// forward evaluation takes for these Real inputs, in FP64.
+//   near-equal branch: a' = a / (1 + k a)
+//   otherwise:         a' = N / D, N = a d e, D = b - a e, d = b - a, e = exp(-k d)
+template <class Real>
+__device__ __forceinline__ void reaction_source_grad(Real a, Real b, Real k, double& dsa,
+                                                     double& dsb, double& dsk) {
+  const Real abs_a = a < Real{} ? -a : a;
+  const Real abs_b = b < Real{} ? -b : b;
+  const Real diff = b - a;
+  const Real abs_diff = diff < Real{} ? -diff : diff;
+  const Real tol = Real(64.0) * RealEps<Real>::value * (Real(1.0) + abs_a + abs_b);
+  const double A = a, B = b, K = k;
+  if (abs_diff <= tol) {
+    const double q = 1.0 + K * A;
+    const double r = 1.0 / (q * q);
+    dsa = r - 1.0;
+    dsb = 0.0;
+    dsk = -A * A * r;
+  } else {
+    const double d = B - A;
+    const double e = exp(-K * d);
+    const double N = A * d * e, D = B - A * e, ap = N / D;
+    const double dna = e * (d - A + A * d * K), dnb = A * e * (1.0 - d * K), dnk = -A * d * d * e;
+    const double dda = -e * (1.0 + A * K), ddb = 1.0 + A * K * e, ddk = A * d * e;
+    dsa = (dna - ap * dda) / D - 1.0;
+    dsb = (dnb - ap * ddb) / D;
+    dsk = (dnk - ap * ddk) / D;
+  }
+}
+
+struct ReactiveParams {
+  AdjointParams fluid;
+  double omega_c, k;
+};
+
+// Per-block FP64 slots of the reactive adjoint: dJ/dk, dJ/dtau, dJ/domega_c.
+constexpr int kReactiveSlots = 3;
+
+template <class FL, class Real, int CT>
+__global__ void __launch_bounds__(kThreads)
+    reactive_adjoint_step_kernel(const Real* __restrict__ fn, const Real* __restrict__ an,
+                                 const Real* __restrict__ bn, const Real* __restrict__ lf_next,
+                                 const Real* __restrict__ la_next, const Real* __restrict__ lb_next,
+                                 Real* __restrict__ lf, Real* __restrict__ la,
+                                 Real* __restrict__ lb, Grid g, ReactiveParams rp,
+                                 double* __restrict__ slots) {
+  using SL = typename ScalarOf<FL>::type;
+  int x, y, z;
+  const bool active = cell_of(g, x, y, z);
+  double acc[kReactiveSlots] = {0.0, 0.0, 0.0};
+  if (active) {
+    const Neighbours n = neighbours(g, x, y, z);
+    const int cell = (z * g.ny + y) * g.nx + x;
+    Real gv[FL::Q], rho, u[FL::D];
+    gather<FL>(fn, g, n, x, y, z, gv);
+    macro_state<FL>(gv, rho, u);
+
+    // ---- reaction step --------------------------------------------------
+    Real ubar[FL::D];
+    {
+      Real ga[SL::Q], gb[SL::Q], lA[SL::Q], lB[SL::Q];
+      gather<SL>(an, g, n, x, y, z, ga);
+      gather<SL>(bn, g, n, x, y, z, gb);
+      load_cell<SL>(la_next, g, cell, lA);
+      load_cell<SL>(lb_next, g, cell, lB);
+      const Real ca = concentration<SL>(ga), cb = concentration<SL>(gb);
+      double dsa, dsb, dsk;
+      reaction_source_grad<Real>(ca, cb, Real(rp.k), dsa, dsb, dsk);
+      const Real oc = Real(rp.omega_c);
+      const Real inv_cs2 = Real(1.0 / SL::cs2);
+      Real sigma = Real(0), ea = Real(0), eb = Real(0), doc = Real(0);
+      static_for<FL::D>([&](auto D) { ubar[LB_I(D)] = Real(0); });
+      static_for<SL::Q>([&](auto I) {
+        constexpr int i = LB_I(I);
+        constexpr double wd = SL::w[i];
+        const Real w = Real(wd);
+        const Real e = w * (Real(1) + c_dot<SL, i>(u) * inv_cs2);
+        sigma += w * (lA[i] + lB[i]);
+        ea += lA[i] * e;
+        eb += lB[i] * e;
+        doc += lA[i] * (geq<SL, i>(ca, u) - ga[i]) + lB[i] * (geq<SL, i>(cb, u) - gb[i]);
+        const Real s = w * (ca * lA[i] + cb * lB[i]);
+        static_for<FL::D>([&](auto D) {
+          constexpr int c = SL::c[i][LB_I(D)];
+          if constexpr (c > 0) ubar[LB_I(D)] += s;
+          if constexpr (c < 0) ubar[LB_I(D)] -= s;
+        });
+      });
+      static_for<FL::D>([&](auto D) { ubar[LB_I(D)] *= oc * inv_cs2; });
+      acc[0] = (double)sigma * dsk;
+      acc[2] = (double)doc;
+      const Real sa = Real((double)sigma * dsa), sb = Real((double)sigma * dsb);
+      Real ma[SL::Q], mb[SL::Q];
+      static_for<SL::Q>([&](auto I) {
+        constexpr int j = LB_I(I);
+        ma[j] = (Real(1) - oc) * lA[j] + oc * ea + sa;
+        mb[j] = (Real(1) - oc) * lB[j] + oc * eb + sb;
+      });
+      scatter<SL>(la, g, n, x, y, z, ma);
+      scatter<SL>(lb, g, n, x, y, z, mb);
+    }
+
+    // ---- fluid step, with the velocity's adjoint added at this cell ------
+    Real lv[FL::Q], mu[FL::Q];
+    load_cell<FL>(lf_next, g, cell, lv);
+    Real uub = Real(0);
+    static_for<FL::D>([&](auto D) { uub += u[LB_I(D)] * ubar[LB_I(D)]; });
+    const Real inv_rho = Real(1) / rho;
+    static_for<FL::Q>([&](auto I) {
+      constexpr int k = LB_I(I);
+      lv[k] += (c_dot<FL, k>(ubar) - uub) * inv_rho;
+    });
+    acc[1] = fluid_adjoint_cell<FL, Real, CT>(gv, lv, rho, u, rp.fluid, mu);
+    scatter<FL>(lf, g, n, x, y, z, mu);
+  }
+  __shared__ double tot[kReactiveSlots];
+  block_sum_to<kReactiveSlots>(acc, tot);
+  __syncthreads();
+  if (threadIdx.x < kReactiveSlots)
+    slots[block_linear() * kReactiveSlots + threadIdx.x] += tot[threadIdx.x];
+}
+
+// Seeds lambda^N = dJ/d(f^N, A^N, B^N) and writes the block's FP64 share of J.
+//   MEAN_PRODUCT: lf = 0, la = -1/N_c, lb = 0; J partial = sum (A0 - C_A^N)
+//   SEGREGATION:  with ma, mb, <ab> = cov + ma mb of the final fields (stats),
+//     la = (C_B / (ma mb) - <ab> / (ma^2 mb)) / N_c,
+//     lb = (C_A / (ma mb) - <ab> / (ma mb^2)) / N_c   (zero when |ma mb| <= eps,
+//     where compute_reactive_stats sets I_s = 0)
+template <class FL, class Real, int OBJ>
+__global__ void __launch_bounds__(kThreads)
+    reactive_seed_kernel(const Real* __restrict__ aN, const Real* __restrict__ bN,
+                         const Real* __restrict__ a0, const double* __restrict__ stats,
+                         Real* __restrict__ lf, Real* __restrict__ la, Real* __restrict__ lb,
+                         Grid g, double* __restrict__ j_slots) {
+  using SL = typename ScalarOf<FL>::type;
+  int x, y, z;
+  const bool active = cell_of(g, x, y, z);
+  double jpart = 0.0;
+  if (active) {
+    const int cell = (z * g.ny + y) * g.nx + x;
+    const size_t plane = (size_t)g.plane;
+    const double inv_n = 1.0 / (double)g.plane;
+    Real va[SL::Q], vb[SL::Q];
+    load_cell<SL>(aN, g, cell, va);
+    load_cell<SL>(bN, g, cell, vb);
+    const Real ca = concentration<SL>(va), cb = concentration<SL>(vb);
+    Real sa, sb;
+    if constexpr (OBJ == LBM_OBJECTIVE_MEAN_PRODUCT) {
+      jpart = (double)a0[cell] - (double)ca;
+      sa = Real(-inv_n);
+      sb = Real(0);
+    } else {
+      const double ma = stats[0], mb = stats[1], cov = stats[4];
+      const double mp = ma * mb, ab = cov + mp;
+      if (fabs(mp) > 2.220446049250313080847e-16) {
+        sa = Real(inv_n * ((double)cb / mp - ab / (ma * mp)));
+        sb = Real(inv_n * ((double)ca / mp - ab / (mb * mp)));
+      } else {
+        sa = sb = Real(0);
+      }
+    }
+    static_for<SL::Q>([&](auto I) {
+      la[plane * LB_I(I) + cell] = sa;
+      lb[plane * LB_I(I) + cell] = sb;
+    });
+    static_for<FL::Q>([&](auto I) { lf[plane * LB_I(I) + cell] = Real(0); });
+  }
+  double v[1] = {jpart};
+  block_sum_to<1>(v, j_slots + block_linear());
+}
+
+// dJ/dC0(x) for a scalar initialised as g_eq(C0(x), u0(x)):
+//   direct + sum_i lambda^0_i(x) w_i (1 + c_i.u0 / cs2)
+template <class FL, class Real>
+__global__ void __launch_bounds__(kThreads)
+    scalar_init_gradient_kernel(const Real* __restrict__ u0, const Real* __restrict__ lam0,
+                                Real direct, Real* __restrict__ grad, Grid g) {
+  using SL = typename ScalarOf<FL>::type;
+  int x, y, z;
+  if (!cell_of(g, x, y, z)) return;
+  const int cell = (z * g.ny + y) * g.nx + x;
+  const size_t plane = (size_t)g.plane;
+  Real u[FL::D], lv[SL::Q];
+  static_for<FL::D>([&](auto D) { u[LB_I(D)] = u0[plane * LB_I(D) + cell]; });
+  load_cell<SL>(lam0, g, cell, lv);
+  const Real inv_cs2 = Real(1.0 / SL::cs2);
+  Real s = direct;
+  static_for<SL::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr double wd = SL::w[i];
+    s += lv[i] * (Real(wd) * (Real(1) + c_dot<SL, i>(u) * inv_cs2));
+  });
+  grad[cell] = s;
+}
+
+template <class FL, class Real, int CT>
+cudaError_t launch_reactive_adjoint(const Real* const (&st)[3], const Real* const (&ln)[3],
+                                    Real* const (&l)[3], const Grid& g, const ReactiveParams& rp,
+                                    double* slots, cudaStream_t s) {
+  reactive_adjoint_step_kernel<FL, Real, CT><<<grid_dims(g), kThreads, 0, s>>>(
+      st[0], st[1], st[2], ln[0], ln[1], ln[2], l[0], l[1], l[2], g, rp, slots);
+  return cudaGetLastError();
+}
+
+struct ReactiveLayout {
+  size_t ffield, sfield, state;  // bytes: fluid field, one scalar field, one (f, A, B) state
+  long long ckpts, blocks;
+  size_t off_ckpt, off_seg, off_lam, off_slots, off_j, off_part, off_stats, total;
+};
+
+inline ReactiveLayout reactive_layout(int FQ, int SQ, size_t elem, const Grid& g, int steps,
+                                      int interval) {
+  ReactiveLayout l{};
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  l.ffield = up((size_t)FQ * g.plane * elem);
+  l.sfield = up((size_t)SQ * g.plane * elem);
+  l.state = l.ffield + 2 * l.sfield;
+  l.ckpts = (steps + interval - 1) / interval + 1;
+  l.blocks = g.blocks();
+  l.off_ckpt = 0;
+  l.off_seg = l.off_ckpt + (size_t)l.ckpts * l.state;
+  l.off_lam = l.off_seg + (size_t)interval * l.state;
+  l.off_slots = l.off_lam + 2 * l.state;
+  l.off_j = l.off_slots + up((size_t)l.blocks * kReactiveSlots * sizeof(double));
+  l.off_part = l.off_j + up((size_t)l.blocks * sizeof(double));
+  l.off_stats = l.off_part + up((size_t)l.blocks * kStatSums * sizeof(double));
+  l.total = l.off_stats + 256;
+  return l;
+}
+
+template <class FL, class Real>
+cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, const Real* u0,
+                              const Real* a0, const Real* b0, const Grid& g, double tau,
+                              double tau_c, double k, int steps, int interval, char* ws,
+                              const ReactiveLayout& lay, double* out, Real* grad_a0, Real* grad_b0,
+                              cudaStream_t s) {
+  using SL = typename ScalarOf<FL>::type;
+  constexpr int prec = sizeof(Real) == 4 ? LBM_FLOAT : LBM_DOUBLE;
+  const double omega = (double)(Real(1) / Real(tau));
+  const double omega_c = (double)(Real(1) / Real(tau_c));
+  struct State {
+    Real* f;
+    Real* a;
+    Real* b;
+  };
+  auto at = [&](size_t off) {
+    char* p = ws + off;
+    return State{reinterpret_cast<Real*>(p), reinterpret_cast<Real*>(p + lay.ffield),
+                 reinterpret_cast<Real*>(p + lay.ffield + lay.sfield)};
+  };
+  auto ckpt = [&](long long i) { return at(lay.off_ckpt + (size_t)i * lay.state); };
+  auto seg = [&](long long i) { return at(lay.off_seg + (size_t)i * lay.state); };
+  const State lam[2] = {at(lay.off_lam), at(lay.off_lam + lay.state)};
+  double* slots = reinterpret_cast<double*>(ws + lay.off_slots);
+  double* j_slots = reinterpret_cast<double*>(ws + lay.off_j);
+  double* partials = reinterpret_cast<double*>(ws + lay.off_part);
+  double* stats = reinterpret_cast<double*>(ws + lay.off_stats);
+  cudaError_t err;
+  auto step = [&](const State& c, const State& n) {
+    return (cudaError_t)lbm_fluid_reaction_ab_async(FL::id, prec, collision, c.f, n.f, c.a, n.a,
+                                                    c.b, n.b, g.nx, g.ny, g.nz, omega, omega_c, k,
+                                                    nullptr, 0, s);
+  };
+
+  // forward: equilibrium initial state, checkpoints every `interval` steps,
+  // the last segment's states kept for the backward sweep
+  const State s0 = ckpt(0);
+  if ((err = (cudaError_t)lbm_init_equilibrium_async(FL::id, prec, rho0, u0, s0.f, g.nx, g.ny, g.nz,
+                                                     s)) != cudaSuccess)
+    return err;
+  if ((err = (cudaError_t)lbm_init_equilibrium_async(SL::id, prec, a0, u0, s0.a, g.nx, g.ny, g.nz,
+                                                     s)) != cudaSuccess)
+    return err;
+  if ((err = (cudaError_t)lbm_init_equilibrium_async(SL::id, prec, b0, u0, s0.b, g.nx, g.ny, g.nz,
+                                                     s)) != cudaSuccess)
+    return err;
+  const long long nseg = (steps + interval - 1) / interval;
+  const int last0 = (int)((nseg - 1) * interval);
+  State cur = s0;
+  for (int n = 0; n < steps; ++n) {
+    State nxt;
+    if (n + 1 == steps || (n + 1) % interval == 0)
+      nxt = ckpt((n + 1 + interval - 1) / interval);
+    else if (n + 1 > last0)
+      nxt = seg(n + 1 - last0);
+    else
+      nxt = seg(n % 2);
+    if ((err = step(cur, nxt)) != cudaSuccess) return err;
+    cur = nxt;
+  }
+
+  // seed lambda^N and J
+  const State& lN = lam[steps % 2];
+  if (objective == LBM_OBJECTIVE_SEGREGATION) {
+    err = (cudaError_t)lbm_reactive_stats_async(SL::id, prec, cur.a, cur.b, g.nx, g.ny, g.nz, k,
+                                                partials, (size_t)lay.blocks * kStatSums * sizeof(double),
+                                                stats, s);
+    if (err != cudaSuccess) return err;
+    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_SEGREGATION><<<grid_dims(g), kThreads, 0, s>>>(
+        cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, j_slots);
+  } else {
+    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_MEAN_PRODUCT><<<grid_dims(g), kThreads, 0, s>>>(
+        cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, j_slots);
+  }
+  if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  if ((err = cudaMemsetAsync(slots, 0, (size_t)lay.blocks * kReactiveSlots * sizeof(double), s)) !=
+      cudaSuccess)
+    return err;
+
+  ReactiveParams rp{};
+  rp.fluid = make_params<Real>(collision, tau);
+  rp.omega_c = omega_c;
+  rp.k = (double)Real(k);
+  for (long long kk = nseg - 1; kk >= 0; --kk) {
+    const int n0 = (int)(kk * interval);
+    const int n1 = (int)std::min<long long>((long long)steps, (kk + 1) * interval);
+    State src = ckpt(kk);
+    for (int n = n0 + 1; n < n1 && kk < nseg - 1; ++n) {
+      if ((err = step(src, seg(n - n0))) != cudaSuccess) return err;
+      src = seg(n - n0);
+    }
+    for (int n = n1 - 1; n >= n0; --n) {
+      const State sn = n == n0 ? ckpt(kk) : seg(n - n0);
+      const State& ln = lam[(n + 1) % 2];
+      const State& l = lam[n % 2];
+      const Real* const st[3] = {sn.f, sn.a, sn.b};
+      const Real* const lnp[3] = {ln.f, ln.a, ln.b};
+      Real* const lp[3] = {l.f, l.a, l.b};
+      err = collision == kBGK ? launch_reactive_adjoint<FL, Real, kBGK>(st, lnp, lp, g, rp, slots, s)
+                              : launch_reactive_adjoint<FL, Real, kTRT>(st, lnp, lp, g, rp, slots, s);
+      if (err != cudaSuccess) return err;
+    }
+  }
+
+  // results: J, dJ/dk, dJ/dtau, dJ/dtau_c; dJ/dA0 (and dJ/dB0)
+  const Real direct_a = objective == LBM_OBJECTIVE_MEAN_PRODUCT ? Real(1.0 / (double)g.plane) : Real(0);
+  scalar_init_gradient_kernel<FL, Real><<<grid_dims(g), kThreads, 0, s>>>(u0, lam[0].a, direct_a,
+                                                                          grad_a0, g);
+  if (grad_b0 != nullptr)
+    scalar_init_gradient_kernel<FL, Real><<<grid_dims(g), kThreads, 0, s>>>(u0, lam[0].b, Real(0),
+                                                                            grad_b0, g);
+  if (objective == LBM_OBJECTIVE_SEGREGATION) {
+    if ((err = cudaMemcpyAsync(out, stats + 5, sizeof(double), cudaMemcpyDeviceToDevice, s)) !=
+        cudaSuccess)
+      return err;
+  } else {
+    sum_slots_kernel<<<1, 1024, 0, s>>>(j_slots, lay.blocks, 1, 1.0 / (double)g.plane, out);
+  }
+  sum_slots_kernel<<<1, 1024, 0, s>>>(slots + 0, lay.blocks, kReactiveSlots, 1.0, out + 1);
+  sum_slots_kernel<<<1, 1024, 0, s>>>(slots + 1, lay.blocks, kReactiveSlots, 1.0, out + 2);
+  sum_slots_kernel<<<1, 1024, 0, s>>>(slots + 2, lay.blocks, kReactiveSlots, -omega_c * omega_c,
+                                      out + 3);
+  return cudaGetLastError();
+}
+
+inline int scalar_q(int fluid_lattice) { return fluid_lattice == kD2Q9 ? 5 : 7; }
+inline int fluid_q(int fluid_lattice) {
+  return fluid_lattice == kD2Q9 ? 9 : (fluid_lattice == kD3Q19 ? 19 : 27);
+}
+
+template <class Real>
+cudaError_t reactive_dispatch(int lattice, int collision, int objective, const void* rho0,
+                              const void* u0, const void* a0, const void* b0, size_t nx, size_t ny,
+                              size_t nz, double tau, double tau_c, double k, int steps,
+                              int interval, void* ws, size_t ws_bytes, double* out, void* grad_a0,
+                              void* grad_b0, cudaStream_t s) {
+  Grid g;
+  const int dims = lattice == kD2Q9 ? 2 : 3;
+  cudaError_t err = validate_domain(rho0 == nullptr || u0 == nullptr || a0 == nullptr ||
+                                        b0 == nullptr || ws == nullptr || out == nullptr ||
+                                        grad_a0 == nullptr,
+                                    1, 1, 1, dims, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  if (lattice != kD2Q9 && lattice != kD3Q19 && lattice != kD3Q27) return cudaErrorInvalidValue;
+  if (steps < 1 || interval < 2 || (collision != kBGK && collision != kTRT) ||
+      (objective != LBM_OBJECTIVE_MEAN_PRODUCT && objective != LBM_OBJECTIVE_SEGREGATION) ||
+      !(tau > 0.5) || !(tau_c > 0.5))
+    return cudaErrorInvalidValue;
+  const ReactiveLayout lay =
+      reactive_layout(fluid_q(lattice), scalar_q(lattice), sizeof(Real), g, steps, interval);
+  if (ws_bytes < lay.total) return cudaErrorInvalidValue;
+  char* w = static_cast<char*>(ws);
+#define LBCUBE_REACTIVE(FL)                                                                        \
+  return reactive_gradient<FL, Real>(collision, objective, (const Real*)rho0, (const Real*)u0,     \
+                                     (const Real*)a0, (const Real*)b0, g, tau, tau_c, k, steps,    \
+                                     interval, w, lay, out, (Real*)grad_a0, (Real*)grad_b0, s)
+  switch (lattice) {
+    case kD2Q9: LBCUBE_REACTIVE(D2Q9);
+    case kD3Q19: LBCUBE_REACTIVE(D3Q19);
+    default: LBCUBE_REACTIVE(D3Q27);
+  }
+#undef LBCUBE_REACTIVE
+}
+
+}  // namespace lbcube
+
+using namespace lbcube;
+
+extern "C" size_t lbm_reactive_gradient_workspace_bytes(int fluid_lattice, int precision,
+                                                        size_t x_extent, size_t y_extent,
+                                                        size_t z_extent, int steps,
+                                                        int checkpoint_interval) {
+  Grid g;
+  if (fluid_lattice != LBM_D2Q9 && fluid_lattice != LBM_D3Q19 && fluid_lattice != LBM_D3Q27)
+    return 0;
+  const int dims = fluid_lattice == LBM_D2Q9 ? 2 : 3;
+  if (validate_domain(false, 1, 1, 1, dims, x_extent, y_extent, z_extent, g) != cudaSuccess)
+    return 0;
+  if (steps < 1 || checkpoint_interval < 2) return 0;
+  if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return 0;
+  return reactive_layout(fluid_q(fluid_lattice), scalar_q(fluid_lattice),
+                         precision == LBM_DOUBLE ? 8 : 4, g, steps, checkpoint_interval)
+      .total;
+}
+
+extern "C" int lbm_reactive_gradient_async(int fluid_lattice, int precision, int collision,
+                                           int objective, const void* rho0, const void* u0,
+                                           const void* a0, const void* b0, size_t x_extent,
+                                           size_t y_extent, size_t z_extent, double tau,
+                                           double tau_c, double k_react, int steps,
+                                           int checkpoint_interval, void* workspace,
+                                           size_t workspace_bytes, double* result,
+                                           void* grad_a0, void* grad_b0, void* stream) {
+  const cudaStream_t s = as_stream(stream);
+  if (precision == LBM_FLOAT)
+    return (int)reactive_dispatch<float>(fluid_lattice, collision, objective, rho0, u0, a0, b0,
+                                         x_extent, y_extent, z_extent, tau, tau_c, k_react, steps,
+                                         checkpoint_interval, workspace, workspace_bytes, result,
+                                         grad_a0, grad_b0, s);
+  if (precision == LBM_DOUBLE)
+    return (int)reactive_dispatch<double>(fluid_lattice, collision, objective, rho0, u0, a0, b0,
+                                          x_extent, y_extent, z_extent, tau, tau_c, k_react, steps,
+                                          checkpoint_interval, workspace, workspace_bytes, result,
+                                          grad_a0, grad_b0, s);
+  return (int)cudaErrorInvalidValue;
+}

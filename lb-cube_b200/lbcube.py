@@ -99,6 +99,8 @@ def _declare(lib):
         "lbm_ke_gradient_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, C.c_int, C.c_int,
                                   _vp, _sz, _vp, _vp, _vp],
         "lbm_adjoint_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp],
+        "lbm_reactive_gradient_async": [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _sz, _sz, _sz,
+                                        d, d, d, C.c_int, C.c_int, _vp, _sz, _vp, _vp, _vp, _vp],
         "lbm_fluid_diagnostics_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
         "lbm_step_diagnostics_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, d, _vp, _sz,
                                        _vp, _vp],
@@ -109,6 +111,8 @@ def _declare(lib):
         fn.argtypes = args
     lib.lbm_stats_partials_bytes.restype = C.c_size_t
     lib.lbm_stats_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
+    lib.lbm_reactive_gradient_workspace_bytes.restype = C.c_size_t
+    lib.lbm_reactive_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, _sz, _sz, _sz, C.c_int, C.c_int]
     lib.lbm_diagnostics_partials_bytes.restype = C.c_size_t
     lib.lbm_diagnostics_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
     lib.lbm_ke_gradient_workspace_bytes.restype = C.c_size_t
@@ -294,6 +298,27 @@ def adjoint_step_async(lattice, real, collision, populations, lambda_next, lam, 
     return load().lbm_adjoint_step_async(LATTICES[lattice], REALS[real_name(real)], COLLISIONS[collision],
                                          _ptr(populations), _ptr(lambda_next), _ptr(lam), nx, ny, nz,
                                          float(tau), _ptr(dtau_slots), _stream(stream))
+
+
+OBJECTIVES = {"mean_product": 0, "segregation": 1}
+
+
+def reactive_gradient_workspace_bytes(fluid_lattice, real, nx, ny, nz, steps, interval) -> int:
+    return load().lbm_reactive_gradient_workspace_bytes(LATTICES[fluid_lattice], REALS[real_name(real)],
+                                                        nx, ny, nz, int(steps), int(interval))
+
+
+def reactive_gradient_async(fluid_lattice, real, collision, objective, rho0, u0, a0, b0, nx, ny, nz,
+                            tau, tau_c, k_react, steps, interval, workspace, workspace_bytes, result,
+                            grad_a0, grad_b0=None, stream=None) -> int:
+    """Checkpointed adjoint of the coupled fluid + A + B -> C run: result
+    (device FP64[4]) = J, dJ/dk, dJ/dtau, dJ/dtau_c; grad_a0 (grad_b0) =
+    dJ/da0 (dJ/db0). objective in OBJECTIVES."""
+    return load().lbm_reactive_gradient_async(
+        LATTICES[fluid_lattice], REALS[real_name(real)], COLLISIONS[collision], OBJECTIVES[objective],
+        _ptr(rho0), _ptr(u0), _ptr(a0), _ptr(b0), nx, ny, nz, float(tau), float(tau_c), float(k_react),
+        int(steps), int(interval), _ptr(workspace), int(workspace_bytes), _ptr(result), _ptr(grad_a0),
+        _ptr(grad_b0), _stream(stream))
 
 
 def diagnostics_partials_bytes(lattice, nx, ny, nz) -> int:

@@ -152,3 +152,33 @@ def test_oracle_diagnostics_semantics():
     dn = O.fluid_diagnostics64(g, "D3Q19", 6, 5, 4, speed_limit=1.0)
     assert np.isnan(dn[0]) and dn[3] == 1 and dn[4] == 1
     assert dn[2] == np.sqrt(np.delete(s2, 7)).max()
+
+
+def test_reactive_gradient_validation(lib):
+    nb = E.reactive_gradient_workspace_bytes("D3Q19", "float", 16, 12, 10, 20, 4)
+    cells = 16 * 12 * 10
+    up = lambda b: (b + 255) // 256 * 256  # noqa: E731
+    state = up(19 * cells * 4) + 2 * up(7 * cells * 4)
+    assert nb >= (6 + 4 + 2) * state  # 6 checkpoints, one segment of 4, two adjoint states
+    assert E.reactive_gradient_workspace_bytes("D2Q5", "float", 16, 12, 1, 20, 4) == 0
+    assert E.reactive_gradient_workspace_bytes("D3Q19", "float", 16, 12, 10, 20, 1) == 0
+    args = dict(rho0=A0, u0=A1, a0=A2, b0=A3, nx=16, ny=12, nz=10, tau=0.8, tau_c=0.7, k_react=0.1,
+                steps=20, interval=4, workspace=A4, workspace_bytes=nb, result=A4 + (1 << 30),
+                grad_a0=A4 + (2 << 30))
+
+    def call(**kw):
+        a = dict(args)
+        a.update(kw)
+        return E.reactive_gradient_async(a.pop("fl", "D3Q19"), a.pop("real", "float"), a.pop("op", "TRT"),
+                                         a.pop("obj", "mean_product"), **a)
+
+    assert call(a0=None) == E.cudaErrorInvalidDevicePointer
+    assert call(grad_a0=None) == E.cudaErrorInvalidDevicePointer
+    assert call(nz=0) == E.cudaErrorInvalidValue
+    assert call(op="MRT") == E.cudaErrorInvalidValue
+    assert call(tau=0.5) == E.cudaErrorInvalidValue
+    assert call(tau_c=0.4) == E.cudaErrorInvalidValue
+    assert call(workspace_bytes=nb - 1) == E.cudaErrorInvalidValue
+    assert call(steps=0) == E.cudaErrorInvalidValue
+    assert E.load().lbm_reactive_gradient_async(1, 0, 1, 7, A0, A1, A2, A3, 16, 12, 10, 0.8, 0.7, 0.1, 20, 4,
+                                                A4, nb, A4 + 8, A4 + 16, None, None) == E.cudaErrorInvalidValue
