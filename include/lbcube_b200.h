@@ -428,6 +428,38 @@ int lbm_step_diagnostics_async(int lattice, int precision, int collision,
     size_t z_extent, double omega, double speed_limit, double* partials, size_t partials_bytes,
     double* diagnostics, void* stream);
 
+/* ---- output ----------------------------------------------------------------
+ * Macroscopic fields for output, computed on the device from the populations
+ * as the reference's VTK writer computes them on the host (write_vtk,
+ * lattice_io.hpp:386-451; compute_macro_state): density[N], velocity[D*N]
+ * (component-major) and speed[N] = |u|, in the population precision. Any of
+ * the three may be null (not all). For D2Q5 / D3Q7 `density` receives the
+ * concentration and velocity / speed must be null. */
+int lbm_macro_fields_async(int lattice, int precision, const void* populations,
+    size_t x_extent, size_t y_extent, size_t z_extent, void* density, void* velocity,
+    void* speed, void* stream);
+
+/* Host functions (plain host pointers; no GPU work). Return 0 or one of: */
+#define LBM_IO_BAD_ARGUMENT 1
+#define LBM_IO_OPEN_FAILED 2
+#define LBM_IO_WRITE_FAILED 3
+#define LBM_IO_BAD_FILE 4
+#define LBM_IO_MISMATCH 5
+/* The legacy ASCII VTK file of lbm::write_vtk (lattice_io.hpp:386-451), byte
+ * for byte, from host copies of lbm_macro_fields_async's three outputs
+ * (dims 2 or 3; the reference names it lbm_<step, 6 digits>.vtk). */
+int lbm_write_vtk_legacy(const char* path, int dims, size_t x_extent, size_t y_extent,
+    size_t z_extent, size_t time_step, int precision, const void* density,
+    const void* velocity, const void* speed);
+/* Restart files (no reference counterpart): a 64-byte header (magic
+ * "LBCUBEP1", lattice, precision, extents, time step) and the raw [Q,Z,Y,X]
+ * populations. lbm_read_populations checks the header against the arguments
+ * (LBM_IO_MISMATCH) and returns the stored time step. */
+int lbm_write_populations(const char* path, int lattice, int precision, size_t x_extent,
+    size_t y_extent, size_t z_extent, size_t time_step, const void* populations);
+int lbm_read_populations(const char* path, int lattice, int precision, size_t x_extent,
+    size_t y_extent, size_t z_extent, size_t* time_step, void* populations);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -1,7 +1,8 @@
 """Builds the engine's shared library, lb-cube_b200/liblbcube_b200.so, in place.
 
 Every CUDA translation unit under csrc/ is compiled for sm_100a only
-(``-gencode arch=compute_100a,code=sm_100a``) in parallel, then linked into one
+(``-gencode arch=compute_100a,code=sm_100a``) in parallel (host-only .cpp units
+go through nvcc to the host compiler), then linked into one
 library that exports the C ABI declared in include/lbcube_b200.h. Collision
 code is built with ``--fmad=false`` so that multiply-adds are rounded exactly
 as LB-Cube's CPU path rounds them (no contraction into FMA); that is what makes
@@ -34,11 +35,16 @@ UNITS = {
     "stats.cu": ["--fmad=false"],
     "init.cu": ["--fmad=false"],
     "diag.cu": ["--fmad=false"],
+    "macro.cu": ["--fmad=false"],
 }
 
 
 def _sources():
-    return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+    return sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
+
+
+def _obj(src):
+    return os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
 
 
 def _headers():
@@ -56,7 +62,7 @@ def _stale(target, deps):
 
 
 def _compile(src, verbose):
-    obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+    obj = _obj(src)
     cmd = [NVCC, *COMMON, *ARCH, *UNITS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
@@ -72,7 +78,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     headers = _headers()
     todo, objs = [], []
     for src in _sources():
-        obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+        obj = _obj(src)
         objs.append(obj)
         if force or _stale(obj, [os.path.join(CSRC, src), *headers, __file__]):
             todo.append(src)

@@ -101,6 +101,10 @@ def _declare(lib):
         "lbm_adjoint_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp],
         "lbm_reactive_gradient_async": [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _sz, _sz, _sz,
                                         d, d, d, C.c_int, C.c_int, _vp, _sz, _vp, _vp, _vp, _vp],
+        "lbm_macro_fields_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp, _vp],
+        "lbm_write_vtk_legacy": [C.c_char_p, C.c_int, _sz, _sz, _sz, _sz, C.c_int, _vp, _vp, _vp],
+        "lbm_write_populations": [C.c_char_p, C.c_int, C.c_int, _sz, _sz, _sz, _sz, _vp],
+        "lbm_read_populations": [C.c_char_p, C.c_int, C.c_int, _sz, _sz, _sz, C.POINTER(C.c_size_t), _vp],
         "lbm_fluid_diagnostics_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, d, _vp, _sz, _vp, _vp],
         "lbm_step_diagnostics_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, d, _vp, _sz,
                                        _vp, _vp],
@@ -319,6 +323,45 @@ def reactive_gradient_async(fluid_lattice, real, collision, objective, rho0, u0,
         _ptr(rho0), _ptr(u0), _ptr(a0), _ptr(b0), nx, ny, nz, float(tau), float(tau_c), float(k_react),
         int(steps), int(interval), _ptr(workspace), int(workspace_bytes), _ptr(result), _ptr(grad_a0),
         _ptr(grad_b0), _stream(stream))
+
+
+def macro_fields_async(lattice, real, populations, nx, ny, nz, density, velocity=None, speed=None,
+                       stream=None) -> int:
+    """Density (concentration for scalars), velocity [D, ...] and |u| on the
+    device, in the population precision."""
+    return load().lbm_macro_fields_async(LATTICES[lattice], REALS[real_name(real)], _ptr(populations), nx,
+                                         ny, nz, _ptr(density), _ptr(velocity), _ptr(speed), _stream(stream))
+
+
+def _host(a):
+    """Host address of a contiguous numpy array or CPU tensor."""
+    if hasattr(a, "ctypes"):
+        assert a.flags.c_contiguous
+        return a.ctypes.data
+    assert not a.is_cuda and a.is_contiguous()
+    return a.data_ptr()
+
+
+def write_vtk_legacy(path, dims, nx, ny, nz, step, real, density, velocity, speed) -> int:
+    """The reference's legacy ASCII VTK file from host macroscopic fields."""
+    return load().lbm_write_vtk_legacy(os.fsencode(path), int(dims), nx, ny, nz, int(step),
+                                       REALS[real_name(real)], _host(density), _host(velocity), _host(speed))
+
+
+def write_populations(path, lattice, real, nx, ny, nz, step, populations) -> int:
+    return load().lbm_write_populations(os.fsencode(path), LATTICES[lattice], REALS[real_name(real)], nx, ny,
+                                        nz, int(step), _host(populations))
+
+
+def read_populations(path, lattice, real, nx, ny, nz, out):
+    """Fills host array ``out``; returns (code, stored time step)."""
+    st = C.c_size_t(0)
+    rc = load().lbm_read_populations(os.fsencode(path), LATTICES[lattice], REALS[real_name(real)], nx, ny,
+                                     nz, C.byref(st), _host(out))
+    return rc, st.value
+
+
+IO_ERRORS = {"bad_argument": 1, "open_failed": 2, "write_failed": 3, "bad_file": 4, "mismatch": 5}
 
 
 def diagnostics_partials_bytes(lattice, nx, ny, nz) -> int:

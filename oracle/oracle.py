@@ -58,6 +58,7 @@ def _bind(lib, prefix):
         sig["init_equilibrium"] = (C.c_int, [C.c_int, C.c_int, _dp, _dp, _vp, _sz, _sz, _sz])
     else:
         sig["reactive_stats"] = (C.c_int, [C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, C.c_double, _dp])
+        sig["write_vtk"] = (C.c_int, [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _sz])
     out = {}
     for name, (res, args) in sig.items():
         fn = getattr(lib, prefix + name)
@@ -202,6 +203,20 @@ def equilibrium(lattice, rho, u, dtype=np.float64, lib=ORACLE):
     out = np.zeros(Q_OF[lattice], dtype)
     _check(lib.equilibrium(LATTICES[lattice], _prec(dtype), float(rho), _dptr(uu), _ptr(out)), "equilibrium")
     return out
+
+
+def reference_vtk(f, lattice, nx, ny, nz, step, workdir):
+    """The reference build's write_vtk output for populations ``f`` (text), run
+    in ``workdir`` (it writes lbm_<step, 6 digits>.vtk to the current directory)."""
+    f = np.ascontiguousarray(f)
+    old = os.getcwd()
+    os.chdir(workdir)
+    try:
+        _check(REF.write_vtk(LATTICES[lattice], _prec(f.dtype), _ptr(f), nx, ny, nz, step), "write_vtk")
+        with open(f"lbm_{step:06d}.vtk", "rb") as fh:
+            return fh.read()
+    finally:
+        os.chdir(old)
 
 
 def init_equilibrium(lattice, rho, u, nx, ny, nz, dtype=np.float64):

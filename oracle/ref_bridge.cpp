@@ -10,6 +10,8 @@
 //   compute_reactive_stats         include/lattice_io.hpp:256-338
 //   compute_equilibrium            include/lattice_physics.hpp:267-290
 //   mrt transforms                 include/lattice_mrt.hpp:439-534, :617-892, :1023-1225
+//   write_vtk                      include/lattice_io.hpp:386-451 (writes lbm_<step>.vtk
+//                                  into the current directory, as the reference does)
 //
 // Enum codes (shared with oracle/lbm_oracle.h and the engine's C ABI):
 //   lattice: 0 D2Q9, 1 D3Q19, 2 D3Q27, 3 D2Q5, 4 D3Q7
@@ -189,9 +191,35 @@ void scalar_equilibrium(double conc, const double* u, void* out) {
   }
 }
 
+template <typename L, typename Real>
+int run_write_vtk(const void* f, std::size_t nx, std::size_t ny, std::size_t nz, std::size_t step) {
+  auto mem = make_memory<L, Real>(nx, ny, nz);
+  load(mem, f);
+  lbm::write_vtk<L, Real>(mem, nx, ny, nz, step);
+  return 0;
+}
+
+template <typename Real>
+int write_vtk_lattice(int lattice, const void* f, std::size_t nx, std::size_t ny, std::size_t nz,
+                      std::size_t step) {
+  switch (lattice) {
+    case 0: return run_write_vtk<lbm::D2Q9, Real>(f, nx, ny, nz, step);
+    case 1: return run_write_vtk<lbm::D3Q19, Real>(f, nx, ny, nz, step);
+    case 2: return run_write_vtk<lbm::D3Q27, Real>(f, nx, ny, nz, step);
+    default: return -1;
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+int ref_write_vtk(int lattice, int precision, const void* f, std::size_t nx, std::size_t ny,
+                  std::size_t nz, std::size_t step) {
+  if (precision == 0) return write_vtk_lattice<float>(lattice, f, nx, ny, nz, step);
+  if (precision == 1) return write_vtk_lattice<double>(lattice, f, nx, ny, nz, step);
+  return -1;
+}
 
 int ref_step(int lattice, int precision, int collision, const void* in, void* out,
              std::size_t nx, std::size_t ny, std::size_t nz, double omega, int steps) {

@@ -53,6 +53,26 @@ def c1_fingerprint(steps=1000, every=100, tau=0.6):
             "diagnostics_every_100": series}
 
 
+VTK_CASES = {"D2Q9": (7, 5, 1), "D3Q19": (4, 3, 2)}
+
+
+def make_vtk_golden():
+    """The reference's write_vtk text for seeded states (legacy ASCII VTK,
+    lattice_io.hpp:386-451), with the populations it was written from."""
+    import tempfile
+
+    inputs = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for lat, (nx, ny, nz) in VTK_CASES.items():
+            for k, (dn, dt) in enumerate((("float", np.float32), ("double", np.float64))):
+                f = U.random_state(lat, nx, ny, nz, dt, seed=300 + k, u_amp=0.05)
+                inputs[f"{lat}_{dn}"] = f
+                text = O.reference_vtk(f, lat, nx, ny, nz, 42 + k, tmp)
+                with open(os.path.join(HERE, f"vtk_{lat}_{dn}.vtk"), "wb") as fh:
+                    fh.write(text)
+    np.savez_compressed(os.path.join(HERE, "vtk_inputs.npz"), **inputs)
+
+
 def main():
     if not O.REF.available:
         raise SystemExit("reference build oracle/_ref/libref.so missing: run make -C oracle ref")
@@ -78,6 +98,8 @@ def main():
     with open(os.path.join(HERE, "c1_tgv64_fp64_bgk.json"), "w") as fh:
         json.dump(c1_fingerprint(), fh, indent=1)
     print("wrote the C1 fingerprint")
+    make_vtk_golden()
+    print("wrote the VTK fixtures")
 
 
 if __name__ == "__main__":
