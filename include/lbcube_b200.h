@@ -428,6 +428,33 @@ int lbm_step_diagnostics_async(int lattice, int precision, int collision,
     size_t z_extent, double omega, double speed_limit, double* partials, size_t partials_bytes,
     double* diagnostics, void* stream);
 
+/* ---- z-slab decomposition (multi-GPU) ---------------------------------------
+ * No reference counterpart. A periodic 3-D box (D3Q19 or D3Q27) cut into
+ * z-slabs, one per rank; each slab is a [Q, z_extent, Y, X] field in the
+ * reference layout. The populations that cross a slab face travel in face
+ * buffers of lbm_slab_face_elems() elements ([k, Y, X], the k populations with
+ * c_z = +1 (or -1) in ascending order):
+ *   halo_lo  c_z = +1 populations of the lower neighbour's top plane
+ *   halo_hi  c_z = -1 populations of the upper neighbour's bottom plane
+ *   send_lo  this step's c_z = -1 populations of plane 0 (the lower neighbour's halo_hi)
+ *   send_hi  this step's c_z = +1 populations of plane z_extent-1 (the upper one's halo_lo)
+ * lbm_step_slab_async steps planes [z_begin, z_end): plane 0 reads halo_lo
+ * and writes send_lo, the top plane reads halo_hi and writes send_hi; other
+ * planes touch no face buffer (those pointers may be null when the range
+ * does not include a face). A box stepped as slabs with the face buffers
+ * exchanged between steps is bit-identical to the box stepped whole.
+ * Requirements as the vectorised step: x_extent even for float, buffers
+ * aligned to 2 elements; D3Q27 double MRT / RLBM are not available.
+ * lbm_slab_pack_async fills send_lo / send_hi from a state (before the first
+ * exchange). */
+size_t lbm_slab_face_elems(int lattice, size_t x_extent, size_t y_extent);
+int lbm_step_slab_async(int lattice, int precision, int collision,
+    const void* current_populations, void* next_populations, size_t x_extent, size_t y_extent,
+    size_t z_extent, double omega, const void* halo_lo, const void* halo_hi, void* send_lo,
+    void* send_hi, size_t z_begin, size_t z_end, void* stream);
+int lbm_slab_pack_async(int lattice, int precision, const void* populations, size_t x_extent,
+    size_t y_extent, size_t z_extent, void* send_lo, void* send_hi, void* stream);
+
 /* ---- output ----------------------------------------------------------------
  * Macroscopic fields for output, computed on the device from the populations
  * as the reference's VTK writer computes them on the host (write_vtk,

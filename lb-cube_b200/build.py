@@ -36,6 +36,7 @@ UNITS = {
     "init.cu": ["--fmad=false"],
     "diag.cu": ["--fmad=false"],
     "macro.cu": ["--fmad=false"],
+    "slab.cu": ["--fmad=false"],
 }
 
 

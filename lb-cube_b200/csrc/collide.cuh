@@ -60,6 +60,17 @@ __device__ __forceinline__ void macro_state(const Real (&f)[L::Q], Real& rho, Re
     });
     u[d] = m / density;
   });
+  // The reference adds f_i * c_id for every i, so a non-finite population
+  // makes every velocity component NaN (0 * inf, inf / inf, or a NaN density),
+  // while finite populations give exactly the sums above (their zero terms
+  // change nothing). Skipping the zero terms loses that, so restore it; a
+  // finite density means every population is finite, so the common path only
+  // tests the density.
+  if (!isfinite(density)) {
+    bool bad = false;
+    static_for<L::Q>([&](auto I) { bad = bad || !isfinite(f[LB_I(I)]); });
+    if (bad) static_for<L::D>([&](auto D) { u[LB_I(D)] = Real(NAN); });
+  }
   rho = density;
 }
 

@@ -212,14 +212,43 @@ inline VecGrid make_vec_grid(const Grid& g, int V) {
   return v;
 }
 
+// ---- z-slab decomposition ---------------------------------------------------
+// A rank owns planes [0, nz) of its slab; the populations that cross a slab
+// face arrive in halo planes instead of the periodic wrap. Population i with
+// c_z = +1 is pulled from z - 1: at z = 0 it is read from halo_lo; c_z = -1 at
+// z = nz - 1 from halo_hi. A halo (or send) buffer holds the crossing
+// populations of one face in ascending i: [zslot, ny, nx].
+template <class L>
+__host__ __device__ constexpr int zslot(int i) {
+  int k = 0;
+  for (int j = 0; j < i; ++j) k += L::c[j][2] == L::c[i][2] ? 1 : 0;
+  return k;
+}
+template <class L>
+__host__ __device__ constexpr int zcount() {
+  int k = 0;
+  for (int j = 0; j < L::Q; ++j) k += L::c[j][2] > 0 ? 1 : 0;
+  return k;
+}
+
+template <class E>
+struct SlabArgs {
+  const E* halo_lo;  // c_z = +1 populations of the lower neighbour's top plane
+  const E* halo_hi;  // c_z = -1 populations of the upper neighbour's bottom plane
+  E* send_lo;        // this step's c_z = -1 populations of plane 0 (for the lower neighbour)
+  E* send_hi;        // this step's c_z = +1 populations of plane nz - 1 (for the upper one)
+  int z_begin;       // first plane of this launch (grid.y planes from here)
+};
+
 // Gathers the Q populations of V cells (x0 .. x0+V-1, row y, slice z) and
 // decodes them. All 32 lanes of every warp must call it (shuffles); inactive
 // lanes (x0 >= nx or y >= ny) load nothing and contribute nothing.
-template <class L, class S>
+template <class L, class S, bool SLAB = false>
 __device__ __forceinline__ void gather_vec(const typename S::elem* __restrict__ cur, const Grid& g,
                                            int x0, int y, int z, bool active,
                                            const typename S::Params& p,
-                                           typename S::compute (&f)[S::V][L::Q]) {
+                                           typename S::compute (&f)[S::V][L::Q],
+                                           const SlabArgs<typename S::elem>& slab = {}) {
   using E = typename S::elem;
   constexpr int V = S::V;
   const int lane = threadIdx.x & 31;
@@ -234,8 +263,17 @@ __device__ __forceinline__ void gather_vec(const typename S::elem* __restrict__ 
     constexpr int i = LB_I(I);
     constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
     const int sy = cy == 0 ? y : (cy > 0 ? ym : yp);
-    const int sz = cz == 0 ? z : (cz > 0 ? zm : zp);
-    const E* row = cur + plane * i + (size_t)(sz * g.ny + sy) * g.nx;
+    const E* row;
+    if constexpr (SLAB && cz > 0) {
+      row = z == 0 ? slab.halo_lo + (size_t)(zslot<L>(i) * g.ny + sy) * g.nx
+                   : cur + plane * i + (size_t)((z - 1) * g.ny + sy) * g.nx;
+    } else if constexpr (SLAB && cz < 0) {
+      row = z == g.nz - 1 ? slab.halo_hi + (size_t)(zslot<L>(i) * g.ny + sy) * g.nx
+                          : cur + plane * i + (size_t)((z + 1) * g.ny + sy) * g.nx;
+    } else {
+      const int sz = cz == 0 ? z : (cz > 0 ? zm : zp);
+      row = cur + plane * i + (size_t)(sz * g.ny + sy) * g.nx;
+    }
     using R = typename S::compute;
     R val[V];
     if (active) {
@@ -263,20 +301,28 @@ __device__ __forceinline__ void gather_vec(const typename S::elem* __restrict__ 
   });
 }
 
-template <class L, class S>
+template <class L, class S, bool SLAB = false>
 __device__ __forceinline__ void store_vec(typename S::elem* __restrict__ nxt, const Grid& g, int x0,
                                           int y, int z, const typename S::Params& p,
-                                          const typename S::compute (&f)[S::V][L::Q]) {
+                                          const typename S::compute (&f)[S::V][L::Q],
+                                          const SlabArgs<typename S::elem>& slab = {}) {
   using E = typename S::elem;
   constexpr int V = S::V;
   const size_t plane = (size_t)g.plane;
   const size_t cell = (size_t)(z * g.ny + y) * g.nx + x0;
   static_for<L::Q>([&](auto I) {
     constexpr int i = LB_I(I);
+    constexpr int cz = L::c[i][2];
     typename S::compute col[V];
 #pragma unroll
     for (int j = 0; j < V; ++j) col[j] = f[j][i];
-    store_word<E, V>(nxt + plane * i + cell, S::template encode_word<L, i>(col, p));
+    const RowWord<E, V> w = S::template encode_word<L, i>(col, p);
+    store_word<E, V>(nxt + plane * i + cell, w);
+    if constexpr (SLAB && cz > 0) {  // leaves through the top face
+      if (z == g.nz - 1) store_word<E, V>(slab.send_hi + (size_t)(zslot<L>(i) * g.ny + y) * g.nx + x0, w);
+    } else if constexpr (SLAB && cz < 0) {  // leaves through the bottom face
+      if (z == 0) store_word<E, V>(slab.send_lo + (size_t)(zslot<L>(i) * g.ny + y) * g.nx + x0, w);
+    }
   });
 }
 
@@ -284,12 +330,15 @@ __device__ __forceinline__ void store_vec(typename S::elem* __restrict__ nxt, co
 // block into partials[block_linear() * kDiagPartials ..]. In the pull scheme
 // the populations a thread writes are exactly the next buffer's populations of
 // its own cells, so this costs no memory traffic. Native storage only.
-template <class L, class S, int CT, bool DIAG = false>
+// SLAB: one launch over planes [slab.z_begin, slab.z_begin + gridDim.y) of a
+// z-slab, with halo planes at the slab faces (see SlabArgs).
+template <class L, class S, int CT, bool DIAG = false, bool SLAB = false>
 __global__ void __launch_bounds__(kThreads)
     fluid_step_vec_kernel(const typename S::elem* __restrict__ cur,
                           typename S::elem* __restrict__ nxt, VecGrid vg,
                           typename S::compute omega, typename S::compute omega_minus,
-                          typename S::Params p, double* __restrict__ partials = nullptr) {
+                          typename S::Params p, double* __restrict__ partials = nullptr,
+                          SlabArgs<typename S::elem> slab = {}) {
   using R = typename S::compute;
   constexpr int V = S::V;
   const Grid& g = vg.g;
@@ -297,10 +346,10 @@ __global__ void __launch_bounds__(kThreads)
   const int xb = blockIdx.x - yb * vg.xblocks;
   const int x0 = (xb * vg.tx + (int)(threadIdx.x % vg.tx)) * V;
   const int y = yb * vg.ty + (int)(threadIdx.x / vg.tx);
-  const int z = blockIdx.y;
+  const int z = SLAB ? slab.z_begin + (int)blockIdx.y : (int)blockIdx.y;
   const bool active = x0 < g.nx && y < g.ny;
   R f[V][L::Q];
-  gather_vec<L, S>(cur, g, x0, y < g.ny ? y : 0, z, active, p, f);
+  gather_vec<L, S, SLAB>(cur, g, x0, y < g.ny ? y : 0, z, active, p, f, slab);
   if constexpr (DIAG) {
     static_assert(std::is_same_v<typename S::elem, R>, "diagnostics need native storage");
     DiagAcc acc;
@@ -316,7 +365,7 @@ __global__ void __launch_bounds__(kThreads)
     if (!active) return;
 #pragma unroll
     for (int j = 0; j < V; ++j) S::template collide_cell<L, CT>(f[j], omega, omega_minus, p);
-    store_vec<L, S>(nxt, g, x0, y, z, p, f);
+    store_vec<L, S, SLAB>(nxt, g, x0, y, z, p, f, slab);
   }
 }
 

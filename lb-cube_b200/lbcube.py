@@ -101,6 +101,9 @@ def _declare(lib):
         "lbm_adjoint_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp],
         "lbm_reactive_gradient_async": [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _sz, _sz, _sz,
                                         d, d, d, C.c_int, C.c_int, _vp, _sz, _vp, _vp, _vp, _vp],
+        "lbm_step_slab_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp, _vp, _vp, _sz,
+                                _sz, _vp],
+        "lbm_slab_pack_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
         "lbm_macro_fields_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp, _vp],
         "lbm_write_vtk_legacy": [C.c_char_p, C.c_int, _sz, _sz, _sz, _sz, C.c_int, _vp, _vp, _vp],
         "lbm_write_populations": [C.c_char_p, C.c_int, C.c_int, _sz, _sz, _sz, _sz, _vp],
@@ -115,6 +118,8 @@ def _declare(lib):
         fn.argtypes = args
     lib.lbm_stats_partials_bytes.restype = C.c_size_t
     lib.lbm_stats_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
+    lib.lbm_slab_face_elems.restype = C.c_size_t
+    lib.lbm_slab_face_elems.argtypes = [C.c_int, _sz, _sz]
     lib.lbm_reactive_gradient_workspace_bytes.restype = C.c_size_t
     lib.lbm_reactive_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, _sz, _sz, _sz, C.c_int, C.c_int]
     lib.lbm_diagnostics_partials_bytes.restype = C.c_size_t
