@@ -17,8 +17,11 @@ roofline achieved HBM GB/s of the step kernel = 152 B/LU x cells / mean launch
 restatement when the reference build is absent) on a bounded sample of the
 same workload and prints the same metric.
 
-Multi-GPU (torchrun): each rank runs the same box on its own GPU (replicas,
-weak scaling); value is the sum over ranks with the time taken as the max.
+Multi-GPU (torchrun, N ranks): one periodic 256 x 256 x 256N box cut into
+z-slabs of 256^3, one per GPU (weak scaling); every step exchanges the face
+populations with the two neighbours over NCCL point-to-point, overlapped with
+the interior planes (lb-cube_b200/slab.py). value = cells of all ranks x
+steps / the max over ranks of the timed region.
 """
 from __future__ import annotations
 
@@ -75,7 +78,6 @@ def config_dict():
         "lattice": "D3Q19", "collision": "TRT", "storage": "fp32",
         "nx": NX, "ny": NY, "nz": NZ, "tau": TAU,
         "l2": f"inputs larger than L2 ({19 * 4 * NX * NY * NZ / 1e9:.2f} GB per population buffer); no flush",
-        "parallelism": "replicas (one box per GPU)",
     }
 
 
@@ -543,7 +545,22 @@ def run_engine(args, rank, world, local_rank):
     f = make_initial_state(torch, E, dev)
     storage = args.storage
     bytes_per_lu = BYTES_PER_LU if storage == "fp32" else BYTES_PER_LU // 2
-    if storage == "fp32":
+    slabs = None
+    launches_per_step = 1
+    if storage == "fp32" and world > 1:
+        # one periodic NX x NY x (NZ * world) box cut into z-slabs, one per rank;
+        # the face populations cross NVLink (NCCL point-to-point) every step
+        import slab
+
+        slabs = slab.SlabDomain(torch, "D3Q19", "float", "TRT", NX, NY, NZ * world, omega, rank, world, dev)
+        exchange = slab.DistributedExchange(dist)
+        slabs.prime(f, exchange)
+        launches_per_step = len(sum(slabs.ranges(), []))
+
+        def step(cur, nxt):
+            slabs.step(cur, nxt, exchange)
+            return 0
+    elif storage == "fp32":
         def step(cur, nxt):
             return E.launch_step_gpu("D3Q19", "float", "TRT", cur, nxt, NX, NY, NZ, omega)
     else:
@@ -575,6 +592,8 @@ def run_engine(args, rank, world, local_rank):
     for _ in range(args.steps):
         rc = step(f, g)
         f, g = g, f
+    if slabs is not None:
+        slabs.finish()
     t1.record(stream)
     torch.cuda.synchronize()
     E.check(rc)
@@ -604,6 +623,8 @@ def run_engine(args, rank, world, local_rank):
         for _ in range(args.steps):
             rc = step(f, g)
             f, g = g, f
+        if slabs is not None:
+            slabs.finish()
         host.copy_(f, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -620,10 +641,21 @@ def run_engine(args, rank, world, local_rank):
                        "field copied back; copies amortised over K"}
         if storage != "fp32":
             e2e["note"] = e2e["note"].replace("lbm_launch_step_gpu_d3q19_float_trt", "lbm_step_shifted_async")
+        elif slabs is not None:
+            e2e["note"] = e2e["note"].replace("lbm_launch_step_gpu_d3q19_float_trt",
+                                              "lbm_step_slab_async + NCCL face exchange")
         del host
 
     if rank != 0:
         return None
+    if world == 1:
+        parallelism = "single GPU"
+    elif slabs is not None:
+        parallelism = (f"z-slab decomposition of one {NX}x{NY}x{NZ * world} periodic box over {world} GPUs "
+                       f"({NZ} planes each), NCCL point-to-point face exchange every step, overlapped with "
+                       f"the interior planes")
+    else:
+        parallelism = f"{world} independent replicas (16-bit storage has no slab path)"
     peak, peak_kind = measured_hbm_peak()
     traffic = committed_traffic(f"d3q19_float_trt_{NX}") if storage == "fp32" else None
     variants = accuracy = fp16_store = adjoint = adjoint_reactive = mixing = None
@@ -650,12 +682,12 @@ def run_engine(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if storage == "fp32" else f"{storage} storage, f32 compute",
-        "data": "synthetic", "config": dict(config_dict(), storage=storage),
+        "data": "synthetic", "config": dict(config_dict(), storage=storage, parallelism=parallelism),
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved_gbs / peak, 4),
                      "traffic": traffic, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_per_lu * cells},
-        "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps,
+        "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps * launches_per_step,
         "fp16_store": fp16_store, "adjoint": adjoint, "adjoint_reactive": adjoint_reactive,
         "reactive_mixing": mixing,
         "variants": variants, "accuracy": accuracy,

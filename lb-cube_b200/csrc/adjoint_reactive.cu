@@ -19,11 +19,15 @@
 //   lf_k  += (c_k - u) . ubar / rho            (u = j / rho of f^{n+1}(x))
 // then the fluid adjoint (adjoint.cuh) on the updated lf; abar, bbar and the
 // fluid mu scatter to the pull sources. dJ/dk gathers sigma dS/dk, dJ/dw_c
-// gathers sum_i la_i (g_eq_i(C_A) - a_i) + lb_i (g_eq_i(C_B) - b_i). The
-// linearisation point uses the cell's pre-collision (rho, u), equal to the
+// gathers sum_i la_i (g_eq_i(C_A) - a_i) + lb_i (g_eq_i(C_B) - b_i).
+// Two kernels per adjoint step: the reaction part reads the advecting velocity
+// u^{n+1} that the forward pass stored with each state (exactly the value the
+// forward reaction used) and writes ubar; the fluid part adds the ubar term at
+// the linearisation point of its own pre-collision (rho, u), equal to the
 // post-collision ones up to rounding (BGK and TRT conserve mass and momentum).
-// The source derivatives are evaluated in FP64 at the step's inputs on the
-// branch the forward step took.
+// Splitting keeps each kernel's registers, and so its occupancy, close to the
+// plain fluid adjoint's. The source derivatives are evaluated in FP64 at the
+// step's inputs on the branch the forward step took.
 //
 // Objectives (final state N, means over the N_c cells):
 //   LBM_OBJECTIVE_MEAN_PRODUCT  <C> = <A0> - <C_A^N>   (C = A0 - A; transport
@@ -33,6 +37,7 @@
 #include <algorithm>
 
 #include "adjoint.cuh"
+#include "adr.cuh"
 #include "cells.cuh"
 #include "collide.cuh"
 #include "common.cuh"
@@ -80,88 +85,113 @@ struct ReactiveParams {
 // Per-block FP64 slots of the reactive adjoint: dJ/dk, dJ/dtau, dJ/domega_c.
 constexpr int kReactiveSlots = 3;
 
-template <class FL, class Real, int CT>
+// Reaction part of adjoint step n at every cell x: from the pulled A^n, B^n,
+// lambda_A^{n+1}, lambda_B^{n+1} at x and the advecting velocity u^{n+1}(x)
+// (stored by the forward pass), scatter abar and bbar to lambda^n_A, lambda^n_B,
+// write ubar(x) = dJ/du^{n+1}(x) for the fluid part, and add the block's
+// dJ/dk and dJ/domega_c to its slots.
+template <class FL, class Real>
 __global__ void __launch_bounds__(kThreads)
-    reactive_adjoint_step_kernel(const Real* __restrict__ fn, const Real* __restrict__ an,
-                                 const Real* __restrict__ bn, const Real* __restrict__ lf_next,
-                                 const Real* __restrict__ la_next, const Real* __restrict__ lb_next,
-                                 Real* __restrict__ lf, Real* __restrict__ la,
-                                 Real* __restrict__ lb, Grid g, ReactiveParams rp,
-                                 double* __restrict__ slots) {
+    reaction_adjoint_kernel(const Real* __restrict__ an, const Real* __restrict__ bn,
+                            const Real* __restrict__ u_next, const Real* __restrict__ la_next,
+                            const Real* __restrict__ lb_next, Real* __restrict__ la,
+                            Real* __restrict__ lb, Real* __restrict__ ubar_out, Grid g,
+                            ReactiveParams rp, double* __restrict__ slots) {
   using SL = typename ScalarOf<FL>::type;
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
-  double acc[kReactiveSlots] = {0.0, 0.0, 0.0};
+  double acc[2] = {0.0, 0.0};
   if (active) {
     const Neighbours n = neighbours(g, x, y, z);
     const int cell = (z * g.ny + y) * g.nx + x;
-    Real gv[FL::Q], rho, u[FL::D];
+    const size_t plane = (size_t)g.plane;
+    Real u[FL::D];
+    static_for<FL::D>([&](auto D) { u[LB_I(D)] = __ldg(u_next + plane * LB_I(D) + cell); });
+    Real ga[SL::Q], gb[SL::Q], lA[SL::Q], lB[SL::Q];
+    gather<SL>(an, g, n, x, y, z, ga);
+    gather<SL>(bn, g, n, x, y, z, gb);
+    load_cell<SL>(la_next, g, cell, lA);
+    load_cell<SL>(lb_next, g, cell, lB);
+    const Real ca = concentration<SL>(ga), cb = concentration<SL>(gb);
+    double dsa, dsb, dsk;
+    reaction_source_grad<Real>(ca, cb, Real(rp.k), dsa, dsb, dsk);
+    const Real oc = Real(rp.omega_c);
+    const Real inv_cs2 = Real(1.0 / SL::cs2);
+    Real sigma = Real(0), ea = Real(0), eb = Real(0), doc = Real(0), ubar[FL::D];
+    static_for<FL::D>([&](auto D) { ubar[LB_I(D)] = Real(0); });
+    static_for<SL::Q>([&](auto I) {
+      constexpr int i = LB_I(I);
+      constexpr double wd = SL::w[i];
+      const Real w = Real(wd);
+      const Real e = w * (Real(1) + c_dot<SL, i>(u) * inv_cs2);
+      sigma += w * (lA[i] + lB[i]);
+      ea += lA[i] * e;
+      eb += lB[i] * e;
+      doc += lA[i] * (geq<SL, i>(ca, u) - ga[i]) + lB[i] * (geq<SL, i>(cb, u) - gb[i]);
+      const Real s = w * (ca * lA[i] + cb * lB[i]);
+      static_for<FL::D>([&](auto D) {
+        constexpr int c = SL::c[i][LB_I(D)];
+        if constexpr (c > 0) ubar[LB_I(D)] += s;
+        if constexpr (c < 0) ubar[LB_I(D)] -= s;
+      });
+    });
+    static_for<FL::D>([&](auto D) { ubar_out[plane * LB_I(D) + cell] = ubar[LB_I(D)] * (oc * inv_cs2); });
+    acc[0] = (double)sigma * dsk;
+    acc[1] = (double)doc;
+    const Real sa = Real((double)sigma * dsa), sb = Real((double)sigma * dsb);
+    Real ma[SL::Q], mb[SL::Q];
+    static_for<SL::Q>([&](auto I) {
+      constexpr int j = LB_I(I);
+      ma[j] = (Real(1) - oc) * lA[j] + oc * ea + sa;
+      mb[j] = (Real(1) - oc) * lB[j] + oc * eb + sb;
+    });
+    scatter<SL>(la, g, n, x, y, z, ma);
+    scatter<SL>(lb, g, n, x, y, z, mb);
+  }
+  __shared__ double tot[2];
+  block_sum_to<2>(acc, tot);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    slots[block_linear() * kReactiveSlots + 0] += tot[0];
+    slots[block_linear() * kReactiveSlots + 2] += tot[1];
+  }
+}
+
+// Fluid part of adjoint step n: lambda_f^{n+1}(x, k) gains
+// (c_k - u) . ubar(x) / rho (u = j / rho of the cell), then the fluid adjoint
+// of adjoint.cuh; dJ/dtau to the block's slot.
+template <class FL, class Real, int CT>
+__global__ void __launch_bounds__(kThreads)
+    coupled_fluid_adjoint_kernel(const Real* __restrict__ fn, const Real* __restrict__ lf_next,
+                                 const Real* __restrict__ ubar_in, Real* __restrict__ lf, Grid g,
+                                 AdjointParams ap, double* __restrict__ slots) {
+  int x, y, z;
+  const bool active = cell_of(g, x, y, z);
+  double dtau = 0.0;
+  if (active) {
+    const Neighbours n = neighbours(g, x, y, z);
+    const int cell = (z * g.ny + y) * g.nx + x;
+    const size_t plane = (size_t)g.plane;
+    Real gv[FL::Q], lv[FL::Q], mu[FL::Q], rho, u[FL::D], ub[FL::D];
     gather<FL>(fn, g, n, x, y, z, gv);
-    macro_state<FL>(gv, rho, u);
-
-    // ---- reaction step --------------------------------------------------
-    Real ubar[FL::D];
-    {
-      Real ga[SL::Q], gb[SL::Q], lA[SL::Q], lB[SL::Q];
-      gather<SL>(an, g, n, x, y, z, ga);
-      gather<SL>(bn, g, n, x, y, z, gb);
-      load_cell<SL>(la_next, g, cell, lA);
-      load_cell<SL>(lb_next, g, cell, lB);
-      const Real ca = concentration<SL>(ga), cb = concentration<SL>(gb);
-      double dsa, dsb, dsk;
-      reaction_source_grad<Real>(ca, cb, Real(rp.k), dsa, dsb, dsk);
-      const Real oc = Real(rp.omega_c);
-      const Real inv_cs2 = Real(1.0 / SL::cs2);
-      Real sigma = Real(0), ea = Real(0), eb = Real(0), doc = Real(0);
-      static_for<FL::D>([&](auto D) { ubar[LB_I(D)] = Real(0); });
-      static_for<SL::Q>([&](auto I) {
-        constexpr int i = LB_I(I);
-        constexpr double wd = SL::w[i];
-        const Real w = Real(wd);
-        const Real e = w * (Real(1) + c_dot<SL, i>(u) * inv_cs2);
-        sigma += w * (lA[i] + lB[i]);
-        ea += lA[i] * e;
-        eb += lB[i] * e;
-        doc += lA[i] * (geq<SL, i>(ca, u) - ga[i]) + lB[i] * (geq<SL, i>(cb, u) - gb[i]);
-        const Real s = w * (ca * lA[i] + cb * lB[i]);
-        static_for<FL::D>([&](auto D) {
-          constexpr int c = SL::c[i][LB_I(D)];
-          if constexpr (c > 0) ubar[LB_I(D)] += s;
-          if constexpr (c < 0) ubar[LB_I(D)] -= s;
-        });
-      });
-      static_for<FL::D>([&](auto D) { ubar[LB_I(D)] *= oc * inv_cs2; });
-      acc[0] = (double)sigma * dsk;
-      acc[2] = (double)doc;
-      const Real sa = Real((double)sigma * dsa), sb = Real((double)sigma * dsb);
-      Real ma[SL::Q], mb[SL::Q];
-      static_for<SL::Q>([&](auto I) {
-        constexpr int j = LB_I(I);
-        ma[j] = (Real(1) - oc) * lA[j] + oc * ea + sa;
-        mb[j] = (Real(1) - oc) * lB[j] + oc * eb + sb;
-      });
-      scatter<SL>(la, g, n, x, y, z, ma);
-      scatter<SL>(lb, g, n, x, y, z, mb);
-    }
-
-    // ---- fluid step, with the velocity's adjoint added at this cell ------
-    Real lv[FL::Q], mu[FL::Q];
     load_cell<FL>(lf_next, g, cell, lv);
+    static_for<FL::D>([&](auto D) { ub[LB_I(D)] = __ldg(ubar_in + plane * LB_I(D) + cell); });
+    macro_state<FL>(gv, rho, u);
     Real uub = Real(0);
-    static_for<FL::D>([&](auto D) { uub += u[LB_I(D)] * ubar[LB_I(D)]; });
+    static_for<FL::D>([&](auto D) { uub += u[LB_I(D)] * ub[LB_I(D)]; });
     const Real inv_rho = Real(1) / rho;
     static_for<FL::Q>([&](auto I) {
       constexpr int k = LB_I(I);
-      lv[k] += (c_dot<FL, k>(ubar) - uub) * inv_rho;
+      lv[k] += (c_dot<FL, k>(ub) - uub) * inv_rho;
     });
-    acc[1] = fluid_adjoint_cell<FL, Real, CT>(gv, lv, rho, u, rp.fluid, mu);
+    dtau = fluid_adjoint_cell<FL, Real, CT>(gv, lv, rho, u, ap, mu);
     scatter<FL>(lf, g, n, x, y, z, mu);
   }
-  __shared__ double tot[kReactiveSlots];
-  block_sum_to<kReactiveSlots>(acc, tot);
+  double v[1] = {dtau};
+  __shared__ double tot;
+  block_sum_to<1>(v, &tot);
   __syncthreads();
-  if (threadIdx.x < kReactiveSlots)
-    slots[block_linear() * kReactiveSlots + threadIdx.x] += tot[threadIdx.x];
+  if (threadIdx.x == 0) slots[block_linear() * kReactiveSlots + 1] += tot;
 }
 
 // Seeds lambda^N = dJ/d(f^N, A^N, B^N) and writes the block's FP64 share of J.
@@ -237,34 +267,47 @@ __global__ void __launch_bounds__(kThreads)
   grad[cell] = s;
 }
 
-template <class FL, class Real, int CT>
-cudaError_t launch_reactive_adjoint(const Real* const (&st)[3], const Real* const (&ln)[3],
-                                    Real* const (&l)[3], const Grid& g, const ReactiveParams& rp,
-                                    double* slots, cudaStream_t s) {
-  reactive_adjoint_step_kernel<FL, Real, CT><<<grid_dims(g), kThreads, 0, s>>>(
-      st[0], st[1], st[2], ln[0], ln[1], ln[2], l[0], l[1], l[2], g, rp, slots);
+template <class FL, class Real>
+cudaError_t launch_reactive_adjoint(int collision, const Real* fn, const Real* an, const Real* bn,
+                                    const Real* u_next, const Real* lf_next, const Real* la_next,
+                                    const Real* lb_next, Real* lf, Real* la, Real* lb, Real* ubar,
+                                    const Grid& g, const ReactiveParams& rp, double* slots,
+                                    cudaStream_t s) {
+  reaction_adjoint_kernel<FL, Real><<<grid_dims(g), kThreads, 0, s>>>(
+      an, bn, u_next, la_next, lb_next, la, lb, ubar, g, rp, slots);
+  if (collision == kBGK)
+    coupled_fluid_adjoint_kernel<FL, Real, kBGK><<<grid_dims(g), kThreads, 0, s>>>(
+        fn, lf_next, ubar, lf, g, rp.fluid, slots);
+  else
+    coupled_fluid_adjoint_kernel<FL, Real, kTRT><<<grid_dims(g), kThreads, 0, s>>>(
+        fn, lf_next, ubar, lf, g, rp.fluid, slots);
   return cudaGetLastError();
 }
 
 struct ReactiveLayout {
-  size_t ffield, sfield, state;  // bytes: fluid field, one scalar field, one (f, A, B) state
+  size_t ffield, sfield, ufield, state;  // bytes: fluid, one scalar, velocity; one state
   long long ckpts, blocks;
-  size_t off_ckpt, off_seg, off_lam, off_slots, off_j, off_part, off_stats, total;
+  size_t off_ckpt, off_seg, off_lam, off_ubar, off_slots, off_j, off_part, off_stats, total;
 };
 
-inline ReactiveLayout reactive_layout(int FQ, int SQ, size_t elem, const Grid& g, int steps,
+// A stored state n holds f^n, A^n, B^n and the velocity u^n that advected the
+// reaction step producing it; an adjoint state holds lambda_f, lambda_A,
+// lambda_B (its velocity slot unused).
+inline ReactiveLayout reactive_layout(int FQ, int SQ, int D, size_t elem, const Grid& g, int steps,
                                       int interval) {
   ReactiveLayout l{};
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
   l.ffield = up((size_t)FQ * g.plane * elem);
   l.sfield = up((size_t)SQ * g.plane * elem);
-  l.state = l.ffield + 2 * l.sfield;
+  l.ufield = up((size_t)D * g.plane * elem);
+  l.state = l.ffield + 2 * l.sfield + l.ufield;
   l.ckpts = (steps + interval - 1) / interval + 1;
   l.blocks = g.blocks();
   l.off_ckpt = 0;
   l.off_seg = l.off_ckpt + (size_t)l.ckpts * l.state;
   l.off_lam = l.off_seg + (size_t)interval * l.state;
-  l.off_slots = l.off_lam + 2 * l.state;
+  l.off_ubar = l.off_lam + 2 * l.state;
+  l.off_slots = l.off_ubar + l.ufield;
   l.off_j = l.off_slots + up((size_t)l.blocks * kReactiveSlots * sizeof(double));
   l.off_part = l.off_j + up((size_t)l.blocks * sizeof(double));
   l.off_stats = l.off_part + up((size_t)l.blocks * kStatSums * sizeof(double));
@@ -286,11 +329,13 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
     Real* f;
     Real* a;
     Real* b;
+    Real* u;
   };
   auto at = [&](size_t off) {
     char* p = ws + off;
     return State{reinterpret_cast<Real*>(p), reinterpret_cast<Real*>(p + lay.ffield),
-                 reinterpret_cast<Real*>(p + lay.ffield + lay.sfield)};
+                 reinterpret_cast<Real*>(p + lay.ffield + lay.sfield),
+                 reinterpret_cast<Real*>(p + lay.ffield + 2 * lay.sfield)};
   };
   auto ckpt = [&](long long i) { return at(lay.off_ckpt + (size_t)i * lay.state); };
   auto seg = [&](long long i) { return at(lay.off_seg + (size_t)i * lay.state); };
@@ -300,10 +345,10 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
   double* partials = reinterpret_cast<double*>(ws + lay.off_part);
   double* stats = reinterpret_cast<double*>(ws + lay.off_stats);
   cudaError_t err;
+  Real* ubar = reinterpret_cast<Real*>(ws + lay.off_ubar);
   auto step = [&](const State& c, const State& n) {
-    return (cudaError_t)lbm_fluid_reaction_ab_async(FL::id, prec, collision, c.f, n.f, c.a, n.a,
-                                                    c.b, n.b, g.nx, g.ny, g.nz, omega, omega_c, k,
-                                                    nullptr, 0, s);
+    return fluid_reaction_with_velocity<FL, Real>(collision, c.f, n.f, c.a, n.a, c.b, n.b, n.u, g,
+                                                  Real(omega), Real(omega_c), Real(k), s);
   };
 
   // forward: equilibrium initial state, checkpoints every `interval` steps,
@@ -365,13 +410,11 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
     }
     for (int n = n1 - 1; n >= n0; --n) {
       const State sn = n == n0 ? ckpt(kk) : seg(n - n0);
+      const State sn1 = n + 1 == n1 ? ckpt(kk + 1) : seg(n + 1 - n0);  // holds u^{n+1}
       const State& ln = lam[(n + 1) % 2];
       const State& l = lam[n % 2];
-      const Real* const st[3] = {sn.f, sn.a, sn.b};
-      const Real* const lnp[3] = {ln.f, ln.a, ln.b};
-      Real* const lp[3] = {l.f, l.a, l.b};
-      err = collision == kBGK ? launch_reactive_adjoint<FL, Real, kBGK>(st, lnp, lp, g, rp, slots, s)
-                              : launch_reactive_adjoint<FL, Real, kTRT>(st, lnp, lp, g, rp, slots, s);
+      err = launch_reactive_adjoint<FL, Real>(collision, sn.f, sn.a, sn.b, sn1.u, ln.f, ln.a, ln.b,
+                                              l.f, l.a, l.b, ubar, g, rp, slots, s);
       if (err != cudaSuccess) return err;
     }
   }
@@ -420,8 +463,8 @@ cudaError_t reactive_dispatch(int lattice, int collision, int objective, const v
       (objective != LBM_OBJECTIVE_MEAN_PRODUCT && objective != LBM_OBJECTIVE_SEGREGATION) ||
       !(tau > 0.5) || !(tau_c > 0.5))
     return cudaErrorInvalidValue;
-  const ReactiveLayout lay =
-      reactive_layout(fluid_q(lattice), scalar_q(lattice), sizeof(Real), g, steps, interval);
+  const ReactiveLayout lay = reactive_layout(fluid_q(lattice), scalar_q(lattice), dims,
+                                             sizeof(Real), g, steps, interval);
   if (ws_bytes < lay.total) return cudaErrorInvalidValue;
   char* w = static_cast<char*>(ws);
 #define LBCUBE_REACTIVE(FL)                                                                        \
@@ -452,7 +495,7 @@ extern "C" size_t lbm_reactive_gradient_workspace_bytes(int fluid_lattice, int p
     return 0;
   if (steps < 1 || checkpoint_interval < 2) return 0;
   if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return 0;
-  return reactive_layout(fluid_q(fluid_lattice), scalar_q(fluid_lattice),
+  return reactive_layout(fluid_q(fluid_lattice), scalar_q(fluid_lattice), dims,
                          precision == LBM_DOUBLE ? 8 : 4, g, steps, checkpoint_interval)
       .total;
 }

@@ -6,8 +6,9 @@
 //                       the reaction driver sequences them
 //                       (src/simulate_reaction.cpp:518-543), optionally with
 //                       the reactive-statistics partial sums of the new fields.
-#include "collide.cuh"
+#include "adr.cuh"
 #include "cells.cuh"
+#include "collide.cuh"
 #include "common.cuh"
 #include "reduce.cuh"
 #include "../../include/lbcube_b200.h"
@@ -66,13 +67,15 @@ __global__ void __launch_bounds__(kThreads)
 // recomputed from the post-collision fluid populations: they are bit for bit
 // the values the reference's separate reaction launch reads back from the new
 // fluid buffer at this cell, so the result equals the two-launch sequence.
-template <class FL, class Real, int CT, bool STATS>
+// UOUT: also store that velocity, u_out[d * N + cell] (the reactive adjoint
+// keeps it with each stored state).
+template <class FL, class Real, int CT, bool STATS, bool UOUT = false>
 __global__ void __launch_bounds__(kThreads)
     fluid_reaction_kernel(const Real* __restrict__ cur_f, Real* __restrict__ nxt_f,
                           const Real* __restrict__ cur_a, Real* __restrict__ nxt_a,
                           const Real* __restrict__ cur_b, Real* __restrict__ nxt_b, Grid g,
                           Real omega, Real omega_minus, Real omega_c, Real k,
-                          double* __restrict__ partials) {
+                          double* __restrict__ partials, Real* __restrict__ u_out = nullptr) {
   using SL = typename ScalarOf<FL>::type;
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
@@ -85,6 +88,9 @@ __global__ void __launch_bounds__(kThreads)
     collide<FL, Real, CT>(f, omega, omega_minus);
     store_cell<FL>(nxt_f, g, cell, f);
     fluid_velocity<FL>(f, u);
+    if constexpr (UOUT) {
+      static_for<FL::D>([&](auto D) { u_out[(size_t)g.plane * LB_I(D) + cell] = u[LB_I(D)]; });
+    }
     Real a[SL::Q], b[SL::Q];
     gather<SL>(cur_a, g, n, x, y, z, a);
     gather<SL>(cur_b, g, n, x, y, z, b);
@@ -178,6 +184,38 @@ cudaError_t launch_fluid_reaction(const Real* cur_f, Real* nxt_f, const Real* cu
   }
   return cudaGetLastError();
 }
+
+// The fused step with the advecting velocity stored (no statistics), for the
+// reactive adjoint's forward and recomputation passes. Buffers are checked by
+// the caller (they are slices of its workspace).
+template <class FL, class Real>
+cudaError_t fluid_reaction_with_velocity(int collision, const Real* cur_f, Real* nxt_f,
+                                         const Real* cur_a, Real* nxt_a, const Real* cur_b,
+                                         Real* nxt_b, Real* u_out, const Grid& g, Real omega,
+                                         Real omega_c, Real k, cudaStream_t s) {
+  if (collision == kBGK) {
+    fluid_reaction_kernel<FL, Real, kBGK, false, true><<<grid_dims(g), kThreads, 0, s>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, nullptr, u_out);
+  } else if (collision == kTRT) {
+    fluid_reaction_kernel<FL, Real, kTRT, false, true><<<grid_dims(g), kThreads, 0, s>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, trt_omega_minus<Real>(omega), omega_c,
+        k, nullptr, u_out);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+#define LBCUBE_FRV(FL, R)                                                                     \
+  template cudaError_t fluid_reaction_with_velocity<FL, R>(                                   \
+      int, const R*, R*, const R*, R*, const R*, R*, R*, const Grid&, R, R, R, cudaStream_t);
+LBCUBE_FRV(D2Q9, float)
+LBCUBE_FRV(D2Q9, double)
+LBCUBE_FRV(D3Q19, float)
+LBCUBE_FRV(D3Q19, double)
+LBCUBE_FRV(D3Q27, float)
+LBCUBE_FRV(D3Q27, double)
+#undef LBCUBE_FRV
 
 template <class FL, class Real>
 cudaError_t fused_by_collision(int collision, const void* cf, void* nf, const void* ca, void* na,
