@@ -68,12 +68,13 @@ __device__ __forceinline__ void reaction_source_grad(Real a, Real b, Real k, dou
   } else {
     const double d = B - A;
     const double e = exp(-K * d);
-    const double N = A * d * e, D = B - A * e, ap = N / D;
+    const double inv = 1.0 / (B - A * e);  // 1 / D
+    const double ap = A * d * e * inv;      // N / D
     const double dna = e * (d - A + A * d * K), dnb = A * e * (1.0 - d * K), dnk = -A * d * d * e;
     const double dda = -e * (1.0 + A * K), ddb = 1.0 + A * K * e, ddk = A * d * e;
-    dsa = (dna - ap * dda) / D - 1.0;
-    dsb = (dnb - ap * ddb) / D;
-    dsk = (dnk - ap * ddk) / D;
+    dsa = (dna - ap * dda) * inv - 1.0;
+    dsb = (dnb - ap * ddb) * inv;
+    dsk = (dnk - ap * ddk) * inv;
   }
 }
 
@@ -160,8 +161,9 @@ __global__ void __launch_bounds__(kThreads)
 // Fluid part of adjoint step n: lambda_f^{n+1}(x, k) gains
 // (c_k - u) . ubar(x) / rho (u = j / rho of the cell), then the fluid adjoint
 // of adjoint.cuh; dJ/dtau to the block's slot.
+// Five blocks of 128 per SM (96 registers instead of 115).
 template <class FL, class Real, int CT>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 5)
     coupled_fluid_adjoint_kernel(const Real* __restrict__ fn, const Real* __restrict__ lf_next,
                                  const Real* __restrict__ ubar_in, Real* __restrict__ lf, Grid g,
                                  AdjointParams ap, double* __restrict__ slots) {
