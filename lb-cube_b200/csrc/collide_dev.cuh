@@ -210,4 +210,146 @@ __device__ __forceinline__ void collide_dev(float (&v)[L::Q], float omega, float
   });
 }
 
+// ---- MRT on deviation variables (D2Q9, D3Q19) -----------------------------------
+// The reference MRT (collide_mrt_d2q9, lattice_mrt.hpp:586-603; collide_mrt_d3q19,
+// :971-1009) relaxes the orthogonal moments m = M f towards m_eq and maps back
+// with M^-1 = M^T D^-1 (D = diag |M_k|^2). In deviation form, with
+// mu_k = S (m_k - rho0 m_k(rest)) = sum_j M_kj w_j v_j (m(rest) = M w, the moments
+// of f = w), the post-collision deviations are
+//   v_i = (1 / w_i) sum_k (M_ki / D_k) mu_post_k,
+// mu_post = mu for conserved moments, mu_eq for moments relaxed with rate 1, and
+// mu - s (mu - mu_eq) otherwise, where mu_eq is S (m_eq - rho0 m(rest)) of the
+// reference's equilibrium moments written with R = S rho and j_v = S j = R u:
+//   D2Q9  (:548-569)  e: -2 dv + 3 R u.u   eps: dv - 3 R u.u   q: -j_v
+//                     p_xx: R (ux^2 - uy^2)  p_xy: R ux uy; rates 1.63, 1.14, 1.92, omega
+//   D3Q19 (:908-947)  e: -11 dv + 19 R u.u  eps: 3 dv - 5.5 R u.u  q: -2/3 j_v
+//                     3p_xx: 3 R (2ux^2 - uy^2 - uz^2)  p_ww: R (uy^2 - uz^2)
+//                     p_xy, p_yz, p_xz: R u_a u_b; rates: omega on 9-13, 1 on the
+//                     rest, ghost modes 14-18 with equilibrium 0 (:981-1001)
+// Only the moments with a rate other than 1 are formed from v; algebraically
+// this is the reference operator, evaluated in FP32 on the stored deviations.
+template <class L>
+struct DevMrt;
+
+// kinds: 0 conserved, 1 relaxed with rate 1 (to mu_eq), 2 relaxed with rate s,
+// 3 relaxed with rate 1 to an equilibrium of 0
+template <>
+struct DevMrt<D2Q9> {
+  using Mx = Mrt9;
+  static constexpr int kind[9] = {0, 2, 2, 0, 2, 0, 2, 2, 2};
+  __device__ __forceinline__ static float rate(int k, float omega) {
+    return k == 1 ? 1.63f : k == 2 ? 1.14f : (k == 4 || k == 6) ? 1.92f : omega;
+  }
+  template <int k>
+  __device__ __forceinline__ static float eq(float dv, float R, const float (&u)[2], const float (&j)[2],
+                                             float usq) {
+    if constexpr (k == 1) return fmaf(3.0f * R, usq, -2.0f * dv);
+    if constexpr (k == 2) return fmaf(-3.0f * R, usq, dv);
+    if constexpr (k == 4) return -j[0];
+    if constexpr (k == 6) return -j[1];
+    if constexpr (k == 7) return R * (u[0] * u[0] - u[1] * u[1]);
+    if constexpr (k == 8) return R * u[0] * u[1];
+    return 0.0f;
+  }
+};
+
+template <>
+struct DevMrt<D3Q19> {
+  using Mx = Mrt19;
+  static constexpr int kind[19] = {0, 1, 1, 0, 1, 0, 1, 0, 1, 2, 2, 2, 2, 2, 3, 3, 3, 3, 3};
+  __device__ __forceinline__ static float rate(int, float omega) { return omega; }
+  template <int k>
+  __device__ __forceinline__ static float eq(float dv, float R, const float (&u)[3], const float (&j)[3],
+                                             float usq) {
+    if constexpr (k == 1) return fmaf(19.0f * R, usq, -11.0f * dv);
+    if constexpr (k == 2) return fmaf(-5.5f * R, usq, 3.0f * dv);
+    if constexpr (k == 4) return (-2.0f / 3.0f) * j[0];
+    if constexpr (k == 6) return (-2.0f / 3.0f) * j[1];
+    if constexpr (k == 8) return (-2.0f / 3.0f) * j[2];
+    if constexpr (k == 9) return 3.0f * R * (2.0f * u[0] * u[0] - u[1] * u[1] - u[2] * u[2]);
+    if constexpr (k == 10) return R * (u[1] * u[1] - u[2] * u[2]);
+    if constexpr (k == 11) return R * u[0] * u[1];
+    if constexpr (k == 12) return R * u[1] * u[2];
+    if constexpr (k == 13) return R * u[0] * u[2];
+    return 0.0f;
+  }
+};
+
+// Index of the momentum component a conserved moment k > 0 carries (3 -> x,
+// 5 -> y, 7 -> z in both bases).
+__host__ __device__ constexpr int conserved_axis(int k) { return (k - 3) / 2; }
+
+template <class L, int FMT>
+__device__ __forceinline__ void collide_dev_mrt(float (&v)[L::Q], float omega, float rho0) {
+  using MR = DevMrt<L>;
+  using Mx = typename MR::Mx;
+  constexpr float S = Codec<FMT>::S;
+  constexpr int K = WeightClasses<L>::count;
+  float sv[K], sj[K][L::D];
+  static_for<K>([&](auto k) {
+    sv[LB_I(k)] = 0.0f;
+    static_for<L::D>([&](auto D) { sj[LB_I(k)][LB_I(D)] = 0.0f; });
+  });
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr int k = WeightClasses<L>::of(i);
+    sv[k] += v[i];
+    static_for<L::D>([&](auto D) {
+      constexpr int c = L::c[i][LB_I(D)];
+      if constexpr (c > 0) sj[k][LB_I(D)] += v[i];
+      if constexpr (c < 0) sj[k][LB_I(D)] -= v[i];
+    });
+  });
+  float dv = 0.0f, j[L::D];
+  static_for<L::D>([&](auto D) { j[LB_I(D)] = 0.0f; });
+  static_for<K>([&](auto kk) {
+    constexpr int k = LB_I(kk);
+    constexpr float w = (float)L::w[WeightClasses<L>::first(k)];
+    dv = fmaf(w, sv[k], dv);
+    static_for<L::D>([&](auto D) { j[LB_I(D)] = fmaf(w, sj[k][LB_I(D)], j[LB_I(D)]); });
+  });
+  const float R = fmaf(S, rho0, dv);
+  const float inv = __frcp_rn(R);
+  float u[L::D];
+  static_for<L::D>([&](auto D) { u[LB_I(D)] = j[LB_I(D)] * inv; });
+  float usq = 0.0f;
+  static_for<L::D>([&](auto D) { usq = fmaf(u[LB_I(D)], u[LB_I(D)], usq); });
+  // post-collision deviation moments
+  float mp[L::Q];
+  static_for<L::Q>([&](auto KK) {
+    constexpr int k = LB_I(KK);
+    constexpr int kind = MR::kind[k];
+    if constexpr (kind == 0) {
+      if constexpr (k == 0) mp[k] = dv;
+      else mp[k] = j[conserved_axis(k)];
+    } else if constexpr (kind == 1) {
+      mp[k] = MR::template eq<k>(dv, R, u, j, usq);
+    } else if constexpr (kind == 2) {
+      float m = 0.0f;
+      static_for<L::Q>([&](auto JJ) {
+        constexpr int jj = LB_I(JJ);
+        constexpr int coef = Mx::M.m[k][jj];
+        constexpr float cw = (float)(coef * L::w[jj]);
+        if constexpr (coef != 0) m = fmaf(cw, v[jj], m);
+      });
+      const float e = MR::template eq<k>(dv, R, u, j, usq);
+      mp[k] = fmaf(-MR::rate(k, omega), m - e, m);
+    } else {
+      mp[k] = 0.0f;
+    }
+  });
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    float acc = 0.0f;
+    static_for<L::Q>([&](auto KK) {
+      constexpr int k = LB_I(KK);
+      constexpr int coef = Mx::M.m[k][i];
+      constexpr int kind = MR::kind[k];
+      constexpr float cb = (float)((double)coef / ((double)Mx::M.norm[k] * L::w[i]));
+      if constexpr (coef != 0 && kind != 3) acc = fmaf(cb, mp[k], acc);
+    });
+    v[i] = acc;
+  });
+}
+
 }  // namespace lbcube

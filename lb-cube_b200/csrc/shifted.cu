@@ -21,15 +21,17 @@ namespace lbcube {
 // Cells per thread of the 16-bit kernels (8-byte words).
 constexpr int kShiftedCells = 4;
 
-// BGK and TRT collide on the stored deviations; MRT and RLBM decode to f.
-template <int FMT, int CT>
-using ShiftedPolicy = std::conditional_t<CT == kBGK || CT == kTRT, DevStorage<FMT, kShiftedCells>,
-                                         ShiftedStorage<FMT, kShiftedCells>>;
+// BGK, TRT and the D2Q9 / D3Q19 MRT collide on the stored deviations; D3Q27
+// MRT and RLBM decode to f and run the reference operator.
+template <class L, int FMT, int CT>
+using ShiftedPolicy =
+    std::conditional_t<CT == kBGK || CT == kTRT || (CT == kMRT && L::Q != 27),
+                       DevStorage<FMT, kShiftedCells>, ShiftedStorage<FMT, kShiftedCells>>;
 
 template <class L, int FMT, int CT>
 cudaError_t launch_shifted_step(const void* cur, void* nxt, size_t nx, size_t ny, size_t nz,
                                 float omega, float rho0, cudaStream_t stream) {
-  using S = ShiftedPolicy<FMT, CT>;
+  using S = ShiftedPolicy<L, FMT, CT>;
   Grid g;
   cudaError_t err = validate_domain(cur == nullptr || nxt == nullptr, 1, 1, 1, L::D, nx, ny, nz, g);
   if (err != cudaSuccess) return err;

@@ -164,8 +164,10 @@ struct DevStorage {
   template <class L, int CT>
   __device__ __forceinline__ static void collide_cell(compute (&v)[L::Q], compute omega,
                                                       compute omega_minus, const Params& p) {
-    static_assert(CT == kBGK || CT == kTRT, "deviation-space collision is BGK / TRT");
-    collide_dev<L, CT, FMT>(v, omega, omega_minus, p.rho0);
+    static_assert(CT == kBGK || CT == kTRT || (CT == kMRT && L::Q != 27),
+                  "deviation-space collision is BGK, TRT, or D2Q9 / D3Q19 MRT");
+    if constexpr (CT == kMRT) collide_dev_mrt<L, FMT>(v, omega, p.rho0);
+    else collide_dev<L, CT, FMT>(v, omega, omega_minus, p.rho0);
   }
 };
 
