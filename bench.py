@@ -241,6 +241,17 @@ def run_variants(torch, E, dev, f32, peak, fp32_ms):
                                                                     part, nb, diag, speed_limit=0.2),
                      f32.clone(), g, 200, 10)
     rec("D3Q19 TRT fp32 + diagnostics every step", ms, 152, vs_plain_step=round(fp32_ms / ms, 3))
+    count = [0]
+
+    def every10(a, b):  # the drivers' usual cadence: diagnostics on every 10th step
+        count[0] += 1
+        if count[0] % 10 == 0:
+            return E.step_diagnostics_async("D3Q19", "float", "TRT", a, b, NX, NY, NZ, omega, part, nb, diag,
+                                            speed_limit=0.2)
+        return E.launch_step_gpu("D3Q19", "float", "TRT", a, b, NX, NY, NZ, omega)
+
+    ms = _time_steps(torch, every10, f32.clone(), g, 200, 10)
+    rec("D3Q19 TRT fp32 + diagnostics every 10th step", ms, 152, vs_plain_step=round(fp32_ms / ms, 3))
     del part, diag
     h = torch.empty(f32.shape, dtype=torch.int16, device=dev)
     hg = torch.empty_like(h)
@@ -667,16 +678,20 @@ def run_engine(args, rank, world, local_rank):
         adjoint = run_adjoint_cost(torch, E, dev)
         adjoint_reactive = run_reactive_adjoint_cost(torch, E, dev)
         mixing = run_reactive_mixing(torch, E, dev)
-        # the fastest 16-bit format meeting the 1e-3 velocity error bar for TRT
-        ok = [v for v in variants if v["variant"].startswith("D3Q19 TRT ") and v["variant"][10:] in FORMATS16
-              and accuracy["by_collision"]["TRT"][v["variant"][10:]] <= 1e-3]
-        if ok:
-            best = max(ok, key=lambda v: v["mlups"])
-            fmt = best["variant"][10:]
-            fp16_store = {"format": FORMAT_NOTE[fmt], "mlups": best["mlups"], "hbm_frac": best["hbm_frac"],
-                          "speedup_vs_fp32": best["speedup_vs_fp32"],
-                          "velocity_rel_l2_2000_steps": accuracy["by_collision"]["TRT"][fmt],
-                          "velocity_rel_l2_2000_steps_mrt": accuracy["by_collision"]["MRT"][fmt]}
+        # per operator: the fastest 16-bit format meeting the 1e-3 velocity error
+        # bar, with its speed-up over FP32 storage of the same operator
+        fp16_store = {"bar": "velocity rel-L2 <= 1e-3 after 2000 steps vs the FP64 run", "by_collision": {}}
+        for op in ("TRT", "MRT"):
+            pre = f"D3Q19 {op} "
+            ok = [v for v in variants if v["variant"].startswith(pre) and v["variant"][len(pre):] in FORMATS16
+                  and accuracy["by_collision"][op][v["variant"][len(pre):]] <= 1e-3]
+            if ok:
+                best = max(ok, key=lambda v: v["mlups"])
+                fmt = best["variant"][len(pre):]
+                fp16_store["by_collision"][op] = {
+                    "format": FORMAT_NOTE[fmt], "mlups": best["mlups"], "hbm_frac": best["hbm_frac"],
+                    "speedup_vs_fp32": best["speedup_vs_fp32"],
+                    "velocity_rel_l2_2000_steps": accuracy["by_collision"][op][fmt]}
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
