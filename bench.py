@@ -62,6 +62,9 @@ def parse():
                     help="population storage of the timed run (16-bit ones are shifted)")
     ap.add_argument("--size", type=int, default=256,
                     help="cube edge; smaller sizes are for profiling captures only")
+    ap.add_argument("--kernel-survey", action="store_true",
+                    help="launch every kernel family a few times at 128^3 (1024^2 for 2-D), time each with "
+                         "CUDA events and print one JSON line; the command the per-kernel ncu summary captures")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="run only the adjoint cost measurement (D3Q19 BGK FP32, --size cube, --steps "
                          "steps, checkpoint every min(100, steps)) and print it; for profiling captures")
@@ -541,6 +544,118 @@ def run_reactive_mixing(torch, E, dev, n=1024, steps=20000, every=10, tau=0.6):
     return out
 
 
+def run_kernel_survey(torch, E, dev, n=128, reps=3):
+    """Every kernel family once per rep at n^3 (D2Q9 at (8n)^2), timed with CUDA
+    events; algorithmic bytes per launch give the achieved GB/s."""
+    import slab
+
+    f32, f64 = torch.float32, torch.float64
+    cells = n ** 3
+    om, omc, k = 1.0 / TAU, 1.0 / 0.55, 0.002
+    out = []
+
+    def timed(name, bytes_per_launch, launch):
+        for _ in range(2):
+            E.check(launch())
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(reps):
+            E.check(launch())
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / reps
+        out.append({"kernel": name, "ms": round(ms, 4), "bytes": int(bytes_per_launch),
+                    "gbs": round(bytes_per_launch / (ms * 1e-3) / 1e9, 1)})
+
+    rho = torch.ones((n, n, n), dtype=f32, device=dev)
+    u = 0.02 * torch.randn((3, n, n, n), dtype=f32, device=dev, generator=torch.Generator(device=dev).manual_seed(1))
+    f = torch.empty((19, n, n, n), dtype=f32, device=dev)
+    g = torch.empty_like(f)
+    timed("init_equilibrium D3Q19 f32", cells * (4 * 4 + 76), lambda: E.init_equilibrium_async("D3Q19", "float", rho, u, f, n, n, n))
+    for op in ("TRT", "BGK", "MRT", "RLBM"):
+        timed(f"step D3Q19 f32 {op}", cells * 152, lambda op=op: E.step_async("D3Q19", "float", op, f, g, n, n, n, om))
+    fd, gd = f.double(), torch.empty((19, n, n, n), dtype=f64, device=dev)
+    timed("step D3Q19 f64 BGK", cells * 304, lambda: E.step_async("D3Q19", "double", "BGK", fd, gd, n, n, n, om))
+    del fd, gd
+    f27 = torch.empty((27, n, n, n), dtype=f32, device=dev)
+    E.check(E.init_equilibrium_async("D3Q27", "float", rho, u, f27, n, n, n))
+    g27 = torch.empty_like(f27)
+    timed("step D3Q27 f32 BGK", cells * 216, lambda: E.step_async("D3Q27", "float", "BGK", f27, g27, n, n, n, om))
+    del f27, g27
+    h = torch.empty((19, n, n, n), dtype=torch.int16, device=dev)
+    hg = torch.empty_like(h)
+    timed("encode_shifted D3Q19 q15s", cells * (76 + 38), lambda: E.encode_shifted_async("D3Q19", "q15s", "float", f, h, n, n, n))
+    for fmt, op in (("q15s", "TRT"), ("f16s", "TRT"), ("f16s", "MRT"), ("e3m12s", "TRT")):
+        E.check(E.encode_shifted_async("D3Q19", fmt, "float", f, h, n, n, n))
+        timed(f"step_shifted D3Q19 {fmt} {op}", cells * 76,
+              lambda fmt=fmt, op=op: E.step_shifted_async("D3Q19", fmt, op, h, hg, n, n, n, om))
+    timed("decode_shifted D3Q19 f16s", cells * (38 + 76), lambda: E.decode_shifted_async("D3Q19", "f16s", "float", h, g, n, n, n))
+    del h, hg
+    # scalars and the coupled step
+    a = torch.empty((7, n, n, n), dtype=f32, device=dev)
+    b = torch.empty_like(a)
+    E.check(E.init_equilibrium_async("D3Q7", "float", rho, u, a, n, n, n))
+    E.check(E.init_equilibrium_async("D3Q7", "float", rho * 0.5, u, b, n, n, n))
+    a2, b2 = torch.empty_like(a), torch.empty_like(b)
+    timed("scalar_step D3Q19/D3Q7 f32", cells * (56 + 76), lambda: E.scalar_step_async("D3Q19", "float", a, a2, f, n, n, n, omc))
+    timed("reaction_ab D3Q19/D3Q7 f32", cells * (112 + 76), lambda: E.reaction_ab_async("D3Q19", "float", a, a2, b, b2, f, n, n, n, omc, k))
+    pb = E.stats_partials_bytes("D3Q19", n, n, n)
+    part = torch.empty(pb, dtype=torch.uint8, device=dev)
+    st = torch.empty(8, dtype=f64, device=dev)
+    timed("fluid_reaction D3Q19 f32 TRT", cells * 264,
+          lambda: E.fluid_reaction_ab_async("D3Q19", "float", "TRT", f, g, a, a2, b, b2, n, n, n, om, omc, k))
+    timed("fluid_reaction D3Q19 f32 TRT + stats", cells * 264,
+          lambda: E.fluid_reaction_ab_async("D3Q19", "float", "TRT", f, g, a, a2, b, b2, n, n, n, om, omc, k, part, pb))
+    timed("reactive_stats D3Q7 f32 (2 passes)", cells * 56,
+          lambda: E.reactive_stats_async("D3Q7", "float", a, b, n, n, n, k, part, pb, st))
+    dpb = E.diagnostics_partials_bytes("D3Q19", n, n, n)
+    dpart = torch.empty(dpb, dtype=torch.uint8, device=dev)
+    dg = torch.empty(5, dtype=f64, device=dev)
+    timed("fluid_diagnostics D3Q19 f32 (2 passes)", cells * 76,
+          lambda: E.fluid_diagnostics_async("D3Q19", "float", f, n, n, n, dpart, dpb, dg))
+    timed("step_diagnostics D3Q19 f32 TRT", cells * 152,
+          lambda: E.step_diagnostics_async("D3Q19", "float", "TRT", f, g, n, n, n, om, dpart, dpb, dg))
+    mr, mu, ms = torch.empty(cells, dtype=f32, device=dev), torch.empty((3, cells), dtype=f32, device=dev), \
+        torch.empty(cells, dtype=f32, device=dev)
+    timed("macro_fields D3Q19 f32", cells * (76 + 20), lambda: E.macro_fields_async("D3Q19", "float", f, n, n, n, mr, mu, ms))
+    # adjoint steps
+    lam, lam2 = torch.zeros_like(f), torch.zeros_like(f)
+    timed("adjoint_step D3Q19 f32 TRT", cells * 228,
+          lambda: E.adjoint_step_async("D3Q19", "float", "TRT", f, lam, lam2, n, n, n, TAU))
+    del lam, lam2
+    # the slab step: one rank, faces exchanged locally
+    d = slab.SlabDomain(torch, "D3Q19", "float", "TRT", n, n, n, om, 0, 1, dev)
+    d.pack(f)
+    ex = slab.LocalExchange([d])
+    ex.exchange_all()
+
+    def slab_step():
+        d.compute(f, g)
+        ex.exchange_all()
+        return 0
+    timed("slab step D3Q19 f32 TRT (3 launches + face copies)", cells * 152, slab_step)
+    del a, b, a2, b2, part, dpart, mr, mu, ms
+    # 2-D: D2Q9 MRT + two D2Q5 at (8n)^2
+    m2 = 8 * n
+    c2 = m2 * m2
+    rho2 = torch.ones((m2, m2), dtype=f32, device=dev)
+    u2 = 0.02 * torch.randn((2, m2, m2), dtype=f32, device=dev, generator=torch.Generator(device=dev).manual_seed(2))
+    q = torch.empty((9, m2, m2), dtype=f32, device=dev)
+    q2 = torch.empty_like(q)
+    E.check(E.init_equilibrium_async("D2Q9", "float", rho2, u2, q, m2, m2, 1))
+    timed("step D2Q9 f32 MRT", c2 * 72, lambda: E.step_async("D2Q9", "float", "MRT", q, q2, m2, m2, 1, om))
+    s5 = [torch.empty((5, m2, m2), dtype=f32, device=dev) for _ in range(4)]
+    for t in s5:
+        E.check(E.init_equilibrium_async("D2Q5", "float", rho2 * 0.5, u2, t, m2, m2, 1))
+    timed("fluid_reaction D2Q9 f32 MRT", c2 * 152,
+          lambda: E.fluid_reaction_ab_async("D2Q9", "float", "MRT", q, q2, s5[0], s5[1], s5[2], s5[3], m2, m2, 1, om, omc, k))
+    torch.cuda.synchronize()
+    return {"kernel_survey": out, "size": f"{n}^3 (2-D: {m2}^2)", "reps": reps,
+            "note": "ms = CUDA-event mean over reps after 2 warm-ups; bytes = algorithmic bytes per launch"}
+
+
 def run_engine(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -790,6 +905,16 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
+        return
+    if args.kernel_survey:
+        import torch
+
+        import lbcube as E
+
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        E.load()
+        print(json.dumps(run_kernel_survey(torch, E, dev, n=args.size if args.size != 256 else 128)), flush=True)
         return
     if args.adjoint_only:
         import torch

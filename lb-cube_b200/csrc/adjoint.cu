@@ -18,7 +18,7 @@
 namespace lbcube {
 
 template <class L, class Real, int CT>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 5)
     adjoint_step_kernel(const Real* __restrict__ fn, const Real* __restrict__ lam_next,
                         Real* __restrict__ lam, Grid g, AdjointParams ap,
                         double* __restrict__ dtau_slots) {

@@ -49,51 +49,57 @@ inline AdjointParams make_params(int collision, double tau) {
 // mu = J_C(g)^T lambda at one cell, from the pulled pre-collision populations
 // gv (with their rho and u) and lambda^{n+1} at the cell (lv). Returns the
 // cell's lambda . dC/dtau (the tau-derivative of the step, evaluated per cell
-// in the population precision).
+// in the population precision). One pass over the opposite pairs (i, o):
+// f_eq_i = E + O, f_eq_o = E - O with E = w rho (1 + 4.5 (c.u)^2 - 1.5 u.u) and
+// O = 3 w rho c.u, so every sum needs only the pair's own values.
 template <class L, class Real, int CT>
 __device__ __forceinline__ double fluid_adjoint_cell(const Real (&gv)[L::Q], const Real (&lv)[L::Q],
                                                      Real rho, const Real (&u)[L::D],
                                                      const AdjointParams& ap, Real (&mu)[L::Q]) {
   const Real usq = u_dot_u<L>(u);
-  Real eq[L::Q];
-  equilibria<L>(rho, u, usq, eq);
   const Real om = Real(ap.omega), omm = Real(ap.omega_minus);
-  // weights of f_eq in C, and the tau-derivative of the step
-  Real Lam[L::Q];
-  Real dt1 = Real(0), dt2 = Real(0);
+  const Real base = Real(1) - Real(1.5) * usq;
+  Real dt1 = Real(0), dt2 = Real(0), W = Real(0), Aq = Real(0), B[L::D];
+  static_for<L::D>([&](auto D) { B[LB_I(D)] = Real(0); });
   static_for<L::Q>([&](auto I) {
     constexpr int i = LB_I(I);
     constexpr int o = L::opp[i];
-    if constexpr (CT == kBGK) {
-      Lam[i] = om * lv[i];
-      dt1 += lv[i] * (eq[i] - gv[i]);
-    } else {
-      const Real lp = Real(0.5) * (lv[i] + lv[o]), lm = Real(0.5) * (lv[i] - lv[o]);
-      Lam[i] = om * lp + omm * lm;
-      dt1 += lv[i] * (Real(0.5) * ((gv[i] + gv[o]) - (eq[i] + eq[o])));  // g+ - f_eq+
-      dt2 += lv[i] * (Real(0.5) * ((gv[i] - gv[o]) - (eq[i] - eq[o])));  // g- - f_eq-
+    constexpr double wd = L::w[i];
+    const Real wr = Real(wd) * rho;
+    if constexpr (i == o) {  // rest population: f_eq = w rho (1 - 1.5 u.u)
+      if constexpr (CT == kBGK) dt1 += lv[i] * (wr * base - gv[i]);
+      else dt1 += lv[i] * (gv[i] - wr * base);
+      W += Real(wd) * (om * lv[i]);
+    } else if constexpr (i < o) {
+      const Real cu = c_dot<L, i>(u);
+      const Real E = wr * (base + Real(4.5) * cu * cu), O = Real(3) * wr * cu;
+      Real sum, dif;  // Lam_i + Lam_o, Lam_i - Lam_o
+      if constexpr (CT == kBGK) {
+        sum = om * (lv[i] + lv[o]);
+        dif = om * (lv[i] - lv[o]);
+        dt1 += lv[i] * ((E + O) - gv[i]) + lv[o] * ((E - O) - gv[o]);
+      } else {
+        const Real lp = lv[i] + lv[o], lm = lv[i] - lv[o];
+        sum = om * lp;
+        dif = omm * lm;
+        dt1 += lp * (Real(0.5) * (gv[i] + gv[o]) - E);  // (lambda_i + lambda_o) (g+ - f_eq+)
+        dt2 += lm * (Real(0.5) * (gv[i] - gv[o]) - O);  // (lambda_i - lambda_o) (g- - f_eq-)
+      }
+      W += Real(wd) * sum;
+      Aq += Real(wd) * sum * cu * cu;
+      // w (Lam_i (3 + 9 cu) - Lam_o (3 - 9 cu)) = w (3 (Lam_i - Lam_o) + 9 cu (Lam_i + Lam_o))
+      const Real s = Real(wd) * (Real(3) * dif + Real(9) * cu * sum);
+      static_for<L::D>([&](auto D) {
+        constexpr int c = L::c[i][LB_I(D)];
+        if constexpr (c > 0) B[LB_I(D)] += s;
+        if constexpr (c < 0) B[LB_I(D)] -= s;
+      });
     }
   });
   const double dtau = CT == kBGK ? (double)dt1 * ap.domega_dtau
                                  : -((double)dt1 * ap.domega_dtau + (double)dt2 * ap.domega_minus_dtau);
   // A = sum_i w_i Lam_i (1 + 1.5 u.u) - 4.5 sum_i w_i Lam_i (c_i.u)^2
   // B = sum_i w_i Lam_i (3 + 9 c_i.u) c_i - 3 u sum_i w_i Lam_i
-  Real W = Real(0), Aq = Real(0), B[L::D];
-  static_for<L::D>([&](auto D) { B[LB_I(D)] = Real(0); });
-  static_for<L::Q>([&](auto I) {
-    constexpr int i = LB_I(I);
-    constexpr double wd = L::w[i];
-    const Real cu = c_dot<L, i>(u);
-    const Real wl = Real(wd) * Lam[i];
-    W += wl;
-    Aq += wl * cu * cu;
-    const Real s = wl * (Real(3) + Real(9) * cu);
-    static_for<L::D>([&](auto D) {
-      constexpr int c = L::c[i][LB_I(D)];
-      if constexpr (c > 0) B[LB_I(D)] += s;
-      if constexpr (c < 0) B[LB_I(D)] -= s;
-    });
-  });
   const Real A = W * (Real(1) + Real(1.5) * usq) - Real(4.5) * Aq;
   static_for<L::D>([&](auto D) { B[LB_I(D)] -= Real(3) * W * u[LB_I(D)]; });
   const Real a = CT == kBGK ? Real(1) - om : Real(1) - Real(0.5) * (om + omm);
