@@ -356,7 +356,8 @@ int lbm_adjoint_step_async(int lattice, int precision, int collision, const void
  *                               compute_reactive_stats (lattice_io.hpp:318-337)
  * result (device, 4 doubles): J, dJ/dk, dJ/dtau, dJ/dtau_c (omega = 1/tau,
  * omega_c = 1/tau_c rounded to the population precision, as the launchers
- * take them); grad_a0 = dJ/da0 and, if non-null, grad_b0 = dJ/db0 ([Z,Y,X]).
+ * take them); grad_a0 = dJ/da0 and, if non-null, grad_b0 = dJ/db0 ([Z,Y,X]) and
+ * grad_u0 = dJ/du0 ([D,Z,Y,X]: through f^0, A^0 and B^0).
  * Workspace of lbm_reactive_gradient_workspace_bytes bytes, not overlapping
  * the inputs or outputs. Cost: about 2 forward runs + 1 adjoint run. */
 #define LBM_OBJECTIVE_MEAN_PRODUCT 0
@@ -367,7 +368,7 @@ int lbm_reactive_gradient_async(int fluid_lattice, int precision, int collision,
     const void* rho0, const void* u0, const void* a0, const void* b0, size_t x_extent,
     size_t y_extent, size_t z_extent, double tau, double tau_c, double k_react, int steps,
     int checkpoint_interval, void* workspace, size_t workspace_bytes, double* result,
-    void* grad_a0, void* grad_b0, void* stream);
+    void* grad_a0, void* grad_b0, void* grad_u0, void* stream);
 
 /* Allocation-free form of lbm_reactive_stats_async. No counterpart in the
  * reference. For callers that cannot allocate device memory, e.g. a plugin or

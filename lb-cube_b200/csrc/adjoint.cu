@@ -108,10 +108,10 @@ cudaError_t launch_adjoint_step(int collision, const Real* fn, const Real* lam_n
                                 const Grid& g, const AdjointParams& ap, double* dtau_slots,
                                 cudaStream_t s) {
   if (collision == kBGK)
-    adjoint_step_kernel<L, Real, kBGK><<<grid_dims(g), kThreads, 0, s>>>(fn, lam_next, lam, g, ap,
+    adjoint_step_kernel<L, Real, kBGK><<<grid_dims(g), block_dims(g), 0, s>>>(fn, lam_next, lam, g, ap,
                                                                           dtau_slots);
   else if (collision == kTRT)
-    adjoint_step_kernel<L, Real, kTRT><<<grid_dims(g), kThreads, 0, s>>>(fn, lam_next, lam, g, ap,
+    adjoint_step_kernel<L, Real, kTRT><<<grid_dims(g), block_dims(g), 0, s>>>(fn, lam_next, lam, g, ap,
                                                                           dtau_slots);
   else
     return cudaErrorInvalidValue;
@@ -184,7 +184,7 @@ cudaError_t ke_gradient(int collision, const Real* rho0, const Real* u0, const G
     cur = nxt;
   }
   // seed: lambda^N and J from f^N (the last checkpoint written)
-  ke_seed_kernel<L, Real><<<grid_dims(g), kThreads, 0, s>>>(cur, lam[steps % 2], g, ke_slots);
+  ke_seed_kernel<L, Real><<<grid_dims(g), block_dims(g), 0, s>>>(cur, lam[steps % 2], g, ke_slots);
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
   if ((err = cudaMemsetAsync(dtau_slots, 0, lay.slots * sizeof(double), s)) != cudaSuccess) return err;
   const AdjointParams ap = make_params<Real>(collision, tau);
@@ -207,7 +207,7 @@ cudaError_t ke_gradient(int collision, const Real* rho0, const Real* u0, const G
       if (err != cudaSuccess) return err;
     }
   }
-  velocity_gradient_kernel<L, Real><<<grid_dims(g), kThreads, 0, s>>>(rho0, u0, lam[0], grad_u0, g);
+  velocity_gradient_kernel<L, Real><<<grid_dims(g), block_dims(g), 0, s>>>(rho0, u0, lam[0], grad_u0, g);
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
   sum_slots_kernel<<<1, 1024, 0, s>>>(ke_slots, lay.slots, 1, 1.0, out);
   sum_slots_kernel<<<1, 1024, 0, s>>>(dtau_slots, lay.slots, 1, 1.0, out + 1);

@@ -1,7 +1,8 @@
 // Checkpointed discrete adjoint of the coupled fluid + A + B -> C step, and
 // the gradients of a reactive-mixing objective with respect to the reaction
-// rate k, the fluid relaxation time tau, the scalar relaxation time tau_c and
-// the initial concentration fields A0, B0. No reference counterpart.
+// rate k, the fluid relaxation time tau, the scalar relaxation time tau_c, the
+// initial concentration fields A0, B0 and the initial velocity field u0. No
+// reference counterpart.
 //
 // Forward step n (src/simulate_reaction.cpp:518-543, one fused launch here):
 //   f^{n+1} = S(f^n)                            fluid collide-stream
@@ -269,19 +270,66 @@ __global__ void __launch_bounds__(kThreads)
   grad[cell] = s;
 }
 
+// dJ/du0(x) for f^0 = f_eq(rho0, u0), A^0 = g_eq(a0, u0), B^0 = g_eq(b0, u0):
+//   sum_i lf_i w_i rho0 (3 c_ia + 9 (c_i.u0) c_ia - 3 u0_a)
+//   + sum_i (la_i a0 + lb_i b0) w_i c_ia / cs2      (scalar lattice)
+template <class FL, class Real>
+__global__ void __launch_bounds__(kThreads)
+    reactive_velocity_gradient_kernel(const Real* __restrict__ rho0, const Real* __restrict__ u0,
+                                      const Real* __restrict__ a0, const Real* __restrict__ b0,
+                                      const Real* __restrict__ lf, const Real* __restrict__ la,
+                                      const Real* __restrict__ lb, Real* __restrict__ grad, Grid g) {
+  using SL = typename ScalarOf<FL>::type;
+  int x, y, z;
+  if (!cell_of(g, x, y, z)) return;
+  const int cell = (z * g.ny + y) * g.nx + x;
+  const size_t plane = (size_t)g.plane;
+  Real u[FL::D], gr[FL::D];
+  static_for<FL::D>([&](auto D) {
+    u[LB_I(D)] = u0[plane * LB_I(D) + cell];
+    gr[LB_I(D)] = Real(0);
+  });
+  const Real r = rho0[cell], ca = a0[cell], cb = b0[cell];
+  static_for<FL::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr double wd = FL::w[i];
+    const Real wl = Real(wd) * r * __ldg(lf + plane * i + cell);
+    const Real s = wl * (Real(3) + Real(9) * c_dot<FL, i>(u));
+    static_for<FL::D>([&](auto D) {
+      constexpr int c = FL::c[i][LB_I(D)];
+      if constexpr (c > 0) gr[LB_I(D)] += s;
+      if constexpr (c < 0) gr[LB_I(D)] -= s;
+      gr[LB_I(D)] -= Real(3) * wl * u[LB_I(D)];
+    });
+  });
+  const Real inv_cs2 = Real(1.0 / SL::cs2);
+  static_for<SL::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr double wd = SL::w[i];
+    const Real s = Real(wd) * inv_cs2 *
+                   (ca * __ldg(la + plane * i + cell) + cb * __ldg(lb + plane * i + cell));
+    static_for<FL::D>([&](auto D) {
+      constexpr int c = SL::c[i][LB_I(D)];
+      if constexpr (c > 0) gr[LB_I(D)] += s;
+      if constexpr (c < 0) gr[LB_I(D)] -= s;
+    });
+  });
+  static_for<FL::D>([&](auto D) { grad[plane * LB_I(D) + cell] = gr[LB_I(D)]; });
+}
+
 template <class FL, class Real>
 cudaError_t launch_reactive_adjoint(int collision, const Real* fn, const Real* an, const Real* bn,
                                     const Real* u_next, const Real* lf_next, const Real* la_next,
                                     const Real* lb_next, Real* lf, Real* la, Real* lb, Real* ubar,
                                     const Grid& g, const ReactiveParams& rp, double* slots,
                                     cudaStream_t s) {
-  reaction_adjoint_kernel<FL, Real><<<grid_dims(g), kThreads, 0, s>>>(
+  reaction_adjoint_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, s>>>(
       an, bn, u_next, la_next, lb_next, la, lb, ubar, g, rp, slots);
   if (collision == kBGK)
-    coupled_fluid_adjoint_kernel<FL, Real, kBGK><<<grid_dims(g), kThreads, 0, s>>>(
+    coupled_fluid_adjoint_kernel<FL, Real, kBGK><<<grid_dims(g), block_dims(g), 0, s>>>(
         fn, lf_next, ubar, lf, g, rp.fluid, slots);
   else
-    coupled_fluid_adjoint_kernel<FL, Real, kTRT><<<grid_dims(g), kThreads, 0, s>>>(
+    coupled_fluid_adjoint_kernel<FL, Real, kTRT><<<grid_dims(g), block_dims(g), 0, s>>>(
         fn, lf_next, ubar, lf, g, rp.fluid, slots);
   return cudaGetLastError();
 }
@@ -322,7 +370,7 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
                               const Real* a0, const Real* b0, const Grid& g, double tau,
                               double tau_c, double k, int steps, int interval, char* ws,
                               const ReactiveLayout& lay, double* out, Real* grad_a0, Real* grad_b0,
-                              cudaStream_t s) {
+                              Real* grad_u0, cudaStream_t s) {
   using SL = typename ScalarOf<FL>::type;
   constexpr int prec = sizeof(Real) == 4 ? LBM_FLOAT : LBM_DOUBLE;
   const double omega = (double)(Real(1) / Real(tau));
@@ -387,10 +435,10 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
                                                 partials, (size_t)lay.blocks * kStatSums * sizeof(double),
                                                 stats, s);
     if (err != cudaSuccess) return err;
-    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_SEGREGATION><<<grid_dims(g), kThreads, 0, s>>>(
+    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_SEGREGATION><<<grid_dims(g), block_dims(g), 0, s>>>(
         cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, j_slots);
   } else {
-    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_MEAN_PRODUCT><<<grid_dims(g), kThreads, 0, s>>>(
+    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_MEAN_PRODUCT><<<grid_dims(g), block_dims(g), 0, s>>>(
         cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, j_slots);
   }
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
@@ -423,11 +471,14 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
 
   // results: J, dJ/dk, dJ/dtau, dJ/dtau_c; dJ/dA0 (and dJ/dB0)
   const Real direct_a = objective == LBM_OBJECTIVE_MEAN_PRODUCT ? Real(1.0 / (double)g.plane) : Real(0);
-  scalar_init_gradient_kernel<FL, Real><<<grid_dims(g), kThreads, 0, s>>>(u0, lam[0].a, direct_a,
+  scalar_init_gradient_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, s>>>(u0, lam[0].a, direct_a,
                                                                           grad_a0, g);
   if (grad_b0 != nullptr)
-    scalar_init_gradient_kernel<FL, Real><<<grid_dims(g), kThreads, 0, s>>>(u0, lam[0].b, Real(0),
+    scalar_init_gradient_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, s>>>(u0, lam[0].b, Real(0),
                                                                             grad_b0, g);
+  if (grad_u0 != nullptr)
+    reactive_velocity_gradient_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, s>>>(
+        rho0, u0, a0, b0, lam[0].f, lam[0].a, lam[0].b, grad_u0, g);
   if (objective == LBM_OBJECTIVE_SEGREGATION) {
     if ((err = cudaMemcpyAsync(out, stats + 5, sizeof(double), cudaMemcpyDeviceToDevice, s)) !=
         cudaSuccess)
@@ -452,7 +503,7 @@ cudaError_t reactive_dispatch(int lattice, int collision, int objective, const v
                               const void* u0, const void* a0, const void* b0, size_t nx, size_t ny,
                               size_t nz, double tau, double tau_c, double k, int steps,
                               int interval, void* ws, size_t ws_bytes, double* out, void* grad_a0,
-                              void* grad_b0, cudaStream_t s) {
+                              void* grad_b0, void* grad_u0, cudaStream_t s) {
   Grid g;
   const int dims = lattice == kD2Q9 ? 2 : 3;
   cudaError_t err = validate_domain(rho0 == nullptr || u0 == nullptr || a0 == nullptr ||
@@ -472,7 +523,8 @@ cudaError_t reactive_dispatch(int lattice, int collision, int objective, const v
 #define LBCUBE_REACTIVE(FL)                                                                        \
   return reactive_gradient<FL, Real>(collision, objective, (const Real*)rho0, (const Real*)u0,     \
                                      (const Real*)a0, (const Real*)b0, g, tau, tau_c, k, steps,    \
-                                     interval, w, lay, out, (Real*)grad_a0, (Real*)grad_b0, s)
+                                     interval, w, lay, out, (Real*)grad_a0, (Real*)grad_b0,     \
+                                     (Real*)grad_u0, s)
   switch (lattice) {
     case kD2Q9: LBCUBE_REACTIVE(D2Q9);
     case kD3Q19: LBCUBE_REACTIVE(D3Q19);
@@ -509,17 +561,18 @@ extern "C" int lbm_reactive_gradient_async(int fluid_lattice, int precision, int
                                            double tau_c, double k_react, int steps,
                                            int checkpoint_interval, void* workspace,
                                            size_t workspace_bytes, double* result,
-                                           void* grad_a0, void* grad_b0, void* stream) {
+                                           void* grad_a0, void* grad_b0, void* grad_u0,
+                                           void* stream) {
   const cudaStream_t s = as_stream(stream);
   if (precision == LBM_FLOAT)
     return (int)reactive_dispatch<float>(fluid_lattice, collision, objective, rho0, u0, a0, b0,
                                          x_extent, y_extent, z_extent, tau, tau_c, k_react, steps,
                                          checkpoint_interval, workspace, workspace_bytes, result,
-                                         grad_a0, grad_b0, s);
+                                         grad_a0, grad_b0, grad_u0, s);
   if (precision == LBM_DOUBLE)
     return (int)reactive_dispatch<double>(fluid_lattice, collision, objective, rho0, u0, a0, b0,
                                           x_extent, y_extent, z_extent, tau, tau_c, k_react, steps,
                                           checkpoint_interval, workspace, workspace_bytes, result,
-                                          grad_a0, grad_b0, s);
+                                          grad_a0, grad_b0, grad_u0, s);
   return (int)cudaErrorInvalidValue;
 }

@@ -125,7 +125,7 @@ cudaError_t launch_scalar(const Real* cur_s, Real* nxt_s, const Real* cur_f, siz
   const Span reads[2] = {{cur_s, sb}, {cur_f, fb}};
   const Span writes[1] = {{nxt_s, sb}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  scalar_step_kernel<FL, Real><<<grid_dims(g), kThreads, 0, stream>>>(cur_s, nxt_s, cur_f, g,
+  scalar_step_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, stream>>>(cur_s, nxt_s, cur_f, g,
                                                                        omega_c, source);
   return cudaGetLastError();
 }
@@ -146,7 +146,7 @@ cudaError_t launch_reaction(const Real* cur_a, Real* nxt_a, const Real* cur_b, R
   const Span reads[3] = {{cur_a, sb}, {cur_b, sb}, {cur_f, fb}};
   const Span writes[2] = {{nxt_a, sb}, {nxt_b, sb}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  reaction_ab_kernel<FL, Real><<<grid_dims(g), kThreads, 0, stream>>>(cur_a, nxt_a, cur_b, nxt_b,
+  reaction_ab_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, stream>>>(cur_a, nxt_a, cur_b, nxt_b,
                                                                        cur_f, g, omega_c, k);
   return cudaGetLastError();
 }
@@ -176,10 +176,10 @@ cudaError_t launch_fluid_reaction(const Real* cur_f, Real* nxt_f, const Real* cu
   }
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
   if (partials != nullptr) {
-    fluid_reaction_kernel<FL, Real, CT, true><<<grid_dims(g), kThreads, 0, stream>>>(
+    fluid_reaction_kernel<FL, Real, CT, true><<<grid_dims(g), block_dims(g), 0, stream>>>(
         cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, partials);
   } else {
-    fluid_reaction_kernel<FL, Real, CT, false><<<grid_dims(g), kThreads, 0, stream>>>(
+    fluid_reaction_kernel<FL, Real, CT, false><<<grid_dims(g), block_dims(g), 0, stream>>>(
         cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, nullptr);
   }
   return cudaGetLastError();
@@ -194,10 +194,10 @@ cudaError_t fluid_reaction_with_velocity(int collision, const Real* cur_f, Real*
                                          Real* nxt_b, Real* u_out, const Grid& g, Real omega,
                                          Real omega_c, Real k, cudaStream_t s) {
   if (collision == kBGK) {
-    fluid_reaction_kernel<FL, Real, kBGK, false, true><<<grid_dims(g), kThreads, 0, s>>>(
+    fluid_reaction_kernel<FL, Real, kBGK, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
         cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, nullptr, u_out);
   } else if (collision == kTRT) {
-    fluid_reaction_kernel<FL, Real, kTRT, false, true><<<grid_dims(g), kThreads, 0, s>>>(
+    fluid_reaction_kernel<FL, Real, kTRT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
         cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, trt_omega_minus<Real>(omega), omega_c,
         k, nullptr, u_out);
   } else {

@@ -11,15 +11,19 @@
 
 namespace lbcube {
 
-// Threads per block along x. Each thread owns one cell of an x-row; a block
-// covers kThreads consecutive cells of one (y, z) row.
+// Most threads per block. In the one-cell-per-thread kernels each thread owns
+// one cell of an x-row and a block covers bx <= kThreads consecutive cells of
+// one (y, z) row.
 constexpr int kThreads = 128;
 
 // Domain extents and the block decomposition: grid.x = xblocks * ny
-// (row-major over y, then x-block), grid.y = nz.
+// (row-major over y, then x-block), grid.y = nz; xblocks = ceil(nx / kThreads)
+// blocks of bx threads, bx = ceil(nx / xblocks) rounded up to a warp, so that a
+// row of, e.g., 192 cells runs as two full blocks of 96 rather than 128 + 64.
 struct Grid {
   int nx, ny, nz;
   int xblocks;
+  int bx;           // threads per block
   long long plane;  // cells per population plane, nx * ny * nz (< 2^31)
 
   __host__ __device__ long long blocks() const { return (long long)xblocks * ny * nz; }
@@ -28,7 +32,7 @@ struct Grid {
 __device__ __forceinline__ bool cell_of(const Grid& g, int& x, int& y, int& z) {
   const int row = blockIdx.x / g.xblocks;
   const int xb = blockIdx.x - row * g.xblocks;
-  x = xb * kThreads + threadIdx.x;
+  x = xb * g.bx + threadIdx.x;
   y = row;
   z = blockIdx.y;
   return x < g.nx;
@@ -40,6 +44,7 @@ __device__ __forceinline__ long long block_linear() {
 }
 
 inline dim3 grid_dims(const Grid& g) { return dim3((unsigned)(g.xblocks * g.ny), (unsigned)g.nz, 1); }
+inline unsigned block_dims(const Grid& g) { return (unsigned)g.bx; }
 
 // Validation in the reference's order (src/lattice_cuda.cu:488-503), then the
 // engine's own limits. On success fills `g`.
@@ -57,6 +62,7 @@ inline cudaError_t validate_domain(bool any_null, unsigned bx, unsigned by, unsi
   g.ny = (int)ny;
   g.nz = (int)nz;
   g.xblocks = (int)((nx + kThreads - 1) / kThreads);
+  g.bx = (int)(((nx + g.xblocks - 1) / g.xblocks + 31) / 32 * 32);
   g.plane = (long long)(cells * nz);
   if ((long long)g.xblocks * g.ny > (long long)INT_MAX) return cudaErrorInvalidValue;
   return cudaSuccess;

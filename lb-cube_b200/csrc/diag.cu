@@ -86,7 +86,7 @@ cudaError_t launch_diagnostics(const void* vf, size_t nx, size_t ny, size_t nz, 
   const Span reads[1] = {{f, (size_t)L::Q * g.plane * sizeof(Real)}};
   const Span writes[2] = {{partials, need}, {out, kDiagOut * sizeof(double)}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  diag_partials_kernel<L, Real><<<grid_dims(g), kThreads, 0, s>>>(f, g, partials);
+  diag_partials_kernel<L, Real><<<grid_dims(g), block_dims(g), 0, s>>>(f, g, partials);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   return launch_diag_finalize(partials, g.blocks(), speed_limit, out, s);

@@ -95,7 +95,7 @@ cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, 
     fluid_step_vec_kernel<L, S, CT><<<vec_grid_dims(vg), vec_block_threads(vg), 0, stream>>>(
         cur, nxt, vg, omega, omega_minus, typename S::Params{});
   } else {
-    fluid_step_kernel<L, Real, CT><<<grid_dims(g), kThreads, 0, stream>>>(cur, nxt, g, omega,
+    fluid_step_kernel<L, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(cur, nxt, g, omega,
                                                                            omega_minus);
   }
   return cudaGetLastError();
@@ -124,12 +124,12 @@ cudaError_t launch_fluid_step_diag(const Real* cur, Real* nxt, size_t nx, size_t
   if (kUseVec<L, Real, CT> && vec_eligible<S>(g, cur, nxt)) {
     const VecGrid vg = make_vec_grid(g, S::V);
     const dim3 grid = vec_grid_dims(vg);
-    count = (long long)grid.x * grid.y;  // <= g.blocks(): a block covers >= kThreads cells
+    count = (long long)grid.x * grid.y;  // <= g.blocks(): a vector block spans >= one row block
     fluid_step_vec_kernel<L, S, CT, true><<<grid, vec_block_threads(vg), 0, stream>>>(
         cur, nxt, vg, omega, omega_minus, typename S::Params{}, partials);
   } else {
     count = g.blocks();
-    fluid_step_kernel<L, Real, CT, true><<<grid_dims(g), kThreads, 0, stream>>>(
+    fluid_step_kernel<L, Real, CT, true><<<grid_dims(g), block_dims(g), 0, stream>>>(
         cur, nxt, g, omega, omega_minus, partials);
   }
   err = cudaGetLastError();

@@ -43,7 +43,7 @@ cudaError_t launch_init(const void* rho, const void* u, void* out, size_t nx, si
                          {u, (size_t)L::D * g.plane * sizeof(Real)}};
   const Span writes[1] = {{out, (size_t)L::Q * g.plane * sizeof(Real)}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  init_equilibrium_kernel<L, Real, SCALAR><<<grid_dims(g), kThreads, 0, s>>>(
+  init_equilibrium_kernel<L, Real, SCALAR><<<grid_dims(g), block_dims(g), 0, s>>>(
       static_cast<const Real*>(rho), static_cast<const Real*>(u), static_cast<Real*>(out), g);
   return cudaGetLastError();
 }

@@ -46,7 +46,7 @@ cudaError_t launch_macro(const void* vf, size_t nx, size_t ny, size_t nz, void* 
   const Span reads[1] = {{vf, (size_t)L::Q * n}};
   const Span writes[3] = {{rho, rho ? n : 0}, {u, u ? (size_t)L::D * n : 0}, {speed, speed ? n : 0}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  macro_fields_kernel<L, Real><<<grid_dims(g), kThreads, 0, s>>>(
+  macro_fields_kernel<L, Real><<<grid_dims(g), block_dims(g), 0, s>>>(
       static_cast<const Real*>(vf), g, static_cast<Real*>(rho), static_cast<Real*>(u),
       static_cast<Real*>(speed));
   return cudaGetLastError();

@@ -13,12 +13,12 @@ namespace lbcube {
 // sum C_A, sum C_B, sum C_A^2, sum C_B^2, sum C_A C_B (lattice_io.hpp:266-271).
 constexpr int kStatSums = 5;
 
-// Sums v[0..N) over the block (all kThreads threads must call it) and writes
-// the block's totals to out[0..N) from thread 0. Fixed reduction tree.
+// Sums v[0..N) over the block (every thread must call it; the block is a
+// whole number of warps, at most kThreads threads) and writes the block's
+// totals to out[0..N) from thread 0. Fixed reduction tree.
 template <int N>
 __device__ __forceinline__ void block_sum_to(double (&v)[N], double* out) {
-  constexpr int kWarps = kThreads / 32;
-  __shared__ double part[kWarps][N];
+  __shared__ double part[kThreads / 32][N];
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll
@@ -31,11 +31,11 @@ __device__ __forceinline__ void block_sum_to(double (&v)[N], double* out) {
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    const int warps = (int)(blockDim.x >> 5);
 #pragma unroll
     for (int k = 0; k < N; ++k) {
       double s = part[0][k];
-#pragma unroll
-      for (int w = 1; w < kWarps; ++w) s += part[w][k];
+      for (int w = 1; w < warps; ++w) s += part[w][k];
       out[k] = s;
     }
   }

@@ -100,7 +100,7 @@ cudaError_t launch_stats(const void* va, const void* vb, size_t nx, size_t ny, s
   const Span reads[2] = {{a, sb}, {b, sb}};
   const Span writes[2] = {{partials, need}, {out, 8 * sizeof(double)}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  stats_partials_kernel<SL, Real><<<grid_dims(g), kThreads, 0, s>>>(a, b, g, partials);
+  stats_partials_kernel<SL, Real><<<grid_dims(g), block_dims(g), 0, s>>>(a, b, g, partials);
   err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   // k_react has the population precision, as in compute_reactive_stats<SL, Real>.

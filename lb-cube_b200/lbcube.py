@@ -100,7 +100,7 @@ def _declare(lib):
                                   _vp, _sz, _vp, _vp, _vp],
         "lbm_adjoint_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp],
         "lbm_reactive_gradient_async": [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _sz, _sz, _sz,
-                                        d, d, d, C.c_int, C.c_int, _vp, _sz, _vp, _vp, _vp, _vp],
+                                        d, d, d, C.c_int, C.c_int, _vp, _sz, _vp, _vp, _vp, _vp, _vp],
         "lbm_step_slab_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp, _vp, _vp, _sz,
                                 _sz, _vp],
         "lbm_slab_pack_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
@@ -319,15 +319,15 @@ def reactive_gradient_workspace_bytes(fluid_lattice, real, nx, ny, nz, steps, in
 
 def reactive_gradient_async(fluid_lattice, real, collision, objective, rho0, u0, a0, b0, nx, ny, nz,
                             tau, tau_c, k_react, steps, interval, workspace, workspace_bytes, result,
-                            grad_a0, grad_b0=None, stream=None) -> int:
+                            grad_a0, grad_b0=None, grad_u0=None, stream=None) -> int:
     """Checkpointed adjoint of the coupled fluid + A + B -> C run: result
-    (device FP64[4]) = J, dJ/dk, dJ/dtau, dJ/dtau_c; grad_a0 (grad_b0) =
-    dJ/da0 (dJ/db0). objective in OBJECTIVES."""
+    (device FP64[4]) = J, dJ/dk, dJ/dtau, dJ/dtau_c; grad_a0 (grad_b0,
+    grad_u0) = dJ/da0 (dJ/db0, dJ/du0). objective in OBJECTIVES."""
     return load().lbm_reactive_gradient_async(
         LATTICES[fluid_lattice], REALS[real_name(real)], COLLISIONS[collision], OBJECTIVES[objective],
         _ptr(rho0), _ptr(u0), _ptr(a0), _ptr(b0), nx, ny, nz, float(tau), float(tau_c), float(k_react),
         int(steps), int(interval), _ptr(workspace), int(workspace_bytes), _ptr(result), _ptr(grad_a0),
-        _ptr(grad_b0), _stream(stream))
+        _ptr(grad_b0), _ptr(grad_u0), _stream(stream))
 
 
 def macro_fields_async(lattice, real, populations, nx, ny, nz, density, velocity=None, speed=None,

@@ -181,4 +181,4 @@ def test_reactive_gradient_validation(lib):
     assert call(workspace_bytes=nb - 1) == E.cudaErrorInvalidValue
     assert call(steps=0) == E.cudaErrorInvalidValue
     assert E.load().lbm_reactive_gradient_async(1, 0, 1, 7, A0, A1, A2, A3, 16, 12, 10, 0.8, 0.7, 0.1, 20, 4,
-                                                A4, nb, A4 + 8, A4 + 16, None, None) == E.cudaErrorInvalidValue
+                                                A4, nb, A4 + 8, A4 + 16, None, None, None) == E.cudaErrorInvalidValue

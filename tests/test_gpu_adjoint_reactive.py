@@ -4,7 +4,7 @@ central finite differences of its own forward run, in FP64.
 The coupled step is the fused fluid + A + B -> C launch (bit-identical to the
 reference's two-launch sequence). Checked, for the mean-product objective
 <C> = <A0> - <A> and the segregation intensity I_s, with BGK and TRT fluids:
-dJ/dk, dJ/dtau, dJ/dtau_c and <dJ/dA0, d>, <dJ/dB0, d> along seeded unit
+dJ/dk, dJ/dtau, dJ/dtau_c and <dJ/dA0, d>, <dJ/dB0, d>, <dJ/du0, d> along seeded unit
 directions, relative error <= 1e-6 plus the rounding noise of the
 differences, 1e-13 |J| / h (central differences at h = 1e-3 and 5e-4 combined
 by one Richardson step, error O(h^4)) (step count not a multiple of the
@@ -49,10 +49,11 @@ def gradient(fl, real, op, obj, rho, u, a, b, dims, steps, interval, tau=TAU, ta
     nb = E.reactive_gradient_workspace_bytes(fl, real, nx, ny, nz, steps, interval)
     ws = torch.empty(nb, dtype=torch.uint8, device=a.device)
     res = torch.zeros(4, dtype=torch.float64, device=a.device)
-    ga, gb = torch.empty_like(a), torch.empty_like(b)
+    ga, gb, gu = torch.empty_like(a), torch.empty_like(b), torch.empty_like(u)
     E.check(E.reactive_gradient_async(fl, real, op, obj, rho, u, a, b, nx, ny, nz, tau, tau_c, k, steps,
-                                      interval, ws, nb, res, ga, gb))
+                                      interval, ws, nb, res, ga, gb, gu))
     torch.cuda.synchronize()
+    gradient.last_u = gu
     return res.cpu().tolist(), ga, gb
 
 
@@ -94,14 +95,15 @@ def test_reactive_gradient_central_differences_fp64(fl, dims, op, obj):
     steps, interval = 23, 5
     rho, u, a, b = fields(fl, shape, dev, torch.float64, seed=11)
     (J, dk, dtau, dtc), ga, gb = gradient(fl, "double", op, obj, rho, u, a, b, dims, steps, interval)
+    gu = gradient.last_u
     Jf = forward_objective(fl, "double", op, obj, rho, u, a, b, dims, steps)
     assert abs(J - Jf) <= 1e-12 * abs(Jf), (J, Jf)
 
     def Jat(**kw):
         kw2 = dict(tau=TAU, tau_c=TAU_C, k=K)
-        aa, bb = kw.pop("a", a), kw.pop("b", b)
+        aa, bb, uu = kw.pop("a", a), kw.pop("b", b), kw.pop("u", u)
         kw2.update(kw)
-        return gradient(fl, "double", op, obj, rho, u, aa, bb, dims, steps, interval, **kw2)[0][0]
+        return gradient(fl, "double", op, obj, rho, uu, aa, bb, dims, steps, interval, **kw2)[0][0]
 
     def richardson(J_of, h):
         """Central difference with one Richardson step (error O(h^4))."""
@@ -120,11 +122,11 @@ def test_reactive_gradient_central_differences_fp64(fl, dims, op, obj):
         fd = richardson(lambda e: Jat(**{name: x0 + e}), h)
         assert close(fd, ad, h / 2), (name, fd, ad)
     gen = torch.Generator().manual_seed(99)
-    for field, grad in (("a", ga), ("b", gb)):
-        for _ in range(4):
-            d = torch.randn(shape, generator=gen, dtype=torch.float64).to(dev)
+    for field, grad in (("a", ga), ("b", gb), ("u", gu)):
+        for _ in range(4 if field != "u" else 3):
+            d = torch.randn(grad.shape, generator=gen, dtype=torch.float64).to(dev)
             d /= torch.linalg.vector_norm(d)
-            base = a if field == "a" else b
+            base = {"a": a, "b": b, "u": u}[field]
             fd = richardson(lambda e: Jat(**{field: base + e * d}), h)
             ad = float((grad * d).sum())
             assert close(fd, ad, h / 2), (field, fd, ad)
