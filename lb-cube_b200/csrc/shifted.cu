@@ -72,20 +72,21 @@ cudaError_t shifted_by_lattice(int lattice, int collision, const void* cur, void
 }
 
 // ---- conversions --------------------------------------------------------------
-// One thread per (population, cell) element; plane i uses weight w_i.
+// grid.y = population i (its weight w_i is a compile-time constant of the
+// block's branch), grid-stride over the cells of that plane.
 template <class L, int FMT, class Real, bool ENCODE>
 __global__ void __launch_bounds__(256)
     convert_kernel(const void* __restrict__ in, void* __restrict__ out, long long plane,
                    float rho0) {
   using S = ShiftedStorage<FMT>;
-  const long long n = plane * L::Q;
   const typename S::Params p{rho0};
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(e / plane);
-    static_for<L::Q>([&](auto I) {
-      constexpr int q = LB_I(I);
-      if (q != i) return;
+  const int i = (int)blockIdx.y;
+  static_for<L::Q>([&](auto I) {
+    constexpr int q = LB_I(I);
+    if (q != i) return;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < plane;
+         c += (long long)gridDim.x * blockDim.x) {
+      const long long e = (long long)q * plane + c;
       if constexpr (ENCODE) {
         const float f = (float)static_cast<const Real*>(in)[e];
         static_cast<unsigned short*>(out)[e] = S::template encode<L, q>(f, p);
@@ -93,8 +94,8 @@ __global__ void __launch_bounds__(256)
         const float f = S::template decode<L, q>(static_cast<const unsigned short*>(in)[e], p);
         static_cast<Real*>(out)[e] = (Real)f;
       }
-    });
-  }
+    }
+  });
 }
 
 template <class L, int FMT, bool ENCODE>
@@ -109,12 +110,11 @@ cudaError_t launch_convert(int precision, const void* in, void* out, size_t nx, 
   const Span reads[1] = {{in, ENCODE ? wide : narrow}};
   const Span writes[1] = {{out, ENCODE ? narrow : wide}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  const long long n = (long long)L::Q * g.plane;
-  const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 32);
+  const dim3 grid((unsigned)std::min<long long>((g.plane + 255) / 256, 148LL * 8), (unsigned)L::Q, 1);
   if (precision == LBM_FLOAT)
-    convert_kernel<L, FMT, float, ENCODE><<<blocks, 256, 0, s>>>(in, out, g.plane, rho0);
+    convert_kernel<L, FMT, float, ENCODE><<<grid, 256, 0, s>>>(in, out, g.plane, rho0);
   else
-    convert_kernel<L, FMT, double, ENCODE><<<blocks, 256, 0, s>>>(in, out, g.plane, rho0);
+    convert_kernel<L, FMT, double, ENCODE><<<grid, 256, 0, s>>>(in, out, g.plane, rho0);
   return cudaGetLastError();
 }
 
