@@ -319,7 +319,7 @@ int lbm_decode_shifted_async(int lattice, int format, int precision, const void*
 /* ---------------------------------------------------------------------------
  * Discrete reverse-mode adjoint (no reference counterpart). Objective:
  * J = sum_x 0.5 rho |u|^2 of the state after `steps` collide-stream steps
- * (BGK or TRT) started from f^0 = f_eq(rho0, u0). The gradient driver runs
+ * (BGK or TRT; MRT on D2Q9 / D3Q19) started from f^0 = f_eq(rho0, u0). The gradient driver runs
  * the forward pass storing a checkpoint every `checkpoint_interval` steps,
  * then for each segment, last first, recomputes the segment's states from
  * its checkpoint and runs the adjoint steps back through it. Outputs (device):
@@ -347,7 +347,7 @@ int lbm_adjoint_step_async(int lattice, int precision, int collision, const void
 
 /* Reactive-mixing gradients (no reference counterpart): the checkpointed
  * discrete adjoint of the coupled step of lbm_fluid_reaction_ab_async (fluid
- * BGK or TRT, then the A + B -> C reaction step of launch_reaction_AB_gpu on
+ * BGK or TRT, or MRT on D2Q9 / D3Q19, then the A + B -> C reaction step of launch_reaction_AB_gpu on
  * the post-step fluid, src/simulate_reaction.cpp:518-543). Initial state:
  * f^0 = f_eq(rho0, u0), A^0 = g_eq(a0, u0), B^0 = g_eq(b0, u0) (fields [Z,Y,X],
  * u0 [D,Z,Y,X], population precision). Objective of the state after `steps`:

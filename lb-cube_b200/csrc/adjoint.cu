@@ -1,5 +1,6 @@
-// Discrete reverse-mode adjoint of the collide-stream step (BGK, TRT) and the
-// checkpointed gradient of the final kinetic energy. No reference counterpart.
+// Discrete reverse-mode adjoint of the collide-stream step (BGK, TRT; MRT on
+// D2Q9 and D3Q19) and the checkpointed gradient of the final kinetic energy.
+// No reference counterpart.
 //
 // adjoint_step_kernel applies the transposed step Jacobian of adjoint.cuh at
 // every cell and scatters to the pull sources. The tau-derivative of the step,
@@ -113,8 +114,13 @@ cudaError_t launch_adjoint_step(int collision, const Real* fn, const Real* lam_n
   else if (collision == kTRT)
     adjoint_step_kernel<L, Real, kTRT><<<grid_dims(g), block_dims(g), 0, s>>>(fn, lam_next, lam, g, ap,
                                                                           dtau_slots);
-  else
+  else if constexpr (L::Q != 27) {
+    if (collision != kMRT) return cudaErrorInvalidValue;
+    adjoint_step_kernel<L, Real, kMRT><<<grid_dims(g), block_dims(g), 0, s>>>(fn, lam_next, lam, g, ap,
+                                                                          dtau_slots);
+  } else {
     return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
@@ -224,7 +230,8 @@ cudaError_t gradient_dispatch(int lattice, int collision, const void* rho0, cons
                                         out == nullptr || grad == nullptr,
                                     1, 1, 1, dims, nx, ny, nz, g);
   if (err != cudaSuccess) return err;
-  if (steps < 1 || interval < 2 || (collision != kBGK && collision != kTRT) || !(tau > 0.5))
+  const bool mrt_ok = collision == kMRT && lattice != kD3Q27;
+  if (steps < 1 || interval < 2 || (collision != kBGK && collision != kTRT && !mrt_ok) || !(tau > 0.5))
     return cudaErrorInvalidValue;
   const int Q = lattice == kD2Q9 ? 9 : (lattice == kD3Q19 ? 19 : 27);
   const GradientLayout lay = gradient_layout(Q, sizeof(Real), g, steps, interval);

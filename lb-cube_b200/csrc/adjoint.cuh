@@ -52,10 +52,16 @@ inline AdjointParams make_params(int collision, double tau) {
 // in the population precision). One pass over the opposite pairs (i, o):
 // f_eq_i = E + O, f_eq_o = E - O with E = w rho (1 + 4.5 (c.u)^2 - 1.5 u.u) and
 // O = 3 w rho c.u, so every sum needs only the pair's own values.
+template <class L, class Real>
+__device__ __forceinline__ double fluid_adjoint_cell_mrt(const Real (&gv)[L::Q], const Real (&lv)[L::Q],
+                                                         Real rho, const Real (&u)[L::D],
+                                                         const AdjointParams& ap, Real (&mu)[L::Q]);
+
 template <class L, class Real, int CT>
 __device__ __forceinline__ double fluid_adjoint_cell(const Real (&gv)[L::Q], const Real (&lv)[L::Q],
                                                      Real rho, const Real (&u)[L::D],
                                                      const AdjointParams& ap, Real (&mu)[L::Q]) {
+  if constexpr (CT == kMRT) return fluid_adjoint_cell_mrt<L, Real>(gv, lv, rho, u, ap, mu);
   const Real usq = u_dot_u<L>(u);
   const Real om = Real(ap.omega), omm = Real(ap.omega_minus);
   const Real base = Real(1) - Real(1.5) * usq;
@@ -106,12 +112,130 @@ __device__ __forceinline__ double fluid_adjoint_cell(const Real (&gv)[L::Q], con
   const Real b = CT == kBGK ? Real(0) : Real(0.5) * (omm - om);
   static_for<L::Q>([&](auto I) {
     constexpr int j = LB_I(I);
-    constexpr int o = L::opp[j];
+    [[maybe_unused]] constexpr int o = L::opp[j];
     Real m = a * lv[j] + A + c_dot<L, j>(B);
     if constexpr (CT != kBGK) m += b * lv[o];
     mu[j] = m;
   });
   return dtau;
+}
+
+// ---- MRT (D2Q9, D3Q19) ---------------------------------------------------------
+// Forward (collide_mrt_d2q9 / collide_mrt_d3q19): m = M g, m_post_k = m_k -
+// s_k (m_k - m_eq_k(rho, j)) (s_k = 0 for rho and j), f = M^T D^-1 m_post. With
+// nu = D^-1 M lambda the transpose is
+//   mu_j = sum_k M_kj (1 - s_k) nu_k + A + B . c_j,
+//   A = sum_k s_k nu_k d m_eq_k / d rho,   B_a = sum_k s_k nu_k d m_eq_k / d j_a,
+// and lambda . df/domega = -sum over the omega-relaxed k of nu_k (m_k - m_eq_k).
+// m_eq written in (rho, j): D2Q9 e = -2 rho + 3 j.j / rho, eps = rho - 3 j.j / rho,
+// q_a = -j_a, p_xx = (jx^2 - jy^2) / rho, p_xy = jx jy / rho (rates 1.63, 1.14,
+// 1.92, omega); D3Q19 e = -11 rho + 19 j.j / rho, eps = 3 rho - 5.5 j.j / rho,
+// q_a = -2/3 j_a, 3p_xx = 3 (2 jx^2 - jy^2 - jz^2) / rho, p_ww = (jy^2 - jz^2) / rho,
+// p_xy, p_yz, p_xz = j_a j_b / rho (rate omega), ghosts 0 (rate 1).
+template <class L>
+struct MrtAdj;
+template <>
+struct MrtAdj<D2Q9> {
+  using Mx = Mrt9;
+  __host__ __device__ static constexpr bool omega_rate(int k) { return k == 7 || k == 8; }
+  template <class Real>
+  __device__ __forceinline__ static Real rate(int k, Real omega) {
+    return k == 1 ? Real(1.63) : k == 2 ? Real(1.14) : (k == 4 || k == 6) ? Real(1.92)
+         : (k == 7 || k == 8) ? omega : Real(0);
+  }
+  // d m_eq_k / d rho and d m_eq_k / d j (u = j / rho), and m_eq_k itself
+  template <int k, class Real>
+  __device__ __forceinline__ static void deq(Real rho, const Real (&u)[2], Real usq, Real& dr,
+                                             Real (&dj)[2], Real& eq) {
+    dj[0] = dj[1] = Real(0);
+    if constexpr (k == 1) { dr = -Real(2) - Real(3) * usq; dj[0] = Real(6) * u[0]; dj[1] = Real(6) * u[1]; eq = -Real(2) * rho + Real(3) * rho * usq; }
+    else if constexpr (k == 2) { dr = Real(1) + Real(3) * usq; dj[0] = -Real(6) * u[0]; dj[1] = -Real(6) * u[1]; eq = rho - Real(3) * rho * usq; }
+    else if constexpr (k == 4) { dr = Real(0); dj[0] = -Real(1); eq = -rho * u[0]; }
+    else if constexpr (k == 6) { dr = Real(0); dj[1] = -Real(1); eq = -rho * u[1]; }
+    else if constexpr (k == 7) { dr = -(u[0] * u[0] - u[1] * u[1]); dj[0] = Real(2) * u[0]; dj[1] = -Real(2) * u[1]; eq = rho * (u[0] * u[0] - u[1] * u[1]); }
+    else if constexpr (k == 8) { dr = -u[0] * u[1]; dj[0] = u[1]; dj[1] = u[0]; eq = rho * u[0] * u[1]; }
+    else { dr = Real(0); eq = Real(0); }
+  }
+};
+template <>
+struct MrtAdj<D3Q19> {
+  using Mx = Mrt19;
+  __host__ __device__ static constexpr bool omega_rate(int k) { return k >= 9 && k <= 13; }
+  template <class Real>
+  __device__ __forceinline__ static Real rate(int k, Real omega) {
+    return (k == 0 || k == 3 || k == 5 || k == 7) ? Real(0) : (k >= 9 && k <= 13) ? omega : Real(1);
+  }
+  template <int k, class Real>
+  __device__ __forceinline__ static void deq(Real rho, const Real (&u)[3], Real usq, Real& dr,
+                                             Real (&dj)[3], Real& eq) {
+    dj[0] = dj[1] = dj[2] = Real(0);
+    if constexpr (k == 1) { dr = -Real(11) - Real(19) * usq; dj[0] = Real(38) * u[0]; dj[1] = Real(38) * u[1]; dj[2] = Real(38) * u[2]; eq = -Real(11) * rho + Real(19) * rho * usq; }
+    else if constexpr (k == 2) { dr = Real(3) + Real(5.5) * usq; dj[0] = -Real(11) * u[0]; dj[1] = -Real(11) * u[1]; dj[2] = -Real(11) * u[2]; eq = Real(3) * rho - Real(5.5) * rho * usq; }
+    else if constexpr (k == 4) { dr = Real(0); dj[0] = -Real(2) / Real(3); eq = -(Real(2) / Real(3)) * rho * u[0]; }
+    else if constexpr (k == 6) { dr = Real(0); dj[1] = -Real(2) / Real(3); eq = -(Real(2) / Real(3)) * rho * u[1]; }
+    else if constexpr (k == 8) { dr = Real(0); dj[2] = -Real(2) / Real(3); eq = -(Real(2) / Real(3)) * rho * u[2]; }
+    else if constexpr (k == 9) {
+      const Real t = Real(2) * u[0] * u[0] - u[1] * u[1] - u[2] * u[2];
+      dr = -Real(3) * t; dj[0] = Real(12) * u[0]; dj[1] = -Real(6) * u[1]; dj[2] = -Real(6) * u[2]; eq = Real(3) * rho * t;
+    }
+    else if constexpr (k == 10) { dr = -(u[1] * u[1] - u[2] * u[2]); dj[1] = Real(2) * u[1]; dj[2] = -Real(2) * u[2]; eq = rho * (u[1] * u[1] - u[2] * u[2]); }
+    else if constexpr (k == 11) { dr = -u[0] * u[1]; dj[0] = u[1]; dj[1] = u[0]; eq = rho * u[0] * u[1]; }
+    else if constexpr (k == 12) { dr = -u[1] * u[2]; dj[1] = u[2]; dj[2] = u[1]; eq = rho * u[1] * u[2]; }
+    else if constexpr (k == 13) { dr = -u[0] * u[2]; dj[0] = u[2]; dj[2] = u[0]; eq = rho * u[0] * u[2]; }
+    else { dr = Real(0); eq = Real(0); }
+  }
+};
+
+template <class L, class Real>
+__device__ __forceinline__ double fluid_adjoint_cell_mrt(const Real (&gv)[L::Q], const Real (&lv)[L::Q],
+                                                         Real rho, const Real (&u)[L::D],
+                                                         const AdjointParams& ap, Real (&mu)[L::Q]) {
+  using MA = MrtAdj<L>;
+  using Mx = typename MA::Mx;
+  const Real om = Real(ap.omega);
+  const Real usq = u_dot_u<L>(u);
+  Real A = Real(0), B[L::D], keep[L::Q];
+  static_for<L::D>([&](auto D) { B[LB_I(D)] = Real(0); });
+  Real dom = Real(0);  // lambda . df/domega
+  static_for<L::Q>([&](auto KK) {
+    constexpr int k = LB_I(KK);
+    constexpr int nrm = Mx::M.norm[k];
+    Real nu = Real(0);
+    static_for<L::Q>([&](auto I) {
+      constexpr int i = LB_I(I);
+      constexpr int c = Mx::M.m[k][i];
+      if constexpr (c == 1) nu += lv[i];
+      else if constexpr (c == -1) nu -= lv[i];
+      else if constexpr (c != 0) nu += Real(c) * lv[i];
+    });
+    nu = nu / Real(nrm);
+    const Real s = MA::template rate<Real>(k, om);
+    keep[k] = (Real(1) - s) * nu;
+    Real dr, dj[L::D], eq;
+    MA::template deq<k, Real>(rho, u, usq, dr, dj, eq);
+    A += s * nu * dr;
+    static_for<L::D>([&](auto D) { B[LB_I(D)] += s * nu * dj[LB_I(D)]; });
+    if constexpr (MA::omega_rate(k)) {
+      Real m = Real(0);  // forward moment of the pulled state
+      static_for<L::Q>([&](auto I) {
+        constexpr int i = LB_I(I);
+        constexpr int c = Mx::M.m[k][i];
+        if constexpr (c != 0) m += Real(c) * gv[i];
+      });
+      dom -= nu * (m - eq);
+    }
+  });
+  static_for<L::Q>([&](auto J) {
+    constexpr int j = LB_I(J);
+    Real m = A + c_dot<L, j>(B);
+    static_for<L::Q>([&](auto KK) {
+      constexpr int k = LB_I(KK);
+      constexpr int c = Mx::M.m[k][j];
+      if constexpr (c != 0) m += Real(c) * keep[k];
+    });
+    mu[j] = m;
+  });
+  return (double)dom * ap.domega_dtau;
 }
 
 // Adjoint of the pull: mu_j(x) goes to lambda^n(x - c_j, j).

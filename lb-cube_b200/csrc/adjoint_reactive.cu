@@ -328,9 +328,14 @@ cudaError_t launch_reactive_adjoint(int collision, const Real* fn, const Real* a
   if (collision == kBGK)
     coupled_fluid_adjoint_kernel<FL, Real, kBGK><<<grid_dims(g), block_dims(g), 0, s>>>(
         fn, lf_next, ubar, lf, g, rp.fluid, slots);
-  else
+  else if (collision == kTRT)
     coupled_fluid_adjoint_kernel<FL, Real, kTRT><<<grid_dims(g), block_dims(g), 0, s>>>(
         fn, lf_next, ubar, lf, g, rp.fluid, slots);
+  else if constexpr (FL::Q != 27)
+    coupled_fluid_adjoint_kernel<FL, Real, kMRT><<<grid_dims(g), block_dims(g), 0, s>>>(
+        fn, lf_next, ubar, lf, g, rp.fluid, slots);
+  else
+    return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
@@ -512,7 +517,8 @@ cudaError_t reactive_dispatch(int lattice, int collision, int objective, const v
                                     1, 1, 1, dims, nx, ny, nz, g);
   if (err != cudaSuccess) return err;
   if (lattice != kD2Q9 && lattice != kD3Q19 && lattice != kD3Q27) return cudaErrorInvalidValue;
-  if (steps < 1 || interval < 2 || (collision != kBGK && collision != kTRT) ||
+  const bool mrt_ok = collision == kMRT && lattice != kD3Q27;
+  if (steps < 1 || interval < 2 || (collision != kBGK && collision != kTRT && !mrt_ok) ||
       (objective != LBM_OBJECTIVE_MEAN_PRODUCT && objective != LBM_OBJECTIVE_SEGREGATION) ||
       !(tau > 0.5) || !(tau_c > 0.5))
     return cudaErrorInvalidValue;

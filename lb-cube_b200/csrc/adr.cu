@@ -200,6 +200,9 @@ cudaError_t fluid_reaction_with_velocity(int collision, const Real* cur_f, Real*
     fluid_reaction_kernel<FL, Real, kTRT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
         cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, trt_omega_minus<Real>(omega), omega_c,
         k, nullptr, u_out);
+  } else if (collision == kMRT) {
+    fluid_reaction_kernel<FL, Real, kMRT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, nullptr, u_out);
   } else {
     return cudaErrorInvalidValue;
   }

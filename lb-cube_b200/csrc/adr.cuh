@@ -5,7 +5,7 @@
 
 namespace lbcube {
 
-// One fused fluid + A + B -> C step (BGK or TRT) that also stores the
+// One fused fluid + A + B -> C step (BGK, TRT or MRT) that also stores the
 // advecting velocity (the fluid velocity of the new state) into u_out [D, N].
 template <class FL, class Real>
 cudaError_t fluid_reaction_with_velocity(int collision, const Real* cur_f, Real* nxt_f,

@@ -1,6 +1,6 @@
 """GPU: the checkpointed discrete adjoint against central finite differences.
 
-* FP64, D3Q19 BGK and TRT, 20^3: <grad J, d> along 16 seeded unit directions
+* FP64, D3Q19 BGK, TRT and MRT, 20^3: <grad J, d> along 16 seeded unit directions
   d of the initial velocity field and dJ/dtau match central differences of
   forward-only runs to relative 1e-6 (the bar the engine is held to is 1e-4);
   the step count is not a multiple of the checkpoint interval, so a partial
@@ -56,7 +56,7 @@ def forward_ke(u0, tau, steps, collision):
     return float((0.5 * (j * j).sum(0) / r).sum())
 
 
-@pytest.mark.parametrize("collision", ["BGK", "TRT"])
+@pytest.mark.parametrize("collision", ["BGK", "TRT", "MRT"])
 def test_gradient_matches_central_differences_fp64(collision):
     dev = torch.device("cuda:0")
     n, steps, interval, tau = 20, 47, 10, 0.56
@@ -100,3 +100,48 @@ def test_autograd_wrapper():
     _, dtau, grad = run_gradient(u0.detach(), 0.6, 30, 8, "TRT")
     assert torch.equal(u0.grad, grad)
     assert float(tau.grad) == dtau
+
+
+def test_d2q9_mrt_gradient_fp64():
+    """D2Q9 MRT (the reference's rates 1.63, 1.14, 1.92, omega): KE gradient
+    against central differences through the public 2-D launchers."""
+    dev = torch.device("cuda:0")
+    n, steps, interval, tau = 24, 31, 8, 0.6
+    g = torch.Generator().manual_seed(77)
+    k = 2 * math.pi / n
+    ax = torch.arange(n, dtype=torch.float64) * k
+    y, x = torch.meshgrid(ax, ax, indexing="ij")
+    u0 = torch.stack([0.03 * torch.sin(x + 0.3) * torch.cos(2 * y), -0.02 * torch.cos(x) * torch.sin(y + 1.0)])
+    u0 = (u0 + 0.005 * torch.randn(u0.shape, generator=g, dtype=torch.float64)).to(dev).contiguous()
+    rho = torch.ones((n, n), dtype=torch.float64, device=dev)
+    C9 = torch.tensor([[0, 0], [1, 0], [0, 1], [-1, 0], [0, -1], [1, 1], [-1, 1], [-1, -1], [1, -1]],
+                      dtype=torch.float64, device=dev)
+
+    def ke(u, t):
+        f = torch.empty((9, n, n), dtype=torch.float64, device=dev)
+        E.check(E.init_equilibrium_async("D2Q9", "double", rho, u.contiguous(), f, n, n, 1))
+        h = torch.empty_like(f)
+        for _ in range(steps):
+            E.check(E.launch_step_gpu("D2Q9", "double", "MRT", f, h, n, n, 1, 1.0 / t))
+            f, h = h, f
+        r = f.sum(0)
+        j = torch.einsum("qd,q...->d...", C9, f)
+        return float((0.5 * (j * j).sum(0) / r).sum())
+
+    nb = E.ke_gradient_workspace_bytes("D2Q9", "double", n, n, 1, steps, interval)
+    ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+    out = torch.zeros(2, dtype=torch.float64, device=dev)
+    grad = torch.empty_like(u0)
+    E.check(E.ke_gradient_async("D2Q9", "double", "MRT", rho, u0, n, n, 1, tau, steps, interval, ws, nb, out,
+                                grad))
+    torch.cuda.synchronize()
+    J, dtau = out.tolist()
+    assert abs(J - ke(u0, tau)) <= 1e-12 * abs(J)
+    for _ in range(6):
+        d = torch.randn(u0.shape, generator=g, dtype=torch.float64).to(dev)
+        d /= torch.linalg.vector_norm(d)
+        fd = (ke(u0 + 1e-4 * d, tau) - ke(u0 - 1e-4 * d, tau)) / 2e-4
+        ad = float((grad * d).sum())
+        assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
+    fd_tau = (ke(u0, tau + 1e-6) - ke(u0, tau - 1e-6)) / 2e-6
+    assert abs(fd_tau - dtau) <= 1e-6 * abs(fd_tau) + 1e-13 * abs(J) / 1e-6, (fd_tau, dtau)

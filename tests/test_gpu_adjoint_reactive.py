@@ -86,7 +86,7 @@ CASES = [("D3Q19", (16, 12, 10)), ("D2Q9", (32, 24, 1))]
 
 
 @pytest.mark.parametrize("fl,dims", CASES)
-@pytest.mark.parametrize("op", ["BGK", "TRT"])
+@pytest.mark.parametrize("op", ["BGK", "TRT", "MRT"])
 @pytest.mark.parametrize("obj", ["mean_product", "segregation"])
 def test_reactive_gradient_central_differences_fp64(fl, dims, op, obj):
     dev = torch.device("cuda:0")
