@@ -175,7 +175,8 @@ def test_reactive_gradient_validation(lib):
     assert call(a0=None) == E.cudaErrorInvalidDevicePointer
     assert call(grad_a0=None) == E.cudaErrorInvalidDevicePointer
     assert call(nz=0) == E.cudaErrorInvalidValue
-    assert call(op="MRT") == E.cudaErrorInvalidValue
+    assert call(op="RLBM") == E.cudaErrorInvalidValue
+    assert call(fl="D3Q27", op="MRT") == E.cudaErrorInvalidValue  # MRT adjoint: D2Q9 and D3Q19 only
     assert call(tau=0.5) == E.cudaErrorInvalidValue
     assert call(tau_c=0.4) == E.cudaErrorInvalidValue
     assert call(workspace_bytes=nb - 1) == E.cudaErrorInvalidValue
