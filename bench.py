@@ -411,7 +411,7 @@ def blob_fields(torch, dev, n, block, seed):
     return a.contiguous(), (1.0 - a).contiguous()
 
 
-def run_reactive_adjoint_cost(torch, E, dev, n=192, steps=3000, interval=60, tau=0.56, tau_c=0.55,
+def run_reactive_adjoint_cost(torch, E, dev, n=192, steps=3000, interval=100, tau=0.56, tau_c=0.55,
                               k=0.03 / 16):
     """Reactive adjoint cost: D3Q19 TRT + two D3Q7 scalars (A + B -> C), FP32,
     objective final mean C; gradient w.r.t. k, tau, tau_c and the initial A

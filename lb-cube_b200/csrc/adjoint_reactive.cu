@@ -405,6 +405,13 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
     return fluid_reaction_with_velocity<FL, Real>(collision, c.f, n.f, c.a, n.a, c.b, n.b, n.u, g,
                                                   Real(omega), Real(omega_c), Real(k), s);
   };
+  // states that only pass through the ping-pong slots of the forward pass are
+  // recomputed later: their velocity need not be stored
+  auto step_plain = [&](const State& c, const State& n) {
+    return (cudaError_t)lbm_fluid_reaction_ab_async(FL::id, prec, collision, c.f, n.f, c.a, n.a,
+                                                    c.b, n.b, g.nx, g.ny, g.nz, omega, omega_c, k,
+                                                    nullptr, 0, s);
+  };
 
   // forward: equilibrium initial state, checkpoints every `interval` steps,
   // the last segment's states kept for the backward sweep
@@ -423,13 +430,16 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
   State cur = s0;
   for (int n = 0; n < steps; ++n) {
     State nxt;
-    if (n + 1 == steps || (n + 1) % interval == 0)
+    bool kept = true;
+    if (n + 1 == steps || (n + 1) % interval == 0) {
       nxt = ckpt((n + 1 + interval - 1) / interval);
-    else if (n + 1 > last0)
+    } else if (n + 1 > last0) {
       nxt = seg(n + 1 - last0);
-    else
+    } else {
       nxt = seg(n % 2);
-    if ((err = step(cur, nxt)) != cudaSuccess) return err;
+      kept = false;
+    }
+    if ((err = kept ? step(cur, nxt) : step_plain(cur, nxt)) != cudaSuccess) return err;
     cur = nxt;
   }
 
