@@ -412,37 +412,56 @@ def blob_fields(torch, dev, n, block, seed):
 
 
 def run_reactive_adjoint_cost(torch, E, dev, n=192, steps=3000, interval=100, tau=0.56, tau_c=0.55,
-                              k=0.03 / 16):
-    """Reactive adjoint cost: D3Q19 TRT + two D3Q7 scalars (A + B -> C), FP32,
-    objective final mean C; gradient w.r.t. k, tau, tau_c and the initial A
-    and B fields, over one forward run of the same fused coupled step."""
+                              k=0.03 / 16, storage=None, c0=0.5):
+    """Reactive adjoint cost: D3Q19 TRT + two D3Q7 scalars (A + B -> C), FP32
+    (storage None) or 16-bit shifted population storage in the forward
+    (storage a format; fluid shifted by 1, scalars by c0) with the FP32 adjoint;
+    objective final mean C; gradient w.r.t. k, tau, tau_c and the initial A and
+    B fields, over one forward run of the same coupled step."""
     u0 = solenoidal_field(torch, dev, n, 0.03, 4.0, SEED).float()
     rho0 = torch.ones((n, n, n), dtype=torch.float32, device=dev)
     a0, b0 = blob_fields(torch, dev, n, 16, SEED)
-    nbytes = E.reactive_gradient_workspace_bytes("D3Q19", "float", n, n, n, steps, interval)
+    nbytes = E.reactive_gradient_workspace_bytes("D3Q19", "float", n, n, n, steps, interval, storage=storage)
     ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
     res = torch.zeros(4, dtype=torch.float64, device=dev)
     ga, gb = torch.empty_like(a0), torch.empty_like(b0)
     omega, omega_c = 1.0 / tau, 1.0 / tau_c
     # forward-only run of the same coupled step, in buffers of the workspace
-    f = [ws[:19 * n ** 3 * 4].view(torch.float32).view(19, n, n, n),
-         ws[19 * n ** 3 * 4:38 * n ** 3 * 4].view(torch.float32).view(19, n, n, n)]
-    base = 38 * n ** 3 * 4
-    sc = [ws[base + i * 7 * n ** 3 * 4: base + (i + 1) * 7 * n ** 3 * 4].view(torch.float32).view(7, n, n, n)
+    elem = torch.float32 if storage is None else torch.int16
+    es = 4 if storage is None else 2
+    f = [ws[i * 19 * n ** 3 * es:(i + 1) * 19 * n ** 3 * es].view(elem).view(19, n, n, n) for i in range(2)]
+    base = 38 * n ** 3 * es
+    sc = [ws[base + i * 7 * n ** 3 * es: base + (i + 1) * 7 * n ** 3 * es].view(elem).view(7, n, n, n)
           for i in range(4)]
+    if storage is not None:  # FP32 initial fields, encoded into the 16-bit buffers
+        tf = torch.empty((19, n, n, n), dtype=torch.float32, device=dev)
+        ts = torch.empty((7, n, n, n), dtype=torch.float32, device=dev)
 
     def forward(nsteps):
-        E.check(E.init_equilibrium_async("D3Q19", "float", rho0, u0, f[0], n, n, n))
-        E.check(E.init_equilibrium_async("D3Q7", "float", a0, u0, sc[0], n, n, n))
-        E.check(E.init_equilibrium_async("D3Q7", "float", b0, u0, sc[2], n, n, n))
-        for s in range(nsteps):
-            i, j = s % 2, (s + 1) % 2
-            E.check(E.fluid_reaction_ab_async("D3Q19", "float", "TRT", f[i], f[j], sc[i], sc[j], sc[2 + i],
-                                              sc[2 + j], n, n, n, omega, omega_c, k))
+        if storage is None:
+            E.check(E.init_equilibrium_async("D3Q19", "float", rho0, u0, f[0], n, n, n))
+            E.check(E.init_equilibrium_async("D3Q7", "float", a0, u0, sc[0], n, n, n))
+            E.check(E.init_equilibrium_async("D3Q7", "float", b0, u0, sc[2], n, n, n))
+        else:
+            E.check(E.init_equilibrium_async("D3Q19", "float", rho0, u0, tf, n, n, n))
+            E.check(E.encode_shifted_async("D3Q19", storage, "float", tf, f[0], n, n, n, 1.0))
+            for src, dst in ((a0, sc[0]), (b0, sc[2])):
+                E.check(E.init_equilibrium_async("D3Q7", "float", src, u0, ts, n, n, n))
+                E.check(E.encode_shifted_async("D3Q7", storage, "float", ts, dst, n, n, n, c0))
+        for s_ in range(nsteps):
+            i, j = s_ % 2, (s_ + 1) % 2
+            if storage is None:
+                E.check(E.fluid_reaction_ab_async("D3Q19", "float", "TRT", f[i], f[j], sc[i], sc[j], sc[2 + i],
+                                                  sc[2 + j], n, n, n, omega, omega_c, k))
+            else:
+                E.check(E.fluid_reaction_ab_shifted_async("D3Q19", storage, "TRT", f[i], f[j], sc[i], sc[j],
+                                                          sc[2 + i], sc[2 + j], n, n, n, omega, omega_c, k,
+                                                          1.0, c0))
 
     def gradient(nsteps, nint):
         E.check(E.reactive_gradient_async("D3Q19", "float", "TRT", "mean_product", rho0, u0, a0, b0, n, n, n,
-                                          tau, tau_c, k, nsteps, nint, ws, nbytes, res, ga, gb))
+                                          tau, tau_c, k, nsteps, nint, ws, nbytes, res, ga, gb, storage=storage,
+                                          c0=c0))
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -459,9 +478,11 @@ def run_reactive_adjoint_cost(torch, E, dev, n=192, steps=3000, interval=100, ta
     fwd_ms = timed(lambda: forward(steps))
     grad_ms = timed(lambda: gradient(steps, interval))
     r = res.tolist()
-    out = {"config": f"D3Q19 TRT + 2 x D3Q7 (A + B -> C) FP32 {n}^3, tau {tau}, tau_c {tau_c}, k {k:.6g}, "
-                     f"{steps} steps, solenoidal u0 (amplitude 0.03, spectrum peak |k| = 4), A, B in {{0, 1}} "
-                     f"on interleaved 16^3 blocks, objective final mean C, checkpoint every {interval}",
+    store = "FP32" if storage is None else f"{FORMAT_NOTE[storage]} populations (scalars shifted by {c0})"
+    out = {"config": f"D3Q19 TRT + 2 x D3Q7 (A + B -> C) {n}^3, {store} in the forward, FP32 adjoint, "
+                     f"tau {tau}, tau_c {tau_c}, k {k:.6g}, {steps} steps, solenoidal u0 (amplitude 0.03, "
+                     f"spectrum peak |k| = 4), A, B in {{0, 1}} on interleaved 16^3 blocks, objective final mean "
+                     f"C, checkpoint every {interval}",
            "forward_ms": round(fwd_ms, 2), "gradient_ms": round(grad_ms, 2),
            "cost_ratio": round(grad_ms / fwd_ms, 3), "objective": r[0], "dJ_dk": r[1], "dJ_dtau": r[2],
            "dJ_dtau_c": r[3], "grad_a0_l2": float(torch.linalg.vector_norm(ga.double())),
@@ -784,7 +805,7 @@ def run_engine(args, rank, world, local_rank):
         parallelism = f"{world} independent replicas (16-bit storage has no slab path)"
     peak, peak_kind = measured_hbm_peak()
     traffic = committed_traffic(f"d3q19_float_trt_{NX}") if storage == "fp32" else None
-    variants = accuracy = fp16_store = adjoint = adjoint_reactive = mixing = None
+    variants = accuracy = fp16_store = adjoint = adjoint_reactive = adjoint_reactive_16 = mixing = None
     if world == 1 and not args.no_variants and storage == "fp32":
         variants = run_variants(torch, E, dev, f, peak, ms_per_step)
         del f, g
@@ -792,6 +813,12 @@ def run_engine(args, rank, world, local_rank):
         accuracy = run_accuracy(torch, E, dev)
         adjoint = run_adjoint_cost(torch, E, dev)
         adjoint_reactive = run_reactive_adjoint_cost(torch, E, dev)
+        adjoint_reactive_16 = run_reactive_adjoint_cost(torch, E, dev, storage="f16s")
+        adjoint_reactive_16["vs_fp32"] = {
+            key: round(adjoint_reactive_16[key] / adjoint_reactive[key] - 1.0, 6)
+            for key in ("objective", "dJ_dk", "dJ_dtau_c", "grad_a0_l2")}
+        adjoint_reactive_16["forward_speedup_vs_fp32"] = round(adjoint_reactive["forward_ms"] /
+                                                               adjoint_reactive_16["forward_ms"], 3)
         mixing = run_reactive_mixing(torch, E, dev)
         # per operator: the fastest 16-bit format meeting the 1e-3 velocity error
         # bar, with its speed-up over FP32 storage of the same operator
@@ -819,6 +846,7 @@ def run_engine(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": bytes_per_lu * cells},
         "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps * launches_per_step,
         "fp16_store": fp16_store, "adjoint": adjoint, "adjoint_reactive": adjoint_reactive,
+        "adjoint_reactive_f16s": adjoint_reactive_16,
         "reactive_mixing": mixing,
         "variants": variants, "accuracy": accuracy,
     }

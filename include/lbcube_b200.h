@@ -45,6 +45,7 @@ enum { LBM_D2Q9 = 0, LBM_D3Q19 = 1, LBM_D3Q27 = 2, LBM_D2Q5 = 3, LBM_D3Q7 = 4 };
 enum { LBM_FLOAT = 0, LBM_DOUBLE = 1 };
 enum { LBM_BGK = 0, LBM_TRT = 1, LBM_MRT = 2, LBM_RLBM = 3 };
 enum { LBM_F16S = 2, LBM_BF16S = 3, LBM_E3M12S = 4, LBM_Q15S = 5 };
+enum { LBM_NATIVE = 0 }; /* population storage in the stated precision */
 
 /* ---------------------------------------------------------------------------
  * Fused pull collide-stream step, one symbol per instantiation. Each replaces
@@ -265,6 +266,21 @@ int lbm_fluid_reaction_ab_async(int fluid_lattice, int precision, int collision,
     double omega, double omega_c, double k_react, double* stats_partials,
     size_t stats_partials_bytes, void* stream);
 
+/* The same coupled step on shifted 16-bit populations (`format` LBM_F16S,
+ * LBM_BF16S, LBM_E3M12S or LBM_Q15S; no reference counterpart): the fluid is
+ * stored as codes of S (f_i / w_i - rho0) and collides on the deviations (BGK,
+ * TRT, or MRT on D2Q9 / D3Q19), the scalars as codes of S (g_i / w_i - c0)
+ * (c0 a reference concentration, e.g. 0.5 for fields in [0, 1]), reacted in
+ * FP32 as the FP32 step reacts them; half the bytes of the FP32 step. Fields are
+ * encoded and decoded with lbm_encode_shifted_async / lbm_decode_shifted_async
+ * (rho0 for the fluid, c0 for the scalars). Statistics partials as above, of the
+ * FP32 values the step encodes. */
+int lbm_fluid_reaction_ab_shifted_async(int fluid_lattice, int format, int collision,
+    const void* current_fluid, void* next_fluid, const void* current_a, void* next_a,
+    const void* current_b, void* next_b, size_t x_extent, size_t y_extent, size_t z_extent,
+    double omega, double omega_c, double k_react, float rho0, float c0, double* stats_partials,
+    size_t stats_partials_bytes, void* stream);
+
 /* Bytes of FP64 partial sums the statistics kernels write for this domain. */
 size_t lbm_stats_partials_bytes(int fluid_lattice, size_t x_extent, size_t y_extent,
     size_t z_extent);
@@ -362,13 +378,19 @@ int lbm_adjoint_step_async(int lattice, int precision, int collision, const void
  * the inputs or outputs. Cost: about 2 forward runs + 1 adjoint run. */
 #define LBM_OBJECTIVE_MEAN_PRODUCT 0
 #define LBM_OBJECTIVE_SEGREGATION 1
-size_t lbm_reactive_gradient_workspace_bytes(int fluid_lattice, int precision, size_t x_extent,
-    size_t y_extent, size_t z_extent, int steps, int checkpoint_interval);
-int lbm_reactive_gradient_async(int fluid_lattice, int precision, int collision, int objective,
-    const void* rho0, const void* u0, const void* a0, const void* b0, size_t x_extent,
-    size_t y_extent, size_t z_extent, double tau, double tau_c, double k_react, int steps,
-    int checkpoint_interval, void* workspace, size_t workspace_bytes, double* result,
-    void* grad_a0, void* grad_b0, void* grad_u0, void* stream);
+/* storage: LBM_NATIVE keeps the forward states in `precision`; a 16-bit format
+ * (LBM_F16S, ..., precision LBM_FLOAT) runs the forward and its recomputation
+ * with lbm_fluid_reaction_ab_shifted_async (fluid shifted by 1, scalars by c0)
+ * and stores the states in 16 bits; the adjoint then runs in FP32 about the
+ * decoded states (the rounding is not differentiated: the encoding counts as
+ * the identity). */
+size_t lbm_reactive_gradient_workspace_bytes(int fluid_lattice, int precision, int storage,
+    size_t x_extent, size_t y_extent, size_t z_extent, int steps, int checkpoint_interval);
+int lbm_reactive_gradient_async(int fluid_lattice, int precision, int storage, float c0,
+    int collision, int objective, const void* rho0, const void* u0, const void* a0,
+    const void* b0, size_t x_extent, size_t y_extent, size_t z_extent, double tau, double tau_c,
+    double k_react, int steps, int checkpoint_interval, void* workspace, size_t workspace_bytes,
+    double* result, void* grad_a0, void* grad_b0, void* grad_u0, void* stream);
 
 /* Allocation-free form of lbm_reactive_stats_async. No counterpart in the
  * reference. For callers that cannot allocate device memory, e.g. a plugin or

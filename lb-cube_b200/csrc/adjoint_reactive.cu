@@ -39,10 +39,12 @@
 
 #include "adjoint.cuh"
 #include "adr.cuh"
+#include "adr_shifted.cuh"
 #include "cells.cuh"
 #include "collide.cuh"
 #include "common.cuh"
 #include "reduce.cuh"
+#include "stream_vec.cuh"
 #include "../../include/lbcube_b200.h"
 
 namespace lbcube {
@@ -82,6 +84,48 @@ __device__ __forceinline__ void reaction_source_grad(Real a, Real b, Real k, dou
 struct ReactiveParams {
   AdjointParams fluid;
   double omega_c, k;
+  float rho0, c0;  // shifts of 16-bit stored states (fluid, scalars)
+};
+
+// Access to the stored forward states: native Real fields, or shifted 16-bit
+// codes decoded to FP32 populations (fluid shifted by rho0, scalars by c0).
+template <class Real>
+struct NativeState {
+  using elem = Real;
+  template <class L>
+  __device__ __forceinline__ static void pulled(const elem* __restrict__ p, const Grid& g,
+                                                const Neighbours& n, int x, int y, int z, float,
+                                                Real (&out)[L::Q]) {
+    gather<L>(p, g, n, x, y, z, out);
+  }
+  template <class L>
+  __device__ __forceinline__ static void local(const elem* __restrict__ p, const Grid& g, int cell,
+                                               float, Real (&out)[L::Q]) {
+    load_cell<L>(p, g, cell, out);
+  }
+};
+template <int FMT>
+struct ShiftedState {
+  using elem = unsigned short;
+  template <class L>
+  __device__ __forceinline__ static void pulled(const elem* __restrict__ p, const Grid& g,
+                                                const Neighbours& n, int x, int y, int z, float ref,
+                                                float (&out)[L::Q]) {
+    unsigned short h[L::Q];
+    gather<L>(p, g, n, x, y, z, h);
+    static_for<L::Q>([&](auto I) {
+      out[LB_I(I)] = ShiftedStorage<FMT>::template decode<L, LB_I(I)>(h[LB_I(I)], {ref});
+    });
+  }
+  template <class L>
+  __device__ __forceinline__ static void local(const elem* __restrict__ p, const Grid& g, int cell,
+                                               float ref, float (&out)[L::Q]) {
+    unsigned short h[L::Q];
+    load_cell<L>(p, g, cell, h);
+    static_for<L::Q>([&](auto I) {
+      out[LB_I(I)] = ShiftedStorage<FMT>::template decode<L, LB_I(I)>(h[LB_I(I)], {ref});
+    });
+  }
 };
 
 // Per-block FP64 slots of the reactive adjoint: dJ/dk, dJ/dtau, dJ/domega_c.
@@ -92,9 +136,10 @@ constexpr int kReactiveSlots = 3;
 // (stored by the forward pass), scatter abar and bbar to lambda^n_A, lambda^n_B,
 // write ubar(x) = dJ/du^{n+1}(x) for the fluid part, and add the block's
 // dJ/dk and dJ/domega_c to its slots.
-template <class FL, class Real>
+template <class FL, class Real, class SP>
 __global__ void __launch_bounds__(kThreads)
-    reaction_adjoint_kernel(const Real* __restrict__ an, const Real* __restrict__ bn,
+    reaction_adjoint_kernel(const typename SP::elem* __restrict__ an,
+                            const typename SP::elem* __restrict__ bn,
                             const Real* __restrict__ u_next, const Real* __restrict__ la_next,
                             const Real* __restrict__ lb_next, Real* __restrict__ la,
                             Real* __restrict__ lb, Real* __restrict__ ubar_out, Grid g,
@@ -110,8 +155,8 @@ __global__ void __launch_bounds__(kThreads)
     Real u[FL::D];
     static_for<FL::D>([&](auto D) { u[LB_I(D)] = __ldg(u_next + plane * LB_I(D) + cell); });
     Real ga[SL::Q], gb[SL::Q], lA[SL::Q], lB[SL::Q];
-    gather<SL>(an, g, n, x, y, z, ga);
-    gather<SL>(bn, g, n, x, y, z, gb);
+    SP::template pulled<SL>(an, g, n, x, y, z, rp.c0, ga);
+    SP::template pulled<SL>(bn, g, n, x, y, z, rp.c0, gb);
     load_cell<SL>(la_next, g, cell, lA);
     load_cell<SL>(lb_next, g, cell, lB);
     const Real ca = concentration<SL>(ga), cb = concentration<SL>(gb);
@@ -163,11 +208,12 @@ __global__ void __launch_bounds__(kThreads)
 // (c_k - u) . ubar(x) / rho (u = j / rho of the cell), then the fluid adjoint
 // of adjoint.cuh; dJ/dtau to the block's slot.
 // Five blocks of 128 per SM (96 registers instead of 115).
-template <class FL, class Real, int CT>
+template <class FL, class Real, int CT, class SP>
 __global__ void __launch_bounds__(kThreads, 5)
-    coupled_fluid_adjoint_kernel(const Real* __restrict__ fn, const Real* __restrict__ lf_next,
-                                 const Real* __restrict__ ubar_in, Real* __restrict__ lf, Grid g,
-                                 AdjointParams ap, double* __restrict__ slots) {
+    coupled_fluid_adjoint_kernel(const typename SP::elem* __restrict__ fn,
+                                 const Real* __restrict__ lf_next, const Real* __restrict__ ubar_in,
+                                 Real* __restrict__ lf, Grid g, AdjointParams ap, float rho0,
+                                 double* __restrict__ slots) {
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double dtau = 0.0;
@@ -176,7 +222,7 @@ __global__ void __launch_bounds__(kThreads, 5)
     const int cell = (z * g.ny + y) * g.nx + x;
     const size_t plane = (size_t)g.plane;
     Real gv[FL::Q], lv[FL::Q], mu[FL::Q], rho, u[FL::D], ub[FL::D];
-    gather<FL>(fn, g, n, x, y, z, gv);
+    SP::template pulled<FL>(fn, g, n, x, y, z, rho0, gv);
     load_cell<FL>(lf_next, g, cell, lv);
     static_for<FL::D>([&](auto D) { ub[LB_I(D)] = __ldg(ubar_in + plane * LB_I(D) + cell); });
     macro_state<FL>(gv, rho, u);
@@ -203,12 +249,13 @@ __global__ void __launch_bounds__(kThreads, 5)
 //     la = (C_B / (ma mb) - <ab> / (ma^2 mb)) / N_c,
 //     lb = (C_A / (ma mb) - <ab> / (ma mb^2)) / N_c   (zero when |ma mb| <= eps,
 //     where compute_reactive_stats sets I_s = 0)
-template <class FL, class Real, int OBJ>
+template <class FL, class Real, int OBJ, class SP>
 __global__ void __launch_bounds__(kThreads)
-    reactive_seed_kernel(const Real* __restrict__ aN, const Real* __restrict__ bN,
-                         const Real* __restrict__ a0, const double* __restrict__ stats,
-                         Real* __restrict__ lf, Real* __restrict__ la, Real* __restrict__ lb,
-                         Grid g, double* __restrict__ j_slots) {
+    reactive_seed_kernel(const typename SP::elem* __restrict__ aN,
+                         const typename SP::elem* __restrict__ bN, const Real* __restrict__ a0,
+                         const double* __restrict__ stats, Real* __restrict__ lf,
+                         Real* __restrict__ la, Real* __restrict__ lb, Grid g, float c0,
+                         double* __restrict__ j_slots) {
   using SL = typename ScalarOf<FL>::type;
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
@@ -218,8 +265,8 @@ __global__ void __launch_bounds__(kThreads)
     const size_t plane = (size_t)g.plane;
     const double inv_n = 1.0 / (double)g.plane;
     Real va[SL::Q], vb[SL::Q];
-    load_cell<SL>(aN, g, cell, va);
-    load_cell<SL>(bN, g, cell, vb);
+    SP::template local<SL>(aN, g, cell, c0, va);
+    SP::template local<SL>(bN, g, cell, c0, vb);
     const Real ca = concentration<SL>(va), cb = concentration<SL>(vb);
     Real sa, sb;
     if constexpr (OBJ == LBM_OBJECTIVE_MEAN_PRODUCT) {
@@ -317,30 +364,32 @@ __global__ void __launch_bounds__(kThreads)
   static_for<FL::D>([&](auto D) { grad[plane * LB_I(D) + cell] = gr[LB_I(D)]; });
 }
 
-template <class FL, class Real>
-cudaError_t launch_reactive_adjoint(int collision, const Real* fn, const Real* an, const Real* bn,
+template <class FL, class Real, class SP>
+cudaError_t launch_reactive_adjoint(int collision, const typename SP::elem* fn,
+                                    const typename SP::elem* an, const typename SP::elem* bn,
                                     const Real* u_next, const Real* lf_next, const Real* la_next,
                                     const Real* lb_next, Real* lf, Real* la, Real* lb, Real* ubar,
                                     const Grid& g, const ReactiveParams& rp, double* slots,
                                     cudaStream_t s) {
-  reaction_adjoint_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, s>>>(
+  reaction_adjoint_kernel<FL, Real, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
       an, bn, u_next, la_next, lb_next, la, lb, ubar, g, rp, slots);
   if (collision == kBGK)
-    coupled_fluid_adjoint_kernel<FL, Real, kBGK><<<grid_dims(g), block_dims(g), 0, s>>>(
-        fn, lf_next, ubar, lf, g, rp.fluid, slots);
+    coupled_fluid_adjoint_kernel<FL, Real, kBGK, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
+        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots);
   else if (collision == kTRT)
-    coupled_fluid_adjoint_kernel<FL, Real, kTRT><<<grid_dims(g), block_dims(g), 0, s>>>(
-        fn, lf_next, ubar, lf, g, rp.fluid, slots);
+    coupled_fluid_adjoint_kernel<FL, Real, kTRT, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
+        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots);
   else if constexpr (FL::Q != 27)
-    coupled_fluid_adjoint_kernel<FL, Real, kMRT><<<grid_dims(g), block_dims(g), 0, s>>>(
-        fn, lf_next, ubar, lf, g, rp.fluid, slots);
+    coupled_fluid_adjoint_kernel<FL, Real, kMRT, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
+        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots);
   else
     return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
 struct ReactiveLayout {
-  size_t ffield, sfield, ufield, state;  // bytes: fluid, one scalar, velocity; one state
+  size_t ffield, sfield, ufield, state;  // bytes: fluid, one scalar, velocity; one stored state
+  size_t lfield, lsfield, lstate;        // bytes of the adjoint fields and one adjoint state
   long long ckpts, blocks;
   size_t off_ckpt, off_seg, off_lam, off_ubar, off_slots, off_j, off_part, off_stats, total;
 };
@@ -348,20 +397,25 @@ struct ReactiveLayout {
 // A stored state n holds f^n, A^n, B^n and the velocity u^n that advected the
 // reaction step producing it; an adjoint state holds lambda_f, lambda_A,
 // lambda_B (its velocity slot unused).
-inline ReactiveLayout reactive_layout(int FQ, int SQ, int D, size_t elem, const Grid& g, int steps,
-                                      int interval) {
+// elem: bytes of a stored population (2 for 16-bit states); real: bytes of
+// the adjoint fields and the stored velocity.
+inline ReactiveLayout reactive_layout(int FQ, int SQ, int D, size_t elem, size_t real,
+                                      const Grid& g, int steps, int interval) {
   ReactiveLayout l{};
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
   l.ffield = up((size_t)FQ * g.plane * elem);
   l.sfield = up((size_t)SQ * g.plane * elem);
-  l.ufield = up((size_t)D * g.plane * elem);
+  l.ufield = up((size_t)D * g.plane * real);
   l.state = l.ffield + 2 * l.sfield + l.ufield;
+  l.lfield = up((size_t)FQ * g.plane * real);
+  l.lsfield = up((size_t)SQ * g.plane * real);
+  l.lstate = l.lfield + 2 * l.lsfield;
   l.ckpts = (steps + interval - 1) / interval + 1;
   l.blocks = g.blocks();
   l.off_ckpt = 0;
   l.off_seg = l.off_ckpt + (size_t)l.ckpts * l.state;
   l.off_lam = l.off_seg + (size_t)interval * l.state;
-  l.off_ubar = l.off_lam + 2 * l.state;
+  l.off_ubar = l.off_lam + 2 * l.lstate;
   l.off_slots = l.off_ubar + l.ufield;
   l.off_j = l.off_slots + up((size_t)l.blocks * kReactiveSlots * sizeof(double));
   l.off_part = l.off_j + up((size_t)l.blocks * sizeof(double));
@@ -370,61 +424,99 @@ inline ReactiveLayout reactive_layout(int FQ, int SQ, int D, size_t elem, const 
   return l;
 }
 
-template <class FL, class Real>
+// FMT < 0: states stored in Real; otherwise 16-bit codes of that format (Real
+// is float), fluid shifted by rho0 = 1 and scalars by c0.
+template <class FL, class Real, int FMT>
 cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, const Real* u0,
                               const Real* a0, const Real* b0, const Grid& g, double tau,
-                              double tau_c, double k, int steps, int interval, char* ws,
+                              double tau_c, double k, float c0, int steps, int interval, char* ws,
                               const ReactiveLayout& lay, double* out, Real* grad_a0, Real* grad_b0,
                               Real* grad_u0, cudaStream_t s) {
   using SL = typename ScalarOf<FL>::type;
+  constexpr bool NATIVE = FMT < 0;
+  using SP = std::conditional_t<NATIVE, NativeState<Real>, ShiftedState<(FMT < 0 ? 0 : FMT)>>;
+  using E = typename SP::elem;
   constexpr int prec = sizeof(Real) == 4 ? LBM_FLOAT : LBM_DOUBLE;
+  constexpr int api_format = FMT == kF16S ? LBM_F16S : FMT == kBF16S ? LBM_BF16S
+                           : FMT == kE3M12S ? LBM_E3M12S : LBM_Q15S;
   const double omega = (double)(Real(1) / Real(tau));
   const double omega_c = (double)(Real(1) / Real(tau_c));
   struct State {
+    E* f;
+    E* a;
+    E* b;
+    Real* u;
+  };
+  struct Adj {
     Real* f;
     Real* a;
     Real* b;
-    Real* u;
   };
   auto at = [&](size_t off) {
     char* p = ws + off;
-    return State{reinterpret_cast<Real*>(p), reinterpret_cast<Real*>(p + lay.ffield),
-                 reinterpret_cast<Real*>(p + lay.ffield + lay.sfield),
+    return State{reinterpret_cast<E*>(p), reinterpret_cast<E*>(p + lay.ffield),
+                 reinterpret_cast<E*>(p + lay.ffield + lay.sfield),
                  reinterpret_cast<Real*>(p + lay.ffield + 2 * lay.sfield)};
+  };
+  auto adj = [&](size_t off) {
+    char* p = ws + off;
+    return Adj{reinterpret_cast<Real*>(p), reinterpret_cast<Real*>(p + lay.lfield),
+               reinterpret_cast<Real*>(p + lay.lfield + lay.lsfield)};
   };
   auto ckpt = [&](long long i) { return at(lay.off_ckpt + (size_t)i * lay.state); };
   auto seg = [&](long long i) { return at(lay.off_seg + (size_t)i * lay.state); };
-  const State lam[2] = {at(lay.off_lam), at(lay.off_lam + lay.state)};
+  const Adj lam[2] = {adj(lay.off_lam), adj(lay.off_lam + lay.lstate)};
   double* slots = reinterpret_cast<double*>(ws + lay.off_slots);
   double* j_slots = reinterpret_cast<double*>(ws + lay.off_j);
   double* partials = reinterpret_cast<double*>(ws + lay.off_part);
   double* stats = reinterpret_cast<double*>(ws + lay.off_stats);
   cudaError_t err;
   Real* ubar = reinterpret_cast<Real*>(ws + lay.off_ubar);
-  auto step = [&](const State& c, const State& n) {
-    return fluid_reaction_with_velocity<FL, Real>(collision, c.f, n.f, c.a, n.a, c.b, n.b, n.u, g,
-                                                  Real(omega), Real(omega_c), Real(k), s);
-  };
-  // states that only pass through the ping-pong slots of the forward pass are
-  // recomputed later: their velocity need not be stored
-  auto step_plain = [&](const State& c, const State& n) {
-    return (cudaError_t)lbm_fluid_reaction_ab_async(FL::id, prec, collision, c.f, n.f, c.a, n.a,
-                                                    c.b, n.b, g.nx, g.ny, g.nz, omega, omega_c, k,
-                                                    nullptr, 0, s);
+  // one coupled forward step; `keep_u`: store the advecting velocity with the
+  // new state (states that only pass through the ping-pong slots of the
+  // forward pass are recomputed later and need none)
+  auto step = [&](const State& c, const State& n, bool keep_u) -> cudaError_t {
+    if constexpr (NATIVE) {
+      if (keep_u)
+        return fluid_reaction_with_velocity<FL, Real>(collision, c.f, n.f, c.a, n.a, c.b, n.b, n.u,
+                                                      g, Real(omega), Real(omega_c), Real(k), s);
+      return (cudaError_t)lbm_fluid_reaction_ab_async(FL::id, prec, collision, c.f, n.f, c.a, n.a,
+                                                      c.b, n.b, g.nx, g.ny, g.nz, omega, omega_c, k,
+                                                      nullptr, 0, s);
+    } else {
+      return fluid_reaction_shifted<FL, FMT>(collision, c.f, n.f, c.a, n.a, c.b, n.b,
+                                             keep_u ? n.u : nullptr, nullptr, g, (float)omega,
+                                             (float)omega_c, (float)k, 1.0f, c0, s);
+    }
   };
 
-  // forward: equilibrium initial state, checkpoints every `interval` steps,
-  // the last segment's states kept for the backward sweep
+  // forward: equilibrium initial state (16-bit: built in FP32 in the adjoint
+  // buffers, then encoded), checkpoints every `interval` steps, the last
+  // segment's states kept for the backward sweep
   const State s0 = ckpt(0);
-  if ((err = (cudaError_t)lbm_init_equilibrium_async(FL::id, prec, rho0, u0, s0.f, g.nx, g.ny, g.nz,
-                                                     s)) != cudaSuccess)
-    return err;
-  if ((err = (cudaError_t)lbm_init_equilibrium_async(SL::id, prec, a0, u0, s0.a, g.nx, g.ny, g.nz,
-                                                     s)) != cudaSuccess)
-    return err;
-  if ((err = (cudaError_t)lbm_init_equilibrium_async(SL::id, prec, b0, u0, s0.b, g.nx, g.ny, g.nz,
-                                                     s)) != cudaSuccess)
-    return err;
+  {
+    Real* fi = NATIVE ? reinterpret_cast<Real*>(s0.f) : lam[0].f;
+    Real* ai = NATIVE ? reinterpret_cast<Real*>(s0.a) : lam[0].a;
+    Real* bi = NATIVE ? reinterpret_cast<Real*>(s0.b) : lam[0].b;
+    if ((err = (cudaError_t)lbm_init_equilibrium_async(FL::id, prec, rho0, u0, fi, g.nx, g.ny, g.nz,
+                                                       s)) != cudaSuccess)
+      return err;
+    if ((err = (cudaError_t)lbm_init_equilibrium_async(SL::id, prec, a0, u0, ai, g.nx, g.ny, g.nz,
+                                                       s)) != cudaSuccess)
+      return err;
+    if ((err = (cudaError_t)lbm_init_equilibrium_async(SL::id, prec, b0, u0, bi, g.nx, g.ny, g.nz,
+                                                       s)) != cudaSuccess)
+      return err;
+    if constexpr (!NATIVE) {
+      const int r1 = lbm_encode_shifted_async(FL::id, api_format, LBM_FLOAT, fi, s0.f, g.nx, g.ny,
+                                              g.nz, 1.0f, s);
+      const int r2 = lbm_encode_shifted_async(SL::id, api_format, LBM_FLOAT, ai, s0.a, g.nx, g.ny,
+                                              g.nz, c0, s);
+      const int r3 = lbm_encode_shifted_async(SL::id, api_format, LBM_FLOAT, bi, s0.b, g.nx, g.ny,
+                                              g.nz, c0, s);
+      if (r1 != 0 || r2 != 0 || r3 != 0) return (cudaError_t)(r1 ? r1 : r2 ? r2 : r3);
+    }
+  }
   const long long nseg = (steps + interval - 1) / interval;
   const int last0 = (int)((nseg - 1) * interval);
   State cur = s0;
@@ -439,22 +531,36 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
       nxt = seg(n % 2);
       kept = false;
     }
-    if ((err = kept ? step(cur, nxt) : step_plain(cur, nxt)) != cudaSuccess) return err;
+    if ((err = step(cur, nxt, kept)) != cudaSuccess) return err;
     cur = nxt;
   }
 
   // seed lambda^N and J
-  const State& lN = lam[steps % 2];
+  const Adj& lN = lam[steps % 2];
   if (objective == LBM_OBJECTIVE_SEGREGATION) {
-    err = (cudaError_t)lbm_reactive_stats_async(SL::id, prec, cur.a, cur.b, g.nx, g.ny, g.nz, k,
-                                                partials, (size_t)lay.blocks * kStatSums * sizeof(double),
+    const Real* fa = reinterpret_cast<const Real*>(cur.a);
+    const Real* fb = reinterpret_cast<const Real*>(cur.b);
+    if constexpr (!NATIVE) {  // statistics of the decoded final fields (other adjoint buffer)
+      const Adj& tmp = lam[(steps + 1) % 2];
+      const int r1 = lbm_decode_shifted_async(SL::id, api_format, LBM_FLOAT, cur.a, tmp.a, g.nx,
+                                              g.ny, g.nz, c0, s);
+      const int r2 = lbm_decode_shifted_async(SL::id, api_format, LBM_FLOAT, cur.b, tmp.b, g.nx,
+                                              g.ny, g.nz, c0, s);
+      if (r1 != 0 || r2 != 0) return (cudaError_t)(r1 ? r1 : r2);
+      fa = tmp.a;
+      fb = tmp.b;
+    }
+    err = (cudaError_t)lbm_reactive_stats_async(SL::id, prec, fa, fb, g.nx, g.ny, g.nz, k, partials,
+                                                (size_t)lay.blocks * kStatSums * sizeof(double),
                                                 stats, s);
     if (err != cudaSuccess) return err;
-    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_SEGREGATION><<<grid_dims(g), block_dims(g), 0, s>>>(
-        cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, j_slots);
+    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_SEGREGATION, SP>
+        <<<grid_dims(g), block_dims(g), 0, s>>>(cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, c0,
+                                                j_slots);
   } else {
-    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_MEAN_PRODUCT><<<grid_dims(g), block_dims(g), 0, s>>>(
-        cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, j_slots);
+    reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_MEAN_PRODUCT, SP>
+        <<<grid_dims(g), block_dims(g), 0, s>>>(cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, c0,
+                                                j_slots);
   }
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
   if ((err = cudaMemsetAsync(slots, 0, (size_t)lay.blocks * kReactiveSlots * sizeof(double), s)) !=
@@ -465,26 +571,29 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
   rp.fluid = make_params<Real>(collision, tau);
   rp.omega_c = omega_c;
   rp.k = (double)Real(k);
+  rp.rho0 = 1.0f;
+  rp.c0 = c0;
   for (long long kk = nseg - 1; kk >= 0; --kk) {
     const int n0 = (int)(kk * interval);
     const int n1 = (int)std::min<long long>((long long)steps, (kk + 1) * interval);
     State src = ckpt(kk);
     for (int n = n0 + 1; n < n1 && kk < nseg - 1; ++n) {
-      if ((err = step(src, seg(n - n0))) != cudaSuccess) return err;
+      if ((err = step(src, seg(n - n0), true)) != cudaSuccess) return err;
       src = seg(n - n0);
     }
     for (int n = n1 - 1; n >= n0; --n) {
       const State sn = n == n0 ? ckpt(kk) : seg(n - n0);
       const State sn1 = n + 1 == n1 ? ckpt(kk + 1) : seg(n + 1 - n0);  // holds u^{n+1}
-      const State& ln = lam[(n + 1) % 2];
-      const State& l = lam[n % 2];
-      err = launch_reactive_adjoint<FL, Real>(collision, sn.f, sn.a, sn.b, sn1.u, ln.f, ln.a, ln.b,
-                                              l.f, l.a, l.b, ubar, g, rp, slots, s);
+      const Adj& ln = lam[(n + 1) % 2];
+      const Adj& l = lam[n % 2];
+      err = launch_reactive_adjoint<FL, Real, SP>(collision, sn.f, sn.a, sn.b, sn1.u, ln.f, ln.a,
+                                                  ln.b, l.f, l.a, l.b, ubar, g, rp, slots, s);
       if (err != cudaSuccess) return err;
     }
   }
 
-  // results: J, dJ/dk, dJ/dtau, dJ/dtau_c; dJ/dA0 (and dJ/dB0)
+  // results: J, dJ/dk, dJ/dtau, dJ/dtau_c; dJ/dA0 (and dJ/dB0, dJ/du0). For
+  // 16-bit states the encoding of the initial state counts as the identity.
   const Real direct_a = objective == LBM_OBJECTIVE_MEAN_PRODUCT ? Real(1.0 / (double)g.plane) : Real(0);
   scalar_init_gradient_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, s>>>(u0, lam[0].a, direct_a,
                                                                           grad_a0, g);
@@ -513,12 +622,18 @@ inline int fluid_q(int fluid_lattice) {
   return fluid_lattice == kD2Q9 ? 9 : (fluid_lattice == kD3Q19 ? 19 : 27);
 }
 
+// storage: LBM_NATIVE (states in Real) or a 16-bit format (Real float).
+inline int storage_fmt(int storage) {
+  return storage == LBM_F16S ? kF16S : storage == LBM_BF16S ? kBF16S
+       : storage == LBM_E3M12S ? kE3M12S : storage == LBM_Q15S ? kQ15S : -1;
+}
+
 template <class Real>
-cudaError_t reactive_dispatch(int lattice, int collision, int objective, const void* rho0,
-                              const void* u0, const void* a0, const void* b0, size_t nx, size_t ny,
-                              size_t nz, double tau, double tau_c, double k, int steps,
-                              int interval, void* ws, size_t ws_bytes, double* out, void* grad_a0,
-                              void* grad_b0, void* grad_u0, cudaStream_t s) {
+cudaError_t reactive_dispatch(int lattice, int storage, float c0, int collision, int objective,
+                              const void* rho0, const void* u0, const void* a0, const void* b0,
+                              size_t nx, size_t ny, size_t nz, double tau, double tau_c, double k,
+                              int steps, int interval, void* ws, size_t ws_bytes, double* out,
+                              void* grad_a0, void* grad_b0, void* grad_u0, cudaStream_t s) {
   Grid g;
   const int dims = lattice == kD2Q9 ? 2 : 3;
   cudaError_t err = validate_domain(rho0 == nullptr || u0 == nullptr || a0 == nullptr ||
@@ -532,20 +647,33 @@ cudaError_t reactive_dispatch(int lattice, int collision, int objective, const v
       (objective != LBM_OBJECTIVE_MEAN_PRODUCT && objective != LBM_OBJECTIVE_SEGREGATION) ||
       !(tau > 0.5) || !(tau_c > 0.5))
     return cudaErrorInvalidValue;
+  const int fmt = storage_fmt(storage);
+  if (storage != LBM_NATIVE && (fmt < 0 || sizeof(Real) != 4)) return cudaErrorInvalidValue;
   const ReactiveLayout lay = reactive_layout(fluid_q(lattice), scalar_q(lattice), dims,
-                                             sizeof(Real), g, steps, interval);
+                                             fmt < 0 ? sizeof(Real) : 2, sizeof(Real), g, steps,
+                                             interval);
   if (ws_bytes < lay.total) return cudaErrorInvalidValue;
   char* w = static_cast<char*>(ws);
-#define LBCUBE_REACTIVE(FL)                                                                        \
-  return reactive_gradient<FL, Real>(collision, objective, (const Real*)rho0, (const Real*)u0,     \
-                                     (const Real*)a0, (const Real*)b0, g, tau, tau_c, k, steps,    \
-                                     interval, w, lay, out, (Real*)grad_a0, (Real*)grad_b0,     \
-                                     (Real*)grad_u0, s)
+#define LBCUBE_REACTIVE(FL, F)                                                                     \
+  return reactive_gradient<FL, Real, F>(collision, objective, (const Real*)rho0, (const Real*)u0,  \
+                                        (const Real*)a0, (const Real*)b0, g, tau, tau_c, k, c0,    \
+                                        steps, interval, w, lay, out, (Real*)grad_a0,              \
+                                        (Real*)grad_b0, (Real*)grad_u0, s)
+#define LBCUBE_REACTIVE_FMT(FL)                                                                    \
+  if (fmt < 0) LBCUBE_REACTIVE(FL, -1);                                                            \
+  if constexpr (sizeof(Real) == 4) {                                                               \
+    if (fmt == kF16S) LBCUBE_REACTIVE(FL, kF16S);                                                  \
+    if (fmt == kBF16S) LBCUBE_REACTIVE(FL, kBF16S);                                                \
+    if (fmt == kE3M12S) LBCUBE_REACTIVE(FL, kE3M12S);                                              \
+    if (fmt == kQ15S) LBCUBE_REACTIVE(FL, kQ15S);                                                  \
+  }                                                                                                \
+  return cudaErrorInvalidValue;
   switch (lattice) {
-    case kD2Q9: LBCUBE_REACTIVE(D2Q9);
-    case kD3Q19: LBCUBE_REACTIVE(D3Q19);
-    default: LBCUBE_REACTIVE(D3Q27);
+    case kD2Q9: { LBCUBE_REACTIVE_FMT(D2Q9) }
+    case kD3Q19: { LBCUBE_REACTIVE_FMT(D3Q19) }
+    default: { LBCUBE_REACTIVE_FMT(D3Q27) }
   }
+#undef LBCUBE_REACTIVE_FMT
 #undef LBCUBE_REACTIVE
 }
 
@@ -554,9 +682,9 @@ cudaError_t reactive_dispatch(int lattice, int collision, int objective, const v
 using namespace lbcube;
 
 extern "C" size_t lbm_reactive_gradient_workspace_bytes(int fluid_lattice, int precision,
-                                                        size_t x_extent, size_t y_extent,
-                                                        size_t z_extent, int steps,
-                                                        int checkpoint_interval) {
+                                                        int storage, size_t x_extent,
+                                                        size_t y_extent, size_t z_extent,
+                                                        int steps, int checkpoint_interval) {
   Grid g;
   if (fluid_lattice != LBM_D2Q9 && fluid_lattice != LBM_D3Q19 && fluid_lattice != LBM_D3Q27)
     return 0;
@@ -565,30 +693,33 @@ extern "C" size_t lbm_reactive_gradient_workspace_bytes(int fluid_lattice, int p
     return 0;
   if (steps < 1 || checkpoint_interval < 2) return 0;
   if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return 0;
+  const int fmt = storage_fmt(storage);
+  if (storage != LBM_NATIVE && (fmt < 0 || precision != LBM_FLOAT)) return 0;
+  const size_t real = precision == LBM_DOUBLE ? 8 : 4;
   return reactive_layout(fluid_q(fluid_lattice), scalar_q(fluid_lattice), dims,
-                         precision == LBM_DOUBLE ? 8 : 4, g, steps, checkpoint_interval)
+                         fmt < 0 ? real : 2, real, g, steps, checkpoint_interval)
       .total;
 }
 
-extern "C" int lbm_reactive_gradient_async(int fluid_lattice, int precision, int collision,
-                                           int objective, const void* rho0, const void* u0,
-                                           const void* a0, const void* b0, size_t x_extent,
-                                           size_t y_extent, size_t z_extent, double tau,
-                                           double tau_c, double k_react, int steps,
-                                           int checkpoint_interval, void* workspace,
-                                           size_t workspace_bytes, double* result,
-                                           void* grad_a0, void* grad_b0, void* grad_u0,
-                                           void* stream) {
+extern "C" int lbm_reactive_gradient_async(int fluid_lattice, int precision, int storage,
+                                           float c0, int collision, int objective,
+                                           const void* rho0, const void* u0, const void* a0,
+                                           const void* b0, size_t x_extent, size_t y_extent,
+                                           size_t z_extent, double tau, double tau_c,
+                                           double k_react, int steps, int checkpoint_interval,
+                                           void* workspace, size_t workspace_bytes,
+                                           double* result, void* grad_a0, void* grad_b0,
+                                           void* grad_u0, void* stream) {
   const cudaStream_t s = as_stream(stream);
   if (precision == LBM_FLOAT)
-    return (int)reactive_dispatch<float>(fluid_lattice, collision, objective, rho0, u0, a0, b0,
-                                         x_extent, y_extent, z_extent, tau, tau_c, k_react, steps,
-                                         checkpoint_interval, workspace, workspace_bytes, result,
-                                         grad_a0, grad_b0, grad_u0, s);
+    return (int)reactive_dispatch<float>(fluid_lattice, storage, c0, collision, objective, rho0,
+                                         u0, a0, b0, x_extent, y_extent, z_extent, tau, tau_c,
+                                         k_react, steps, checkpoint_interval, workspace,
+                                         workspace_bytes, result, grad_a0, grad_b0, grad_u0, s);
   if (precision == LBM_DOUBLE)
-    return (int)reactive_dispatch<double>(fluid_lattice, collision, objective, rho0, u0, a0, b0,
-                                          x_extent, y_extent, z_extent, tau, tau_c, k_react, steps,
-                                          checkpoint_interval, workspace, workspace_bytes, result,
-                                          grad_a0, grad_b0, grad_u0, s);
+    return (int)reactive_dispatch<double>(fluid_lattice, storage, c0, collision, objective, rho0,
+                                          u0, a0, b0, x_extent, y_extent, z_extent, tau, tau_c,
+                                          k_react, steps, checkpoint_interval, workspace,
+                                          workspace_bytes, result, grad_a0, grad_b0, grad_u0, s);
   return (int)cudaErrorInvalidValue;
 }

@@ -1,0 +1,200 @@
+// The coupled fluid + A + B -> C step (fluid_reaction_kernel of adr.cu) on
+// shifted 16-bit populations. No reference counterpart.
+//
+// The fluid is stored as codes of v_i = S (f_i / w_i - rho0) and collides on
+// the deviations (collide_dev / collide_dev_mrt); the two scalars are stored as
+// codes of S (g_i / w_i - c0) with c0 a reference concentration, decoded to
+// FP32, advected and reacted exactly as in the FP32 step (react_pair: the
+// scalar BGK with the exact A + B -> C source, lattice_physics.hpp:677-743)
+// with the fluid velocity of the post-collision deviations, and re-encoded.
+// Halves the bytes of the coupled step (D3Q19 + 2 D3Q7: 132 B per cell
+// instead of 264). Statistics, when requested, are those of the FP32 values
+// the step encodes.
+#include "adr_shifted.cuh"
+#include "cells.cuh"
+#include "collide.cuh"
+#include "collide_dev.cuh"
+#include "common.cuh"
+#include "reduce.cuh"
+#include "stream_vec.cuh"
+#include "../../include/lbcube_b200.h"
+
+namespace lbcube {
+
+// Pull-gather of 16-bit codes, decoded to deviations (fluid) or to
+// populations (scalars, shifted by c0).
+template <class L, int FMT, bool DEVIATION>
+__device__ __forceinline__ void gather_codes(const unsigned short* __restrict__ cur, const Grid& g,
+                                             const Neighbours& n, int x, int y, int z, float c0,
+                                             float (&out)[L::Q]) {
+  const size_t plane = (size_t)g.plane;
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    const int sx = cx == 0 ? x : (cx > 0 ? n.xm : n.xp);
+    const int sy = cy == 0 ? y : (cy > 0 ? n.ym : n.yp);
+    const int sz = cz == 0 ? z : (cz > 0 ? n.zm : n.zp);
+    const unsigned short h = __ldg(cur + plane * i + ((sz * g.ny + sy) * g.nx + sx));
+    if constexpr (DEVIATION) out[i] = Codec<FMT>::decode(h);
+    else out[i] = ShiftedStorage<FMT>::template decode<L, i>(h, {c0});
+  });
+}
+
+template <class FL, int FMT, int CT, bool STATS, bool UOUT>
+__global__ void __launch_bounds__(kThreads)
+    fluid_reaction_shifted_kernel(const unsigned short* __restrict__ cur_f,
+                                  unsigned short* __restrict__ nxt_f,
+                                  const unsigned short* __restrict__ cur_a,
+                                  unsigned short* __restrict__ nxt_a,
+                                  const unsigned short* __restrict__ cur_b,
+                                  unsigned short* __restrict__ nxt_b, Grid g, float omega,
+                                  float omega_minus, float omega_c, float k, float rho0, float c0,
+                                  double* __restrict__ partials, float* __restrict__ u_out) {
+  using SL = typename ScalarOf<FL>::type;
+  int x, y, z;
+  const bool active = cell_of(g, x, y, z);
+  double sums[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (active) {
+    const int cell = (z * g.ny + y) * g.nx + x;
+    const size_t plane = (size_t)g.plane;
+    const Neighbours n = neighbours(g, x, y, z);
+    float v[FL::Q], u[FL::D];
+    gather_codes<FL, FMT, true>(cur_f, g, n, x, y, z, 0.0f, v);
+    if constexpr (CT == kMRT) collide_dev_mrt<FL, FMT>(v, omega, rho0);
+    else collide_dev<FL, CT, FMT>(v, omega, omega_minus, rho0);
+    static_for<FL::Q>([&](auto I) { nxt_f[plane * LB_I(I) + cell] = Codec<FMT>::encode(v[LB_I(I)]); });
+    dev_velocity<FL, FMT>(v, rho0, u);
+    if constexpr (UOUT) static_for<FL::D>([&](auto D) { u_out[plane * LB_I(D) + cell] = u[LB_I(D)]; });
+    float a[SL::Q], b[SL::Q];
+    gather_codes<SL, FMT, false>(cur_a, g, n, x, y, z, c0, a);
+    gather_codes<SL, FMT, false>(cur_b, g, n, x, y, z, c0, b);
+    const float ca = concentration<SL>(a), cb = concentration<SL>(b);
+    const float src = reaction_source<float>(ca, cb, k);
+    collide_scalar<SL>(a, u, omega_c, src);
+    collide_scalar<SL>(b, u, omega_c, src);
+    const typename ShiftedStorage<FMT>::Params sp{c0};
+    static_for<SL::Q>([&](auto I) {
+      constexpr int i = LB_I(I);
+      nxt_a[plane * i + cell] = ShiftedStorage<FMT>::template encode<SL, i>(a[i], sp);
+      nxt_b[plane * i + cell] = ShiftedStorage<FMT>::template encode<SL, i>(b[i], sp);
+    });
+    if constexpr (STATS) {
+      const double sa = (double)concentration<SL>(a), sb = (double)concentration<SL>(b);
+      sums[0] = sa;
+      sums[1] = sb;
+      sums[2] = sa * sa;
+      sums[3] = sb * sb;
+      sums[4] = sa * sb;
+    }
+  }
+  if constexpr (STATS) block_sum_to<kStatSums>(sums, partials + block_linear() * kStatSums);
+}
+
+template <class FL, int FMT, int CT>
+cudaError_t launch_shifted_coupled(const unsigned short* cf, unsigned short* nf,
+                                   const unsigned short* ca, unsigned short* na,
+                                   const unsigned short* cb, unsigned short* nb, float* u_out,
+                                   double* partials, const Grid& g, float omega, float omega_c,
+                                   float k, float rho0, float c0, cudaStream_t s) {
+  const float om = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
+#define LBCUBE_SC(ST, UO)                                                                          \
+  fluid_reaction_shifted_kernel<FL, FMT, CT, ST, UO><<<grid_dims(g), block_dims(g), 0, s>>>(      \
+      cf, nf, ca, na, cb, nb, g, omega, om, omega_c, k, rho0, c0, partials, u_out)
+  if (partials != nullptr && u_out != nullptr) LBCUBE_SC(true, true);
+  else if (partials != nullptr) LBCUBE_SC(true, false);
+  else if (u_out != nullptr) LBCUBE_SC(false, true);
+  else LBCUBE_SC(false, false);
+#undef LBCUBE_SC
+  return cudaGetLastError();
+}
+
+template <class FL, int FMT>
+cudaError_t fluid_reaction_shifted(int collision, const unsigned short* cur_f,
+                                   unsigned short* nxt_f, const unsigned short* cur_a,
+                                   unsigned short* nxt_a, const unsigned short* cur_b,
+                                   unsigned short* nxt_b, float* u_out, double* partials,
+                                   const Grid& g, float omega, float omega_c, float k, float rho0,
+                                   float c0, cudaStream_t s) {
+  switch (collision) {
+    case kBGK:
+      return launch_shifted_coupled<FL, FMT, kBGK>(cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, u_out,
+                                                   partials, g, omega, omega_c, k, rho0, c0, s);
+    case kTRT:
+      return launch_shifted_coupled<FL, FMT, kTRT>(cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, u_out,
+                                                   partials, g, omega, omega_c, k, rho0, c0, s);
+    case kMRT:
+      if constexpr (FL::Q != 27)
+        return launch_shifted_coupled<FL, FMT, kMRT>(cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b,
+                                                     u_out, partials, g, omega, omega_c, k, rho0,
+                                                     c0, s);
+      return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+#define LBCUBE_FRS(FL, F)                                                                         \
+  template cudaError_t fluid_reaction_shifted<FL, F>(                                             \
+      int, const unsigned short*, unsigned short*, const unsigned short*, unsigned short*,        \
+      const unsigned short*, unsigned short*, float*, double*, const Grid&, float, float, float,  \
+      float, float, cudaStream_t);
+#define LBCUBE_FRS_ALL(FL) LBCUBE_FRS(FL, kF16S) LBCUBE_FRS(FL, kBF16S) LBCUBE_FRS(FL, kE3M12S) LBCUBE_FRS(FL, kQ15S)
+LBCUBE_FRS_ALL(D2Q9)
+LBCUBE_FRS_ALL(D3Q19)
+LBCUBE_FRS_ALL(D3Q27)
+#undef LBCUBE_FRS_ALL
+#undef LBCUBE_FRS
+
+template <int FMT>
+cudaError_t coupled_by_lattice(int lattice, int collision, const void* cf, void* nf, const void* ca,
+                               void* na, const void* cb, void* nb, size_t nx, size_t ny, size_t nz,
+                               double omega, double omega_c, double k, float rho0, float c0,
+                               double* partials, size_t pbytes, cudaStream_t s) {
+  const int dims = lattice == kD2Q9 ? 2 : 3;
+  Grid g;
+  cudaError_t err = validate_domain(cf == nullptr || nf == nullptr || ca == nullptr ||
+                                        na == nullptr || cb == nullptr || nb == nullptr,
+                                    1, 1, 1, dims, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  const int FQ = lattice == kD2Q9 ? 9 : (lattice == kD3Q19 ? 19 : 27), SQ = dims == 2 ? 5 : 7;
+  const size_t fb = (size_t)FQ * g.plane * 2, sb = (size_t)SQ * g.plane * 2;
+  const size_t need = partials != nullptr ? (size_t)g.blocks() * kStatSums * sizeof(double) : 0;
+  if (partials != nullptr && pbytes < need) return cudaErrorInvalidValue;
+  const Span reads[3] = {{cf, fb}, {ca, sb}, {cb, sb}};
+  const Span writes[4] = {{nf, fb}, {na, sb}, {nb, sb}, {partials, need}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  using U = unsigned short;
+#define LBCUBE_CL(FL)                                                                             \
+  return fluid_reaction_shifted<FL, FMT>(collision, (const U*)cf, (U*)nf, (const U*)ca, (U*)na, \
+                                         (const U*)cb, (U*)nb, nullptr, partials, g, (float)omega, \
+                                         (float)omega_c, (float)k, rho0, c0, s)
+  switch (lattice) {
+    case kD2Q9: LBCUBE_CL(D2Q9);
+    case kD3Q19: LBCUBE_CL(D3Q19);
+    case kD3Q27: LBCUBE_CL(D3Q27);
+    default: return cudaErrorInvalidValue;
+  }
+#undef LBCUBE_CL
+}
+
+}  // namespace lbcube
+
+using namespace lbcube;
+
+extern "C" int lbm_fluid_reaction_ab_shifted_async(
+    int fluid_lattice, int format, int collision, const void* current_fluid, void* next_fluid,
+    const void* current_a, void* next_a, const void* current_b, void* next_b, size_t x_extent,
+    size_t y_extent, size_t z_extent, double omega, double omega_c, double k_react, float rho0,
+    float c0, double* stats_partials, size_t stats_partials_bytes, void* stream) {
+  const cudaStream_t s = as_stream(stream);
+#define LBCUBE_FMT(F)                                                                              \
+  return (int)coupled_by_lattice<F>(fluid_lattice, collision, current_fluid, next_fluid,          \
+                                    current_a, next_a, current_b, next_b, x_extent, y_extent,     \
+                                    z_extent, omega, omega_c, k_react, rho0, c0, stats_partials,  \
+                                    stats_partials_bytes, s)
+  if (format == LBM_F16S) LBCUBE_FMT(kF16S);
+  if (format == LBM_BF16S) LBCUBE_FMT(kBF16S);
+  if (format == LBM_E3M12S) LBCUBE_FMT(kE3M12S);
+  if (format == LBM_Q15S) LBCUBE_FMT(kQ15S);
+#undef LBCUBE_FMT
+  return (int)cudaErrorInvalidValue;
+}

@@ -210,6 +210,26 @@ __device__ __forceinline__ void collide_dev(float (&v)[L::Q], float omega, float
   });
 }
 
+// Velocity u = j / rho of deviation variables v (the moments of collide_dev).
+template <class L, int FMT>
+__device__ __forceinline__ void dev_velocity(const float (&v)[L::Q], float rho0, float (&u)[L::D]) {
+  constexpr float S = Codec<FMT>::S;
+  float dv = 0.0f, j[L::D];
+  static_for<L::D>([&](auto D) { j[LB_I(D)] = 0.0f; });
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr float w = (float)L::w[i];
+    dv = fmaf(w, v[i], dv);
+    static_for<L::D>([&](auto D) {
+      constexpr int c = L::c[i][LB_I(D)];
+      if constexpr (c > 0) j[LB_I(D)] = fmaf(w, v[i], j[LB_I(D)]);
+      if constexpr (c < 0) j[LB_I(D)] = fmaf(-w, v[i], j[LB_I(D)]);
+    });
+  });
+  const float inv = __frcp_rn(fmaf(S, rho0, dv));
+  static_for<L::D>([&](auto D) { u[LB_I(D)] = j[LB_I(D)] * inv; });
+}
+
 // ---- MRT on deviation variables (D2Q9, D3Q19) -----------------------------------
 // The reference MRT (collide_mrt_d2q9, lattice_mrt.hpp:586-603; collide_mrt_d3q19,
 // :971-1009) relaxes the orthogonal moments m = M f towards m_eq and maps back

@@ -99,8 +99,11 @@ def _declare(lib):
         "lbm_ke_gradient_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, C.c_int, C.c_int,
                                   _vp, _sz, _vp, _vp, _vp],
         "lbm_adjoint_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp],
-        "lbm_reactive_gradient_async": [C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _sz, _sz, _sz,
-                                        d, d, d, C.c_int, C.c_int, _vp, _sz, _vp, _vp, _vp, _vp, _vp],
+        "lbm_reactive_gradient_async": [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, _vp, _vp, _vp,
+                                        _vp, _sz, _sz, _sz, d, d, d, C.c_int, C.c_int, _vp, _sz, _vp, _vp,
+                                        _vp, _vp, _vp],
+        "lbm_fluid_reaction_ab_shifted_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _sz,
+                                                _sz, _sz, d, d, d, C.c_float, C.c_float, _vp, _sz, _vp],
         "lbm_step_slab_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp, _vp, _vp, _sz,
                                 _sz, _vp],
         "lbm_slab_pack_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
@@ -121,7 +124,8 @@ def _declare(lib):
     lib.lbm_slab_face_elems.restype = C.c_size_t
     lib.lbm_slab_face_elems.argtypes = [C.c_int, _sz, _sz]
     lib.lbm_reactive_gradient_workspace_bytes.restype = C.c_size_t
-    lib.lbm_reactive_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, _sz, _sz, _sz, C.c_int, C.c_int]
+    lib.lbm_reactive_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, C.c_int, _sz, _sz, _sz, C.c_int,
+                                                          C.c_int]
     lib.lbm_diagnostics_partials_bytes.restype = C.c_size_t
     lib.lbm_diagnostics_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
     lib.lbm_ke_gradient_workspace_bytes.restype = C.c_size_t
@@ -244,6 +248,16 @@ def fluid_reaction_ab_async(fluid_lattice, real, collision, cur_f, nxt_f, cur_a,
         float(omega_c), float(k_react), _ptr(partials), int(partials_bytes), _stream(stream))
 
 
+def fluid_reaction_ab_shifted_async(fluid_lattice, fmt, collision, cur_f, nxt_f, cur_a, nxt_a, cur_b,
+                                    nxt_b, nx, ny, nz, omega, omega_c, k_react, rho0=1.0, c0=0.5,
+                                    partials=None, partials_bytes=0, stream=None) -> int:
+    """The coupled fluid + A + B -> C step on shifted 16-bit populations."""
+    return load().lbm_fluid_reaction_ab_shifted_async(
+        LATTICES[fluid_lattice], FORMATS[fmt], COLLISIONS[collision], _ptr(cur_f), _ptr(nxt_f), _ptr(cur_a),
+        _ptr(nxt_a), _ptr(cur_b), _ptr(nxt_b), nx, ny, nz, float(omega), float(omega_c), float(k_react),
+        float(rho0), float(c0), _ptr(partials), int(partials_bytes), _stream(stream))
+
+
 def reactive_stats_async(scalar_lattice, real, a, b, nx, ny, nz, k_react, partials, partials_bytes,
                          diagnostics, stream=None) -> int:
     return load().lbm_reactive_stats_async(LATTICES[scalar_lattice], REALS[real_name(real)], _ptr(a),
@@ -312,19 +326,25 @@ def adjoint_step_async(lattice, real, collision, populations, lambda_next, lam, 
 OBJECTIVES = {"mean_product": 0, "segregation": 1}
 
 
-def reactive_gradient_workspace_bytes(fluid_lattice, real, nx, ny, nz, steps, interval) -> int:
+def _storage(storage):
+    return 0 if storage in (None, "native") else FORMATS[storage]
+
+
+def reactive_gradient_workspace_bytes(fluid_lattice, real, nx, ny, nz, steps, interval, storage=None) -> int:
     return load().lbm_reactive_gradient_workspace_bytes(LATTICES[fluid_lattice], REALS[real_name(real)],
-                                                        nx, ny, nz, int(steps), int(interval))
+                                                        _storage(storage), nx, ny, nz, int(steps), int(interval))
 
 
 def reactive_gradient_async(fluid_lattice, real, collision, objective, rho0, u0, a0, b0, nx, ny, nz,
                             tau, tau_c, k_react, steps, interval, workspace, workspace_bytes, result,
-                            grad_a0, grad_b0=None, grad_u0=None, stream=None) -> int:
+                            grad_a0, grad_b0=None, grad_u0=None, storage=None, c0=0.5, stream=None) -> int:
     """Checkpointed adjoint of the coupled fluid + A + B -> C run: result
     (device FP64[4]) = J, dJ/dk, dJ/dtau, dJ/dtau_c; grad_a0 (grad_b0,
-    grad_u0) = dJ/da0 (dJ/db0, dJ/du0). objective in OBJECTIVES."""
+    grad_u0) = dJ/da0 (dJ/db0, dJ/du0). objective in OBJECTIVES; storage None
+    (states in `real`) or a 16-bit format of FORMATS (scalars shifted by c0)."""
     return load().lbm_reactive_gradient_async(
-        LATTICES[fluid_lattice], REALS[real_name(real)], COLLISIONS[collision], OBJECTIVES[objective],
+        LATTICES[fluid_lattice], REALS[real_name(real)], _storage(storage), float(c0), COLLISIONS[collision],
+        OBJECTIVES[objective],
         _ptr(rho0), _ptr(u0), _ptr(a0), _ptr(b0), nx, ny, nz, float(tau), float(tau_c), float(k_react),
         int(steps), int(interval), _ptr(workspace), int(workspace_bytes), _ptr(result), _ptr(grad_a0),
         _ptr(grad_b0), _ptr(grad_u0), _stream(stream))

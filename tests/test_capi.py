@@ -181,5 +181,14 @@ def test_reactive_gradient_validation(lib):
     assert call(tau_c=0.4) == E.cudaErrorInvalidValue
     assert call(workspace_bytes=nb - 1) == E.cudaErrorInvalidValue
     assert call(steps=0) == E.cudaErrorInvalidValue
-    assert E.load().lbm_reactive_gradient_async(1, 0, 1, 7, A0, A1, A2, A3, 16, 12, 10, 0.8, 0.7, 0.1, 20, 4,
-                                                A4, nb, A4 + 8, A4 + 16, None, None, None) == E.cudaErrorInvalidValue
+    assert E.load().lbm_reactive_gradient_async(1, 0, 0, 0.5, 1, 7, A0, A1, A2, A3, 16, 12, 10, 0.8, 0.7, 0.1,
+                                                20, 4, A4, nb, A4 + 8, A4 + 16, None, None, None) == \
+        E.cudaErrorInvalidValue
+    # 16-bit stored states: FP32 only, and a known format
+    nb16 = E.reactive_gradient_workspace_bytes("D3Q19", "float", 16, 12, 10, 20, 4, storage="f16s")
+    assert 0 < nb16 < nb
+    assert E.reactive_gradient_workspace_bytes("D3Q19", "double", 16, 12, 10, 20, 4, storage="f16s") == 0
+    assert call(real="double", storage="q15s") == E.cudaErrorInvalidValue
+    assert E.load().lbm_reactive_gradient_async(1, 0, 9, 0.5, 1, 0, A0, A1, A2, A3, 16, 12, 10, 0.8, 0.7, 0.1,
+                                                20, 4, A4, nb, A4 + 8, A4 + 16, None, None, None) == \
+        E.cudaErrorInvalidValue

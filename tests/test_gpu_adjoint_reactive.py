@@ -143,3 +143,28 @@ def test_reactive_gradient_fp32_follows_fp64():
         assert abs(r32[q] - r64[q]) <= 2e-3 * abs(r64[q]) + 1e-9, (q, r32[q], r64[q])
     err = float(torch.linalg.vector_norm(ga32.double() - ga64) / torch.linalg.vector_norm(ga64))
     assert err <= 1e-3, err
+
+
+@pytest.mark.parametrize("fmt", ["f16s", "q15s"])
+def test_reactive_gradient_16bit_states_follow_fp32(fmt):
+    """Forward in 16-bit shifted storage (fluid by 1, scalars by 0.5), adjoint in
+    FP32 about the decoded states: J and the gradients follow the all-FP32 ones
+    (bars: J 2e-3 relative, dJ/dk, dJ/dtau, dJ/dtau_c 3e-2, dJ/dA0 rel-L2 3e-2)."""
+    dev = torch.device("cuda:0")
+    dims, steps, interval = (32, 32, 32), 200, 50
+    rho, u, a, b = fields("D3Q19", (32, 32, 32), dev, torch.float32, seed=5)
+    r32, ga32, _ = gradient("D3Q19", "float", "TRT", "mean_product", rho, u, a, b, dims, steps, interval)
+    nx, ny, nz = dims
+    nb = E.reactive_gradient_workspace_bytes("D3Q19", "float", nx, ny, nz, steps, interval, storage=fmt)
+    ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+    res = torch.zeros(4, dtype=torch.float64, device=dev)
+    ga = torch.empty_like(a)
+    E.check(E.reactive_gradient_async("D3Q19", "float", "TRT", "mean_product", rho, u, a, b, nx, ny, nz, TAU, TAU_C,
+                                      K, steps, interval, ws, nb, res, ga, storage=fmt, c0=0.5))
+    torch.cuda.synchronize()
+    r16 = res.tolist()
+    assert abs(r16[0] - r32[0]) <= 2e-3 * abs(r32[0]), (r16[0], r32[0])
+    for q in (1, 2, 3):
+        assert abs(r16[q] - r32[q]) <= 3e-2 * abs(r32[q]) + 1e-9, (q, r16[q], r32[q])
+    err = float(torch.linalg.vector_norm(ga.double() - ga32.double()) / torch.linalg.vector_norm(ga32.double()))
+    assert err <= 3e-2, err

@@ -152,3 +152,48 @@ def test_shifted_2000_steps_vs_fp64(engine, dev, fmt, op):
     err = float(torch.linalg.vector_norm(u_h - u_ref) / torch.linalg.vector_norm(u_ref))
     print(f"{fmt} {op} velocity rel-L2 after {steps} steps: {err:.3e}")
     assert err <= BARS[(fmt, op)]
+
+
+_SW = {"D2Q5": [1 / 3] + [1 / 6] * 4, "D3Q7": [1 / 4] + [1 / 8] * 6}
+
+
+@pytest.mark.parametrize("fmt", ["f16s", "q15s"])
+@pytest.mark.parametrize("fl", ["D2Q9", "D3Q19"])
+@pytest.mark.parametrize("op", ["BGK", "TRT", "MRT"])
+def test_shifted_coupled_step_is_rounded_fp32_step(engine, dev, fmt, fl, op):
+    """The 16-bit fluid + A + B -> C step against encode(FP32 coupled step(decode)):
+    fluid and scalar values within one 16-bit step (+2e-6) of each other, at
+    least 95 % of the codes equal."""
+    sl = "D2Q5" if fl == "D2Q9" else "D3Q7"
+    nx, ny, nz = (64, 12, 1) if fl == "D2Q9" else (32, 6, 5)
+    f = torch.from_numpy(U.random_state(fl, nx, ny, nz, np.float32, seed=8)).to(dev)
+    a = torch.from_numpy(U.random_scalar(sl, nx, ny, nz, np.float32, seed=9)).to(dev)
+    b = torch.from_numpy(U.random_scalar(sl, nx, ny, nz, np.float32, seed=10)).to(dev)
+    c0, k = 0.5, 0.3
+    codes, exact = [], []
+    for lat, t, ref in ((fl, f, 1.0), (sl, a, c0), (sl, b, c0)):
+        h = torch.empty(t.shape, dtype=torch.int16, device=dev)
+        engine.check(engine.encode_shifted_async(lat, fmt, "float", t, h, nx, ny, nz, ref))
+        back = torch.empty_like(t)
+        engine.check(engine.decode_shifted_async(lat, fmt, "float", h, back, nx, ny, nz, ref))
+        codes.append(h)
+        exact.append(back)
+    nxt32 = [torch.empty_like(t) for t in exact]
+    engine.check(engine.fluid_reaction_ab_async(fl, "float", op, exact[0], nxt32[0], exact[1], nxt32[1], exact[2],
+                                                nxt32[2], nx, ny, nz, 1 / 0.6, 1 / 0.8, k))
+    nxt16 = [torch.empty_like(h) for h in codes]
+    engine.check(engine.fluid_reaction_ab_shifted_async(fl, fmt, op, codes[0], nxt16[0], codes[1], nxt16[1],
+                                                        codes[2], nxt16[2], nx, ny, nz, 1 / 0.6, 1 / 0.8, k,
+                                                        1.0, c0))
+    for lat, t32, h16, ref in ((fl, nxt32[0], nxt16[0], 1.0), (sl, nxt32[1], nxt16[1], c0), (sl, nxt32[2], nxt16[2], c0)):
+        want = torch.empty_like(h16)
+        engine.check(engine.encode_shifted_async(lat, fmt, "float", t32, want, nx, ny, nz, ref))
+        got_f, want_f = torch.empty_like(t32), torch.empty_like(t32)
+        engine.check(engine.decode_shifted_async(lat, fmt, "float", h16, got_f, nx, ny, nz, ref))
+        engine.check(engine.decode_shifted_async(lat, fmt, "float", want, want_f, nx, ny, nz, ref))
+        torch.cuda.synchronize()
+        w = (_w(lat) if lat == fl else torch.tensor(_SW[lat], dtype=torch.float64)).to(dev).view(-1, 1)
+        dv = (got_f.double() - want_f.double()).abs() / w
+        step = ULP[fmt] * (want_f.double() / w - ref).abs() * 2 + 2 * ABS_FLOOR[fmt] + 2e-6
+        assert bool((dv <= step).all()), (lat, float((dv - step).max()))
+        assert float((h16 == want).double().mean()) >= 0.95, lat
