@@ -629,6 +629,15 @@ def run_kernel_survey(torch, E, dev, n=128, reps=3):
           lambda: E.fluid_reaction_ab_async("D3Q19", "float", "TRT", f, g, a, a2, b, b2, n, n, n, om, omc, k))
     timed("fluid_reaction D3Q19 f32 TRT + stats", cells * 264,
           lambda: E.fluid_reaction_ab_async("D3Q19", "float", "TRT", f, g, a, a2, b, b2, n, n, n, om, omc, k, part, pb))
+    h19 = [torch.empty((19, n, n, n), dtype=torch.int16, device=dev) for _ in range(2)]
+    h7 = [torch.empty((7, n, n, n), dtype=torch.int16, device=dev) for _ in range(4)]
+    E.check(E.encode_shifted_async("D3Q19", "f16s", "float", f, h19[0], n, n, n, 1.0))
+    E.check(E.encode_shifted_async("D3Q7", "f16s", "float", a, h7[0], n, n, n, 0.5))
+    E.check(E.encode_shifted_async("D3Q7", "f16s", "float", b, h7[2], n, n, n, 0.5))
+    timed("fluid_reaction_shifted D3Q19 f16s TRT", cells * 132,
+          lambda: E.fluid_reaction_ab_shifted_async("D3Q19", "f16s", "TRT", h19[0], h19[1], h7[0], h7[1], h7[2],
+                                                    h7[3], n, n, n, om, omc, k, 1.0, 0.5))
+    del h19, h7
     timed("reactive_stats D3Q7 f32 (2 passes)", cells * 56,
           lambda: E.reactive_stats_async("D3Q7", "float", a, b, n, n, n, k, part, pb, st))
     dpb = E.diagnostics_partials_bytes("D3Q19", n, n, n)
