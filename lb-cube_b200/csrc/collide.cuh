@@ -701,4 +701,16 @@ __device__ __forceinline__ Real reaction_source(Real a, Real b, Real k) {
   return a_after - a;
 }
 
+// Two species pulled, one exact A+B->C source applied to both
+// (lattice_core.hpp:403-411).
+template <class SL, class Real>
+__device__ __forceinline__ void react_pair(Real (&a)[SL::Q], Real (&b)[SL::Q],
+                                           const Real (&u)[SL::D], Real omega_c, Real k) {
+  const Real ca = concentration<SL>(a);
+  const Real cb = concentration<SL>(b);
+  const Real src = reaction_source<Real>(ca, cb, k);
+  collide_scalar<SL>(a, u, omega_c, src);
+  collide_scalar<SL>(b, u, omega_c, src);
+}
+
 }  // namespace lbcube

@@ -29,6 +29,10 @@ SIZES = {"D2Q9": [(37, 23, 1), (150, 3, 1)], "D3Q19": [(13, 11, 7), (150, 3, 2)]
          "D3Q27": [(9, 7, 5), (131, 2, 3)]}
 
 
+FUSED_SIZES = {"D2Q9": [(37, 23, 1), (150, 3, 1)], "D3Q19": [(13, 11, 7), (150, 3, 2)],
+               "D3Q27": [(9, 7, 5), (64, 3, 2)]}
+
+
 def _run_steps(E, lat, real, op, f0, nx, ny, nz, omega, steps, dev):
     cur = torch.from_numpy(f0).to(dev)
     nxt = torch.empty_like(cur)
@@ -161,12 +165,14 @@ def test_reaction_equal_species_branch_bitwise(engine, dev):
 @pytest.mark.parametrize("lat", LATS)
 @pytest.mark.parametrize("real", ["float", "double"])
 @pytest.mark.parametrize("op", ["BGK", "TRT", "MRT"])
-def test_fused_fluid_reaction(engine, dev, lat, real, op):
+@pytest.mark.parametrize("vec", [False, True])
+def test_fused_fluid_reaction(engine, dev, lat, real, op, vec):
     """One fused launch == the reference driver's two launches
     (src/simulate_reaction.cpp:518-543): fluid bit-identical to the oracle,
     scalars bit-identical to the engine's own two-launch sequence and within
-    the exp tolerance of the oracle's coupled loop."""
-    nx, ny, nz = SIZES[lat][0]
+    the exp tolerance of the oracle's coupled loop. Odd x extents run the
+    one-cell kernel, even ones the vectorised kernel."""
+    nx, ny, nz = FUSED_SIZES[lat][int(vec)]
     sl = O.SCALAR_OF[lat]
     dt = REALS[real]
     f0 = U.random_state(lat, nx, ny, nz, dt, seed=41)
