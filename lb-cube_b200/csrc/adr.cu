@@ -10,7 +10,6 @@
 #include "cells.cuh"
 #include "collide.cuh"
 #include "common.cuh"
-#include "coupled_vec.cuh"
 #include "reduce.cuh"
 #include "../../include/lbcube_b200.h"
 
@@ -140,28 +139,6 @@ cudaError_t launch_reaction(const Real* cur_a, Real* nxt_a, const Real* cur_b, R
   return cudaGetLastError();
 }
 
-// The vectorised coupled step (coupled_vec.cuh) when the extents and buffers
-// allow it; returns false (nothing launched) otherwise.
-template <class Real>
-constexpr int kCoupledCells = sizeof(Real) == 4 ? 2 : 1;
-
-template <class FL, class Real, int CT, bool UOUT>
-bool launch_coupled_vec(const Real* cf, Real* nf, const Real* ca, Real* na, const Real* cb, Real* nb,
-                        Real* u_out, const Grid& g, Real omega, Real omega_minus, Real omega_c,
-                        Real k, cudaStream_t s) {
-  if constexpr (FL::Q == 27 && sizeof(Real) == 8 && CT == kMRT) {
-    return false;
-  } else {
-    using S = NativeStorage<Real, kCoupledCells<Real>>;
-    if (!coupled_vec_eligible<S, S>(g, cf, nf, ca, na, cb, nb)) return false;
-    const VecGrid vg = make_vec_grid(g, S::V);
-    fluid_reaction_vec_kernel<FL, S, S, CT, UOUT><<<vec_grid_dims(vg), vec_block_threads(vg), 0, s>>>(
-        cf, nf, ca, na, cb, nb, vg, omega, omega_minus, omega_c, k, typename S::Params{},
-        typename S::Params{}, u_out);
-    return true;
-  }
-}
-
 template <class FL, class Real, int CT>
 cudaError_t launch_fluid_reaction(const Real* cur_f, Real* nxt_f, const Real* cur_a, Real* nxt_a,
                                   const Real* cur_b, Real* nxt_b, size_t nx, size_t ny,
@@ -189,10 +166,6 @@ cudaError_t launch_fluid_reaction(const Real* cur_f, Real* nxt_f, const Real* cu
   if (partials != nullptr) {
     fluid_reaction_kernel<FL, Real, CT, true><<<grid_dims(g), block_dims(g), 0, stream>>>(
         cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, partials);
-  } else if (launch_coupled_vec<FL, Real, CT, false>(cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b,
-                                                     nullptr, g, omega, omega_minus, omega_c, k,
-                                                     stream)) {
-    // vectorised: two FP32 cells (one FP64 cell) per thread
   } else {
     fluid_reaction_kernel<FL, Real, CT, false><<<grid_dims(g), block_dims(g), 0, stream>>>(
         cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, nullptr);
@@ -209,21 +182,15 @@ cudaError_t fluid_reaction_with_velocity(int collision, const Real* cur_f, Real*
                                          Real* nxt_b, Real* u_out, const Grid& g, Real omega,
                                          Real omega_c, Real k, cudaStream_t s) {
   if (collision == kBGK) {
-    if (!launch_coupled_vec<FL, Real, kBGK, true>(cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, u_out,
-                                                  g, omega, Real(0), omega_c, k, s))
-      fluid_reaction_kernel<FL, Real, kBGK, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, nullptr, u_out);
+    fluid_reaction_kernel<FL, Real, kBGK, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, nullptr, u_out);
   } else if (collision == kTRT) {
-    const Real om = trt_omega_minus<Real>(omega);
-    if (!launch_coupled_vec<FL, Real, kTRT, true>(cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, u_out,
-                                                  g, omega, om, omega_c, k, s))
-      fluid_reaction_kernel<FL, Real, kTRT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, om, omega_c, k, nullptr, u_out);
+    fluid_reaction_kernel<FL, Real, kTRT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, trt_omega_minus<Real>(omega), omega_c,
+        k, nullptr, u_out);
   } else if (collision == kMRT) {
-    if (!launch_coupled_vec<FL, Real, kMRT, true>(cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, u_out,
-                                                  g, omega, Real(0), omega_c, k, s))
-      fluid_reaction_kernel<FL, Real, kMRT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, nullptr, u_out);
+    fluid_reaction_kernel<FL, Real, kMRT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, nullptr, u_out);
   } else {
     return cudaErrorInvalidValue;
   }

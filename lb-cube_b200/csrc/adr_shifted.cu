@@ -15,7 +15,6 @@
 #include "collide.cuh"
 #include "collide_dev.cuh"
 #include "common.cuh"
-#include "coupled_vec.cuh"
 #include "reduce.cuh"
 #include "stream_vec.cuh"
 #include "../../include/lbcube_b200.h"
@@ -88,9 +87,6 @@ __global__ void __launch_bounds__(kThreads)
   if constexpr (STATS) block_sum_to<kStatSums>(sums, partials + block_linear() * kStatSums);
 }
 
-// Cells per thread of the vectorised 16-bit coupled step (4-byte words).
-constexpr int kShiftedCoupledCells = 2;
-
 template <class FL, int FMT, int CT>
 cudaError_t launch_shifted_coupled(const unsigned short* cf, unsigned short* nf,
                                    const unsigned short* ca, unsigned short* na,
@@ -98,22 +94,6 @@ cudaError_t launch_shifted_coupled(const unsigned short* cf, unsigned short* nf,
                                    double* partials, const Grid& g, float omega, float omega_c,
                                    float k, float rho0, float c0, cudaStream_t s) {
   const float om = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
-  using SF = std::conditional_t<CT == kBGK || CT == kTRT || (CT == kMRT && FL::Q != 27),
-                                DevStorage<FMT, kShiftedCoupledCells>,
-                                ShiftedStorage<FMT, kShiftedCoupledCells>>;
-  using SS = ShiftedStorage<FMT, kShiftedCoupledCells>;
-  if (partials == nullptr && coupled_vec_eligible<SF, SS>(g, cf, nf, ca, na, cb, nb)) {
-    const VecGrid vg = make_vec_grid(g, SF::V);
-    if (u_out != nullptr)
-      fluid_reaction_vec_kernel<FL, SF, SS, CT, true><<<vec_grid_dims(vg), vec_block_threads(vg), 0, s>>>(
-          cf, nf, ca, na, cb, nb, vg, omega, om, omega_c, k, typename SF::Params{rho0},
-          typename SS::Params{c0}, u_out);
-    else
-      fluid_reaction_vec_kernel<FL, SF, SS, CT, false><<<vec_grid_dims(vg), vec_block_threads(vg), 0, s>>>(
-          cf, nf, ca, na, cb, nb, vg, omega, om, omega_c, k, typename SF::Params{rho0},
-          typename SS::Params{c0}, nullptr);
-    return cudaGetLastError();
-  }
 #define LBCUBE_SC(ST, UO)                                                                          \
   fluid_reaction_shifted_kernel<FL, FMT, CT, ST, UO><<<grid_dims(g), block_dims(g), 0, s>>>(      \
       cf, nf, ca, na, cb, nb, g, omega, om, omega_c, k, rho0, c0, partials, u_out)

@@ -72,13 +72,6 @@ struct NativeStorage {
                                                       compute omega_minus, const Params&) {
     collide<L, compute, CT>(f, omega, omega_minus);
   }
-  // velocity of a cell's populations (compute_macro_state)
-  template <class L>
-  __device__ __forceinline__ static void velocity(const compute (&f)[L::Q], const Params&,
-                                                  compute (&u)[L::D]) {
-    compute rho;
-    macro_state<L>(f, rho, u);
-  }
 };
 
 // Shifted 16-bit storage of LB populations: the stored code h_i stands for
@@ -124,12 +117,6 @@ struct ShiftedStorage {
   __device__ __forceinline__ static void collide_cell(compute (&f)[L::Q], compute omega,
                                                       compute omega_minus, const Params&) {
     collide<L, compute, CT>(f, omega, omega_minus);
-  }
-  template <class L>
-  __device__ __forceinline__ static void velocity(const compute (&f)[L::Q], const Params&,
-                                                  compute (&u)[L::D]) {
-    compute rho;
-    macro_state<L>(f, rho, u);
   }
 };
 
@@ -181,11 +168,6 @@ struct DevStorage {
                   "deviation-space collision is BGK, TRT, or D2Q9 / D3Q19 MRT");
     if constexpr (CT == kMRT) collide_dev_mrt<L, FMT>(v, omega, p.rho0);
     else collide_dev<L, CT, FMT>(v, omega, omega_minus, p.rho0);
-  }
-  template <class L>
-  __device__ __forceinline__ static void velocity(const compute (&v)[L::Q], const Params& p,
-                                                  compute (&u)[L::D]) {
-    dev_velocity<L, FMT>(v, p.rho0, u);
   }
 };
 

@@ -165,14 +165,14 @@ def test_reaction_equal_species_branch_bitwise(engine, dev):
 @pytest.mark.parametrize("lat", LATS)
 @pytest.mark.parametrize("real", ["float", "double"])
 @pytest.mark.parametrize("op", ["BGK", "TRT", "MRT"])
-@pytest.mark.parametrize("vec", [False, True])
-def test_fused_fluid_reaction(engine, dev, lat, real, op, vec):
+@pytest.mark.parametrize("size", [0, 1])
+def test_fused_fluid_reaction(engine, dev, lat, real, op, size):
     """One fused launch == the reference driver's two launches
     (src/simulate_reaction.cpp:518-543): fluid bit-identical to the oracle,
     scalars bit-identical to the engine's own two-launch sequence and within
-    the exp tolerance of the oracle's coupled loop. Odd x extents run the
-    one-cell kernel, even ones the vectorised kernel."""
-    nx, ny, nz = FUSED_SIZES[lat][int(vec)]
+    the exp tolerance of the oracle's coupled loop; at two extents (odd and
+    even x)."""
+    nx, ny, nz = FUSED_SIZES[lat][size]
     sl = O.SCALAR_OF[lat]
     dt = REALS[real]
     f0 = U.random_state(lat, nx, ny, nz, dt, seed=41)
