@@ -466,8 +466,8 @@ int lbm_step_diagnostics_async(int lattice, int precision, int collision,
  * planes touch no face buffer (those pointers may be null when the range
  * does not include a face). A box stepped as slabs with the face buffers
  * exchanged between steps is bit-identical to the box stepped whole.
- * Requirements as the vectorised step: x_extent even for float, buffers
- * aligned to 2 elements; D3Q27 double MRT / RLBM are not available.
+ * Requirements as the vectorised step: x_extent even and buffers aligned to
+ * 2 elements for D3Q19 float; D3Q27 double MRT / RLBM are not available.
  * lbm_slab_pack_async fills send_lo / send_hi from a state (before the first
  * exchange). */
 size_t lbm_slab_face_elems(int lattice, size_t x_extent, size_t y_extent);

@@ -66,13 +66,13 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Cells per thread of the vectorised kernel: 2 FP32 cells (8-byte words) or 1
-// FP64 cell per thread measured fastest on B200 at 256^3 (D3Q19 TRT FP32: 0.99
-// of the copy bandwidth at V = 2 against 0.80 at V = 4 and 0.76 at V = 1;
-// FP64 best at V = 1). Operators whose register footprint would spill use the
-// one-cell kernel.
-template <class Real>
-constexpr int kVecCells = sizeof(Real) == 4 ? 2 : 1;
+// Cells per thread of the vectorised kernel, measured fastest on B200 at 256^3:
+// 2 FP32 D2Q9 / D3Q19 cells (8-byte words; D3Q19 TRT 0.99 of the copy
+// bandwidth against 0.80 at V = 4 and 0.76 at V = 1), 1 D3Q27 FP32 cell (BGK
+// 0.86 against 0.75 at V = 2, TRT 0.80 against 0.58) and 1 FP64 cell.
+// Operators whose register footprint would spill use the one-cell kernel.
+template <class L, class Real>
+constexpr int kVecCells = (sizeof(Real) == 4 && L::Q != 27) ? 2 : 1;
 template <class L, class Real, int CT>
 constexpr bool kUseVec = !(L::Q == 27 && sizeof(Real) == 8 && (CT == kMRT || CT == kRLBM));
 
@@ -89,7 +89,7 @@ cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, 
   const Span writes[1] = {{nxt, bytes}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
-  using S = NativeStorage<Real, kVecCells<Real>>;
+  using S = NativeStorage<Real, kVecCells<L, Real>>;
   if (kUseVec<L, Real, CT> && vec_eligible<S>(g, cur, nxt)) {
     const VecGrid vg = make_vec_grid(g, S::V);
     fluid_step_vec_kernel<L, S, CT><<<vec_grid_dims(vg), vec_block_threads(vg), 0, stream>>>(
@@ -119,7 +119,7 @@ cudaError_t launch_fluid_step_diag(const Real* cur, Real* nxt, size_t nx, size_t
   const Span writes[3] = {{nxt, bytes}, {partials, need}, {out, kDiagOut * sizeof(double)}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
-  using S = NativeStorage<Real, kVecCells<Real>>;
+  using S = NativeStorage<Real, kVecCells<L, Real>>;
   long long count;
   if (kUseVec<L, Real, CT> && vec_eligible<S>(g, cur, nxt)) {
     const VecGrid vg = make_vec_grid(g, S::V);

@@ -24,8 +24,9 @@
 
 namespace lbcube {
 
-template <class Real>
-constexpr int kSlabCells = sizeof(Real) == 4 ? 2 : 1;
+// Cells per thread, as the periodic step (fluid_step.cu kVecCells).
+template <class L, class Real>
+constexpr int kSlabCells = (sizeof(Real) == 4 && L::Q != 27) ? 2 : 1;
 
 template <class L, class Real, int CT>
 cudaError_t launch_slab_step(const Real* cur, Real* nxt, size_t nx, size_t ny, size_t nz,
@@ -42,7 +43,7 @@ cudaError_t launch_slab_step(const Real* cur, Real* nxt, size_t nx, size_t ny, s
   // a face plane reads both halos when nz == 1
   if (nz == 1 && (halo_lo == nullptr || halo_hi == nullptr || send_lo == nullptr || send_hi == nullptr))
     return cudaErrorInvalidDevicePointer;
-  using S = NativeStorage<Real, kSlabCells<Real>>;
+  using S = NativeStorage<Real, kSlabCells<L, Real>>;
   if (!vec_eligible<S>(g, cur, nxt)) return cudaErrorInvalidValue;
   const size_t bytes = (size_t)L::Q * g.plane * sizeof(Real);
   const size_t hbytes = (size_t)zcount<L>() * g.ny * g.nx * sizeof(Real);
