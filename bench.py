@@ -45,6 +45,7 @@ TAU = 0.55
 U0 = 0.05
 NOISE = 1e-3
 SEED = 20261203
+OP = "TRT"  # operator of the timed run
 BYTES_PER_LU = 2 * 19 * 4  # read Q + write Q FP32 populations
 
 
@@ -62,6 +63,8 @@ def parse():
                     help="population storage of the timed run (16-bit ones are shifted)")
     ap.add_argument("--size", type=int, default=256,
                     help="cube edge; smaller sizes are for profiling captures only")
+    ap.add_argument("--collision", choices=["TRT", "BGK", "MRT"], default="TRT",
+                    help="operator of the timed run (TRT is the headline; others for profiling captures)")
     ap.add_argument("--kernel-survey", action="store_true",
                     help="launch every kernel family a few times at 128^3 (1024^2 for 2-D), time each with "
                          "CUDA events and print one JSON line; the command the per-kernel ncu summary captures")
@@ -69,16 +72,17 @@ def parse():
                     help="run only the adjoint cost measurement (D3Q19 BGK FP32, --size cube, --steps "
                          "steps, checkpoint every min(100, steps)) and print it; for profiling captures")
     a = ap.parse_args()
-    global NX, NY, NZ
+    global NX, NY, NZ, OP
     NX = NY = NZ = a.size
+    OP = a.collision
     return a
 
 
 def config_dict():
     return {
-        "workload": f"D3Q19 TRT (Lambda 1/4) {NX}^3 periodic, Taylor-Green u0 0.05 + N(0, 1e-3) "
-                    "velocity noise, tau 0.55, FP32 populations",
-        "lattice": "D3Q19", "collision": "TRT", "storage": "fp32",
+        "workload": f"D3Q19 {OP}{' (Lambda 1/4)' if OP == 'TRT' else ''} {NX}^3 periodic, Taylor-Green u0 0.05 "
+                    "+ N(0, 1e-3) velocity noise, tau 0.55, FP32 populations",
+        "lattice": "D3Q19", "collision": OP, "storage": "fp32",
         "nx": NX, "ny": NY, "nz": NZ, "tau": TAU,
         "l2": f"inputs larger than L2 ({19 * 4 * NX * NY * NZ / 1e9:.2f} GB per population buffer); no flush",
     }
@@ -708,7 +712,7 @@ def run_engine(args, rank, world, local_rank):
         # the face populations cross NVLink (NCCL point-to-point) every step
         import slab
 
-        slabs = slab.SlabDomain(torch, "D3Q19", "float", "TRT", NX, NY, NZ * world, omega, rank, world, dev)
+        slabs = slab.SlabDomain(torch, "D3Q19", "float", OP, NX, NY, NZ * world, omega, rank, world, dev)
         exchange = slab.DistributedExchange(dist)
         slabs.prime(f, exchange)
         launches_per_step = len(sum(slabs.ranges(), []))
@@ -718,7 +722,7 @@ def run_engine(args, rank, world, local_rank):
             return 0
     elif storage == "fp32":
         def step(cur, nxt):
-            return E.launch_step_gpu("D3Q19", "float", "TRT", cur, nxt, NX, NY, NZ, omega)
+            return E.launch_step_gpu("D3Q19", "float", OP, cur, nxt, NX, NY, NZ, omega)
     else:
         h = torch.empty(f.shape, dtype=torch.int16, device=dev)
         E.check(E.encode_shifted_async("D3Q19", storage, "float", f, h, NX, NY, NZ, 1.0))
@@ -726,7 +730,7 @@ def run_engine(args, rank, world, local_rank):
         f = h
 
         def step(cur, nxt):
-            return E.step_shifted_async("D3Q19", storage, "TRT", cur, nxt, NX, NY, NZ, omega, 1.0)
+            return E.step_shifted_async("D3Q19", storage, OP, cur, nxt, NX, NY, NZ, omega, 1.0)
     g = torch.empty_like(f)
 
     for _ in range(args.warmup):
@@ -813,9 +817,9 @@ def run_engine(args, rank, world, local_rank):
     else:
         parallelism = f"{world} independent replicas (16-bit storage has no slab path)"
     peak, peak_kind = measured_hbm_peak()
-    traffic = committed_traffic(f"d3q19_float_trt_{NX}") if storage == "fp32" else None
+    traffic = committed_traffic(f"d3q19_float_trt_{NX}") if storage == "fp32" and OP == "TRT" else None
     variants = accuracy = fp16_store = adjoint = adjoint_reactive = adjoint_reactive_16 = mixing = None
-    if world == 1 and not args.no_variants and storage == "fp32":
+    if world == 1 and not args.no_variants and storage == "fp32" and OP == "TRT":
         variants = run_variants(torch, E, dev, f, peak, ms_per_step)
         del f, g
         torch.cuda.empty_cache()
