@@ -607,7 +607,8 @@ def run_kernel_survey(torch, E, dev, n=128, reps=3):
     f27 = torch.empty((27, n, n, n), dtype=f32, device=dev)
     E.check(E.init_equilibrium_async("D3Q27", "float", rho, u, f27, n, n, n))
     g27 = torch.empty_like(f27)
-    timed("step D3Q27 f32 BGK", cells * 216, lambda: E.step_async("D3Q27", "float", "BGK", f27, g27, n, n, n, om))
+    for op in ("BGK", "TRT", "MRT", "RLBM"):
+        timed(f"step D3Q27 f32 {op}", cells * 216, lambda op=op: E.step_async("D3Q27", "float", op, f27, g27, n, n, n, om))
     del f27, g27
     h = torch.empty((19, n, n, n), dtype=torch.int16, device=dev)
     hg = torch.empty_like(h)

@@ -9,6 +9,8 @@
 // of every partial sum is unchanged (only the sign of an exact zero can differ).
 #pragma once
 
+#include <type_traits>
+
 #include "lattices.cuh"
 
 #define LB_I(I) decltype(I)::value
@@ -433,17 +435,91 @@ __device__ __forceinline__ void moments_d3q27(const Real (&f)[27], Real (&m)[27]
   m[26] = raw[t27(2, 2, 2)];
 }
 
-// transform_to_populations_d3q27 (lattice_mrt.hpp:1130-1225).
+// Correctly rounded x / D for D = 3 and D = 6 without a division
+// instruction: Markstein's correction step (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990; for divisors known in advance, N. Brisebarre, J.-M.
+// Muller, S. K. Raina, IEEE Trans. Computers 53(8), 2004):
+//   z = RN(1/D),  q0 = RN(x z),  r = x - q0 D (exact with one FMA),  q = RN(q0 + r z).
+// With z within half an ulp of 1/D and q0 within one ulp of x / D, q is the
+// correctly rounded quotient unless an intermediate value underflows or
+// overflows (Markstein's theorem). FP32, against IEEE x / D over every input:
+// identical for D = 3 except x = -0 (gives +0) and x = +-inf (gives NaN); for
+// D = 6 identical except x = -0, +-inf and 0 < |x| <= 2^-125. populations_d3q27
+// below uses it only where none of those can occur (FP64: away from the
+// underflow range by a wide margin).
+template <int D, class Real>
+__device__ __forceinline__ Real div_exact_const(Real x) {
+  constexpr Real z = Real(1) / Real(D);
+  if constexpr (std::is_same_v<Real, float>) {
+    const float q0 = __fmul_rn(x, z);
+    const float r = __fmaf_rn(-q0, (float)D, x);
+    return __fmaf_rn(r, z, q0);
+  } else {
+    const double q0 = __dmul_rn(x, z);
+    const double r = __fma_rn(-q0, (double)D, x);
+    return __fma_rn(r, z, q0);
+  }
+}
+
+// Division policies of the D3Q27 population transform: (x * P) / N with
+// N in {2, 3, 6} as IEEE divisions, or through div_exact_const (N = 3, 6)
+// and the exact x * 0.5 (N = 2). Const::checked<N> says which dividends the
+// fast transform must see in the range Const::safe accepts: in FP32 those of
+// the divisions by 6 (division by 3 is exact for every finite FP32 input), in
+// FP64 all of them.
+struct Div27Ieee {
+  template <int N, class Real>
+  __device__ __forceinline__ static Real div(Real x) { return x / Real(N); }
+};
 template <class Real>
-__device__ __forceinline__ void populations_d3q27(const Real (&m)[27], Real (&f)[27]) {
+struct Div27Const {
+  template <int N>
+  __device__ __forceinline__ static Real div(Real x) {
+    if constexpr (N == 2) return x * Real(0.5);
+    else return div_exact_const<N>(x);
+  }
+  template <int N>
+  static constexpr bool checked = std::is_same_v<Real, float> ? N == 6 : N != 2;
+  // zero, or |x| >= 2^-124 (FP32) / 2^-960 (FP64)
+  __device__ __forceinline__ static bool safe(Real x) {
+    if constexpr (std::is_same_v<Real, float>) return x == 0.0f || fabsf(x) >= 0x1p-124f;
+    else return x == 0.0 || fabs(x) >= 0x1p-960;
+  }
+  // every moment finite and small enough that nothing in the transform overflows
+  __device__ __forceinline__ static bool bounded(Real m) {
+    if constexpr (std::is_same_v<Real, float>) return fabsf(m) <= 0x1p100f;
+    else return fabs(m) <= 0x1p900;
+  }
+};
+
+// transform_to_populations_d3q27 (lattice_mrt.hpp:1130-1225). With
+// CHECK, `ok` is cleared when a dividend that Div::checked names is outside
+// the range Div::safe accepts. Each dividend is +-x or +-2x for a value x
+// checked here (|2x| >= |x|, and the sign does not matter).
+template <class Real, class Div, bool CHECK>
+__device__ __forceinline__ void populations_d3q27_with(const Real (&m)[27], Real (&f)[27], bool& ok) {
   Real raw[27], zi[27], yzi[27], p[27];
+  auto check = [&](auto n, Real x) {
+    if constexpr (CHECK) {
+      if constexpr (Div::template checked<decltype(n)::value>) ok = ok && Div::safe(x);
+    }
+  };
+  using N3 = std::integral_constant<int, 3>;
+  using N6 = std::integral_constant<int, 6>;
   raw[t27(0, 0, 0)] = m[0];
   raw[t27(1, 0, 0)] = m[1];
   raw[t27(0, 1, 0)] = m[2];
   raw[t27(0, 0, 1)] = m[3];
-  raw[t27(2, 0, 0)] = (m[4] + m[5]) / Real{3};
-  raw[t27(0, 2, 0)] = (Real{2} * m[4] - m[5] + Real{3} * m[6]) / Real{6};
-  raw[t27(0, 0, 2)] = (Real{2} * m[4] - m[5] - Real{3} * m[6]) / Real{6};
+  const Real d200 = m[4] + m[5];
+  const Real d020 = Real{2} * m[4] - m[5] + Real{3} * m[6];
+  const Real d002 = Real{2} * m[4] - m[5] - Real{3} * m[6];
+  check(N3{}, d200);
+  check(N6{}, d020);
+  check(N6{}, d002);
+  raw[t27(2, 0, 0)] = Div::template div<3>(d200);
+  raw[t27(0, 2, 0)] = Div::template div<6>(d020);
+  raw[t27(0, 0, 2)] = Div::template div<6>(d002);
   raw[t27(1, 1, 0)] = m[7];
   raw[t27(0, 1, 1)] = m[8];
   raw[t27(1, 0, 1)] = m[9];
@@ -464,34 +540,68 @@ __device__ __forceinline__ void populations_d3q27(const Real (&m)[27], Real (&f)
   raw[t27(2, 1, 2)] = m[24];
   raw[t27(1, 2, 2)] = m[25];
   raw[t27(2, 2, 2)] = m[26];
+  static_for<9>([&](auto J) {  // dividends of pass 1: order 0 (/3) and order 2 (/6) rows
+    check(N3{}, raw[t27(LB_I(J) / 3, LB_I(J) % 3, 0)]);
+    check(N6{}, raw[t27(LB_I(J) / 3, LB_I(J) % 3, 2)]);
+  });
   static_for<27>([&](auto J) {  // (ax, ay, iz)
     constexpr int a = LB_I(J) / 9, b = (LB_I(J) / 3) % 3, c = LB_I(J) % 3;
     Real v = Real(0);
     static_for<3>([&](auto K) {
       constexpr int k = LB_I(K);
-      v += raw[t27(a, b, k)] * Real(p27_basis(k, c - 1)) / Real(p27_norm(k));
+      v += Div::template div<p27_norm(k)>(raw[t27(a, b, k)] * Real(p27_basis(k, c - 1)));
     });
     zi[t27(a, b, c)] = v;
+  });
+  static_for<9>([&](auto J) {  // dividends of pass 2
+    check(N3{}, zi[t27(LB_I(J) / 3, 0, LB_I(J) % 3)]);
+    check(N6{}, zi[t27(LB_I(J) / 3, 2, LB_I(J) % 3)]);
   });
   static_for<27>([&](auto J) {  // (ax, iy, iz)
     constexpr int a = LB_I(J) / 9, b = (LB_I(J) / 3) % 3, c = LB_I(J) % 3;
     Real v = Real(0);
     static_for<3>([&](auto K) {
       constexpr int k = LB_I(K);
-      v += zi[t27(a, k, c)] * Real(p27_basis(k, b - 1)) / Real(p27_norm(k));
+      v += Div::template div<p27_norm(k)>(zi[t27(a, k, c)] * Real(p27_basis(k, b - 1)));
     });
     yzi[t27(a, b, c)] = v;
+  });
+  static_for<9>([&](auto J) {  // dividends of pass 3
+    check(N3{}, yzi[t27(0, LB_I(J) / 3, LB_I(J) % 3)]);
+    check(N6{}, yzi[t27(2, LB_I(J) / 3, LB_I(J) % 3)]);
   });
   static_for<27>([&](auto J) {  // (ix, iy, iz)
     constexpr int a = LB_I(J) / 9, b = (LB_I(J) / 3) % 3, c = LB_I(J) % 3;
     Real v = Real(0);
     static_for<3>([&](auto K) {
       constexpr int k = LB_I(K);
-      v += yzi[t27(k, b, c)] * Real(p27_basis(k, a - 1)) / Real(p27_norm(k));
+      v += Div::template div<p27_norm(k)>(yzi[t27(k, b, c)] * Real(p27_basis(k, a - 1)));
     });
     p[t27(a, b, c)] = v;
   });
   static_for<27>([&](auto I) { f[LB_I(I)] = p[tensor_slot27<LB_I(I)>()]; });
+}
+
+// Out of line, so that the rare fallback below keeps its divisions out of the
+// kernel's instruction stream.
+template <class Real>
+static __device__ __noinline__ void populations_d3q27_ieee(const Real (&m)[27], Real (&f)[27]) {
+  bool ok = true;
+  populations_d3q27_with<Real, Div27Ieee, false>(m, f, ok);
+}
+
+// The fast transform (Div27Const) gives the bits of the IEEE one when every
+// moment is bounded (so nothing overflows and no dividend is infinite) and
+// every checked dividend is in the safe range; a zero quotient's sign never
+// matters, since each one is added to a sum that starts at +0. Any other cell
+// is recomputed with IEEE divisions.
+template <class Real>
+__device__ __forceinline__ void populations_d3q27(const Real (&m)[27], Real (&f)[27]) {
+  using Div = Div27Const<Real>;
+  bool ok = true;
+  static_for<27>([&](auto K) { ok = ok && Div::bounded(m[LB_I(K)]); });
+  populations_d3q27_with<Real, Div, true>(m, f, ok);
+  if (!ok) populations_d3q27_ieee<Real>(m, f);
 }
 
 // collide_mrt_d3q27 (lattice_mrt.hpp:1284-1305) with the projected

@@ -54,6 +54,38 @@ def test_step_bitwise(engine, dev, lat, real, op):
         assert np.array_equal(got, want), f"{lat} {real} {op} {nx}x{ny}x{nz}: max |d| {np.abs(got - want).max()}"
 
 
+@pytest.mark.parametrize("scale", [1e-24, 1e-33, 1e-38, 1e-42])
+def test_d3q27_mrt_float_tiny_states_bitwise(engine, dev, scale):
+    """D3Q27 MRT in FP32 divides by 3 and 6 without a division instruction and
+    falls back to IEEE division for a cell whose dividends come near the
+    subnormal range. Every other x cell is scaled down (1e-24 keeps nearly all
+    cells on the fast path, 1e-33 .. 1e-42 send them to the fallback, the last
+    with subnormal populations), so warps mix both paths; five steps stream
+    tiny and normal populations into the same cells. Bit-identical throughout."""
+    nx, ny, nz = 40, 7, 5
+    f0 = U.random_state("D3Q27", nx, ny, nz, np.float32, seed=31).reshape(27, nz, ny, nx)
+    f0[..., ::2] *= np.float32(scale)
+    f0 = np.ascontiguousarray(f0.reshape(27, -1))
+    got = _run_steps(engine, "D3Q27", "float", "MRT", f0, nx, ny, nz, 1 / 0.6, 5, dev)
+    want = O.step(f0, "D3Q27", "MRT", nx, ny, nz, 1 / 0.6, steps=5)
+    assert np.array_equal(got, want), f"max |d| {np.abs(got - want).max()}"
+
+
+@pytest.mark.parametrize("real", ["float", "double"])
+def test_d3q27_mrt_nonfinite_cells(engine, dev, real):
+    """Cells holding an infinite or NaN population (a blown-up run): the FP32
+    fast transform hands them to the IEEE fallback, so inf and NaN land where
+    the reference puts them; the finite cells stay bit-identical."""
+    nx, ny, nz = 9, 7, 5
+    f0 = U.random_state("D3Q27", nx, ny, nz, REALS[real], seed=32)
+    f0[3, 10] = np.inf
+    f0[0, 40] = -np.inf
+    f0[12, 77] = np.nan
+    got = _run_steps(engine, "D3Q27", real, "MRT", f0, nx, ny, nz, 1 / 0.6, 1, dev)
+    want = O.step(f0, "D3Q27", "MRT", nx, ny, nz, 1 / 0.6, steps=1)
+    assert np.array_equal(got, want, equal_nan=True)
+
+
 def test_tgv_d3q19_fp64_bgk_64cube(engine, dev):
     """The C1 workload shape: D3Q19 BGK FP64 64^3 Taylor-Green (u0 0.05, rho 1,
     tau 0.6), 100 steps, bit-identical; KE decays."""
