@@ -334,8 +334,31 @@ __device__ __forceinline__ void store_vec(typename S::elem* __restrict__ nxt, co
 // its own cells, so this costs no memory traffic. Native storage only.
 // SLAB: one launch over planes [slab.z_begin, slab.z_begin + gridDim.y) of a
 // z-slab, with halo planes at the slab faces (see SlabArgs).
+// Resident blocks per SM that the register allocation must leave room for
+// (the launch bounds' second argument), per lattice, precision and operator.
+// The compiler's own allocation leaves these kernels short of warps to hide
+// memory latency; the values were chosen by timing every setting from 1 to 8
+// on B200 at 256^3 (each spills at most 8 bytes). Fraction of the copy
+// bandwidth, compiler's allocation -> this one, under the same power cap:
+//   FP32 D3Q19  MRT 0.75 -> 0.82 (64 registers), RLBM 0.63 -> 0.72 (80)
+//   FP32 D3Q27  BGK 0.65 -> 0.74 (64), TRT 0.61 -> 0.70 (72), RLBM 0.48 -> 0.58 (80)
+//   FP64 D3Q19  BGK 0.85 -> 0.97 (64), TRT 0.83 -> 0.94 (64), RLBM 0.68 -> 0.73 (126)
+//   FP64 D3Q27  BGK 0.83 -> 0.91 (96)
+// Everything else, and the DIAG / SLAB forms (not timed this way), keeps the
+// compiler's allocation (1).
+template <class L, class S, int CT>
+__host__ __device__ constexpr int vec_min_blocks() {
+  constexpr bool f32 = std::is_same_v<typename S::elem, float>;
+  constexpr bool f64 = std::is_same_v<typename S::elem, double>;
+  if constexpr (L::Q == 19 && f32) return CT == kMRT ? 8 : (CT == kRLBM ? 6 : 1);
+  if constexpr (L::Q == 27 && f32) return CT == kBGK ? 8 : (CT == kTRT ? 7 : (CT == kRLBM ? 6 : 1));
+  if constexpr (L::Q == 19 && f64) return (CT == kBGK || CT == kTRT) ? 8 : (CT == kRLBM ? 4 : 1);
+  if constexpr (L::Q == 27 && f64) return CT == kBGK ? 5 : 1;
+  return 1;
+}
+
 template <class L, class S, int CT, bool DIAG = false, bool SLAB = false>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, (DIAG || SLAB) ? 1 : vec_min_blocks<L, S, CT>())
     fluid_step_vec_kernel(const typename S::elem* __restrict__ cur,
                           typename S::elem* __restrict__ nxt, VecGrid vg,
                           typename S::compute omega, typename S::compute omega_minus,
