@@ -221,8 +221,9 @@ def _time_steps(torch, launch, a, b, steps, warmup):
 
 
 def run_variants(torch, E, dev, f32, peak, fp32_ms):
-    """Single-GPU characterisation at the same size: other operators, 16-bit
-    shifted storage, D3Q27 and FP64. Each: 10 warm-up + 200 timed steps."""
+    """Single-GPU characterisation at the same size: every operator in FP32 and
+    FP64 for D3Q19 and D3Q27, and 16-bit shifted storage. 10 warm-up + 200 timed
+    steps each (5 + 50 for the slower FP64 / D3Q27 operators)."""
     omega = 1.0 / TAU
     cells = NX * NY * NZ
     out = []
@@ -236,7 +237,7 @@ def run_variants(torch, E, dev, f32, peak, fp32_ms):
         return d
 
     g = torch.empty_like(f32)
-    for op in ("MRT", "BGK"):
+    for op in ("MRT", "BGK", "RLBM"):
         ms = _time_steps(torch, lambda a, b, op=op: E.launch_step_gpu("D3Q19", "float", op, a, b, NX, NY, NZ, omega),
                          f32.clone(), g, 200, 10)
         rec(f"D3Q19 {op} fp32", ms, 152)
@@ -273,19 +274,28 @@ def run_variants(torch, E, dev, f32, peak, fp32_ms):
     # FP64 (the reference drivers' precision) and the 27-velocity bandwidth case
     f64 = f32.double()
     g64 = torch.empty_like(f64)
-    ms = _time_steps(torch, lambda a, b: E.launch_step_gpu("D3Q19", "double", "BGK", a, b, NX, NY, NZ, omega),
-                     f64, g64, 200, 10)
-    rec("D3Q19 BGK fp64", ms, 304)
+    for op in ("BGK", "TRT", "MRT", "RLBM"):
+        ms = _time_steps(torch, lambda a, b, op=op: E.launch_step_gpu("D3Q19", "double", op, a, b, NX, NY, NZ, omega),
+                         f64.clone(), g64, 200 if op == "BGK" else 50, 5)
+        rec(f"D3Q19 {op} fp64", ms, 304)
     del f64, g64
     f27 = torch.empty((27, NZ, NY, NX), dtype=torch.float32, device=dev)
     rho = torch.ones((NZ, NY, NX), dtype=torch.float32, device=dev)
     u = torch.zeros((3, NZ, NY, NX), dtype=torch.float32, device=dev)
     E.check(E.init_equilibrium_async("D3Q27", "float", rho, u, f27, NX, NY, NZ))
     g27 = torch.empty_like(f27)
-    ms = _time_steps(torch, lambda a, b: E.launch_step_gpu("D3Q27", "float", "BGK", a, b, NX, NY, NZ, omega),
-                     f27, g27, 200, 10)
-    rec("D3Q27 BGK fp32", ms, 216)
-    del f27, g27, rho, u
+    for op in ("BGK", "TRT", "MRT", "RLBM"):
+        ms = _time_steps(torch, lambda a, b, op=op: E.launch_step_gpu("D3Q27", "float", op, a, b, NX, NY, NZ, omega),
+                         f27.clone(), g27, 200 if op == "BGK" else 50, 5)
+        rec(f"D3Q27 {op} fp32", ms, 216)
+    f27d = f27.double()
+    del f27, g27
+    g27d = torch.empty_like(f27d)
+    for op in ("BGK", "MRT"):
+        ms = _time_steps(torch, lambda a, b, op=op: E.launch_step_gpu("D3Q27", "double", op, a, b, NX, NY, NZ, omega),
+                         f27d.clone(), g27d, 50, 5)
+        rec(f"D3Q27 {op} fp64", ms, 432)
+    del f27d, g27d, rho, u
     torch.cuda.empty_cache()
     return out
 
