@@ -579,7 +579,7 @@ def run_reactive_mixing(torch, E, dev, n=1024, steps=20000, every=10, tau=0.6):
     return out
 
 
-def run_kernel_survey(torch, E, dev, n=128, reps=3):
+def run_kernel_survey(torch, E, dev, n=128, reps=10):
     """Every kernel family once per rep at n^3 (D2Q9 at (8n)^2), timed with CUDA
     events; algorithmic bytes per launch give the achieved GB/s."""
     import slab

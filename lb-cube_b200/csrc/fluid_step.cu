@@ -92,8 +92,8 @@ cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, 
   using S = NativeStorage<Real, kVecCells<L, Real>>;
   if (kUseVec<L, Real, CT> && vec_eligible<S>(g, cur, nxt)) {
     const VecGrid vg = make_vec_grid(g, S::V);
-    fluid_step_vec_kernel<L, S, CT><<<vec_grid_dims(vg), vec_block_threads(vg), 0, stream>>>(
-        cur, nxt, vg, omega, omega_minus, typename S::Params{});
+    launch_vec_step<L, S, CT>(vg, vec_grid_dims(vg), vec_block_threads(vg), stream, cur, nxt, omega,
+                              omega_minus, typename S::Params{});
   } else {
     fluid_step_kernel<L, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(cur, nxt, g, omega,
                                                                            omega_minus);

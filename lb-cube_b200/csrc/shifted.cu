@@ -42,9 +42,10 @@ cudaError_t launch_shifted_step(const void* cur, void* nxt, size_t nx, size_t ny
   if (!vec_eligible<S>(g, cur, nxt)) return cudaErrorInvalidValue;  // nx % V, word alignment
   const float omega_minus = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
   const VecGrid vg = make_vec_grid(g, S::V);
-  fluid_step_vec_kernel<L, S, CT><<<vec_grid_dims(vg), vec_block_threads(vg), 0, stream>>>(
-      static_cast<const unsigned short*>(cur), static_cast<unsigned short*>(nxt), vg, omega,
-      omega_minus, typename S::Params{rho0});
+  launch_vec_step<L, S, CT>(vg, vec_grid_dims(vg), vec_block_threads(vg), stream,
+                            static_cast<const unsigned short*>(cur),
+                            static_cast<unsigned short*>(nxt), omega,
+                            omega_minus, typename S::Params{rho0});
   return cudaGetLastError();
 }
 

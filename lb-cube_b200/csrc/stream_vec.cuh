@@ -334,36 +334,14 @@ __device__ __forceinline__ void store_vec(typename S::elem* __restrict__ nxt, co
 // its own cells, so this costs no memory traffic. Native storage only.
 // SLAB: one launch over planes [slab.z_begin, slab.z_begin + gridDim.y) of a
 // z-slab, with halo planes at the slab faces (see SlabArgs).
-// Resident blocks per SM that the register allocation must leave room for
-// (the launch bounds' second argument), per lattice, precision and operator.
-// The compiler's own allocation leaves these kernels short of warps to hide
-// memory latency; the values were chosen by timing every setting from 1 to 8
-// on B200 at 256^3 (each spills at most 8 bytes). Fraction of the copy
-// bandwidth, compiler's allocation -> this one, under the same power cap:
-//   FP32 D3Q19  MRT 0.75 -> 0.82 (64 registers), RLBM 0.63 -> 0.72 (80)
-//   FP32 D3Q27  BGK 0.65 -> 0.74 (64), TRT 0.61 -> 0.70 (72), RLBM 0.48 -> 0.58 (80)
-//   FP64 D3Q19  BGK 0.85 -> 0.97 (64), TRT 0.83 -> 0.94 (64), RLBM 0.68 -> 0.73 (126)
-//   FP64 D3Q27  BGK 0.83 -> 0.91 (96)
-// Everything else, and the DIAG / SLAB forms (not timed this way), keeps the
-// compiler's allocation (1).
-template <class L, class S, int CT>
-__host__ __device__ constexpr int vec_min_blocks() {
-  constexpr bool f32 = std::is_same_v<typename S::elem, float>;
-  constexpr bool f64 = std::is_same_v<typename S::elem, double>;
-  if constexpr (L::Q == 19 && f32) return CT == kMRT ? 8 : (CT == kRLBM ? 6 : 1);
-  if constexpr (L::Q == 27 && f32) return CT == kBGK ? 8 : (CT == kTRT ? 7 : (CT == kRLBM ? 6 : 1));
-  if constexpr (L::Q == 19 && f64) return (CT == kBGK || CT == kTRT) ? 8 : (CT == kRLBM ? 4 : 1);
-  if constexpr (L::Q == 27 && f64) return CT == kBGK ? 5 : 1;
-  return 1;
-}
-
-template <class L, class S, int CT, bool DIAG = false, bool SLAB = false>
-__global__ void __launch_bounds__(kThreads, (DIAG || SLAB) ? 1 : vec_min_blocks<L, S, CT>())
-    fluid_step_vec_kernel(const typename S::elem* __restrict__ cur,
-                          typename S::elem* __restrict__ nxt, VecGrid vg,
-                          typename S::compute omega, typename S::compute omega_minus,
-                          typename S::Params p, double* __restrict__ partials = nullptr,
-                          SlabArgs<typename S::elem> slab = {}) {
+template <class L, class S, int CT, bool DIAG, bool SLAB>
+__device__ __forceinline__ void fluid_step_vec_body(const typename S::elem* __restrict__ cur,
+                                                    typename S::elem* __restrict__ nxt,
+                                                    const VecGrid& vg, typename S::compute omega,
+                                                    typename S::compute omega_minus,
+                                                    const typename S::Params& p,
+                                                    double* __restrict__ partials,
+                                                    const SlabArgs<typename S::elem>& slab) {
   using R = typename S::compute;
   constexpr int V = S::V;
   const Grid& g = vg.g;
@@ -392,6 +370,57 @@ __global__ void __launch_bounds__(kThreads, (DIAG || SLAB) ? 1 : vec_min_blocks<
     for (int j = 0; j < V; ++j) S::template collide_cell<L, CT>(f[j], omega, omega_minus, p);
     store_vec<L, S, SLAB>(nxt, g, x0, y, z, p, f, slab);
   }
+}
+
+template <class L, class S, int CT, bool DIAG = false, bool SLAB = false>
+__global__ void __launch_bounds__(kThreads)
+    fluid_step_vec_kernel(const typename S::elem* __restrict__ cur,
+                          typename S::elem* __restrict__ nxt, VecGrid vg,
+                          typename S::compute omega, typename S::compute omega_minus,
+                          typename S::Params p, double* __restrict__ partials = nullptr,
+                          SlabArgs<typename S::elem> slab = {}) {
+  fluid_step_vec_body<L, S, CT, DIAG, SLAB>(cur, nxt, vg, omega, omega_minus, p, partials, slab);
+}
+
+// The plain step with a register budget: at least MB resident blocks of
+// kThreads per SM (the launch bounds' second argument).
+template <class L, class S, int CT, int MB>
+__global__ void __launch_bounds__(kThreads, MB)
+    fluid_step_vec_kernel_mb(const typename S::elem* __restrict__ cur,
+                             typename S::elem* __restrict__ nxt, VecGrid vg,
+                             typename S::compute omega, typename S::compute omega_minus,
+                             typename S::Params p) {
+  fluid_step_vec_body<L, S, CT, false, false>(cur, nxt, vg, omega, omega_minus, p, nullptr, {});
+}
+
+// Register budget of the plain step per lattice, precision and operator: the
+// resident blocks per SM its allocation must allow, or 0 for the compiler's
+// own allocation (launch bounds without a block count; note that an explicit
+// count of 1 is not the same: it lets the allocation grow, e.g. 64 -> 94
+// registers for the FP32 D3Q19 TRT step). Chosen by timing the settings 4..8
+// against the compiler's allocation at 256^3 on B200; kept only where it won
+// by more than the run-to-run spread, spilling at most 8 bytes:
+//   FP32 D3Q19  MRT 0.75 -> 0.82 of the copy bandwidth (64 registers)
+//               RLBM 0.63 -> 0.72 (80)
+template <class L, class S, int CT>
+__host__ __device__ constexpr int vec_min_blocks() {
+  constexpr bool f32 = std::is_same_v<typename S::elem, float>;
+  if constexpr (L::Q == 19 && f32) return CT == kMRT ? 8 : (CT == kRLBM ? 6 : 0);
+  return 0;
+}
+
+// Launches the plain vectorised step with its register budget.
+template <class L, class S, int CT>
+inline void launch_vec_step(const VecGrid& vg, dim3 grid, unsigned threads, cudaStream_t stream,
+                            const typename S::elem* cur, typename S::elem* nxt,
+                            typename S::compute omega, typename S::compute omega_minus,
+                            const typename S::Params& p) {
+  constexpr int mb = vec_min_blocks<L, S, CT>();
+  if constexpr (mb > 0)
+    fluid_step_vec_kernel_mb<L, S, CT, mb><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega,
+                                                                          omega_minus, p);
+  else
+    fluid_step_vec_kernel<L, S, CT><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega, omega_minus, p);
 }
 
 template <class S>
