@@ -601,7 +601,14 @@ __device__ __forceinline__ void populations_d3q27(const Real (&m)[27], Real (&f)
   bool ok = true;
   static_for<27>([&](auto K) { ok = ok && Div::bounded(m[LB_I(K)]); });
   populations_d3q27_with<Real, Div, true>(m, f, ok);
-  if (!ok) populations_d3q27_ieee<Real>(m, f);
+  if (!ok) {
+    // copies: passing m or f itself to the out-of-line call would make them
+    // addressable and move them to local memory on the fast path as well
+    Real mc[27], fc[27];
+    static_for<27>([&](auto K) { mc[LB_I(K)] = m[LB_I(K)]; });
+    populations_d3q27_ieee<Real>(mc, fc);
+    static_for<27>([&](auto K) { f[LB_I(K)] = fc[LB_I(K)]; });
+  }
 }
 
 // collide_mrt_d3q27 (lattice_mrt.hpp:1284-1305) with the projected
