@@ -7,9 +7,10 @@ The launchers mirror LB-Cube's CUDA launcher API (include/lattice_cuda.cuh:
 object with ``data_ptr()`` (a torch CUDA tensor) or a plain integer address can
 be passed as a buffer; ``None`` is the null pointer.
 
-The engine library (``liblbcube_b200.so`` next to this file) must have been
-built (``python lb-cube_b200/build.py``); importing this module without it
-raises, there is no CPU fallback.
+The engine library (``liblbcube_b200.so`` next to this file, or the file the
+environment variable ``LBCUBE_LIB`` names) must have been built
+(``python lb-cube_b200/build.py``); loading it without it raises, there is no
+CPU fallback.
 """
 from __future__ import annotations
 
@@ -18,7 +19,8 @@ import math
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "liblbcube_b200.so")
+# LBCUBE_LIB selects another build of the library (e.g. of an earlier commit, for A/B timing)
+LIB_PATH = os.environ.get("LBCUBE_LIB") or os.path.join(HERE, "liblbcube_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "lbcube_b200.h")
 
 LATTICES = {"D2Q9": 0, "D3Q19": 1, "D3Q27": 2, "D2Q5": 3, "D3Q7": 4}
