@@ -843,6 +843,9 @@ def run_engine(args, rank, world, local_rank):
             for key in ("objective", "dJ_dk", "dJ_dtau_c", "grad_a0_l2")}
         adjoint_reactive_16["forward_speedup_vs_fp32"] = round(adjoint_reactive["forward_ms"] /
                                                                adjoint_reactive_16["forward_ms"], 3)
+        # the same gradient against the FP32 forward run of the configuration
+        adjoint_reactive_16["cost_ratio_vs_fp32_forward"] = round(adjoint_reactive_16["gradient_ms"] /
+                                                                  adjoint_reactive["forward_ms"], 3)
         mixing = run_reactive_mixing(torch, E, dev)
         # per operator: the fastest 16-bit format meeting the 1e-3 velocity error
         # bar, with its speed-up over FP32 storage of the same operator

@@ -19,7 +19,7 @@
 namespace lbcube {
 
 template <class L, class Real, int CT>
-__global__ void __launch_bounds__(kThreads, 5)
+__global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
     adjoint_step_kernel(const Real* __restrict__ fn, const Real* __restrict__ lam_next,
                         Real* __restrict__ lam, Grid g, AdjointParams ap,
                         double* __restrict__ dtau_slots) {

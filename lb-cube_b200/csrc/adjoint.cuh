@@ -25,6 +25,12 @@
 
 namespace lbcube {
 
+// Resident blocks of kThreads per SM that the fluid adjoint kernels' register
+// allocation must allow: FP32 five (96 registers instead of 115), FP64 two
+// (FP64 values take two registers each; five blocks spilled up to 1 KB).
+template <class Real>
+constexpr int kAdjointBlocks = sizeof(Real) == 4 ? 5 : 2;
+
 struct AdjointParams {
   double omega, omega_minus;
   double domega_dtau, domega_minus_dtau;  // derivatives of the rates w.r.t. tau

@@ -207,9 +207,9 @@ __global__ void __launch_bounds__(kThreads)
 // Fluid part of adjoint step n: lambda_f^{n+1}(x, k) gains
 // (c_k - u) . ubar(x) / rho (u = j / rho of the cell), then the fluid adjoint
 // of adjoint.cuh; dJ/dtau to the block's slot.
-// Five blocks of 128 per SM (96 registers instead of 115).
+// Register budget kAdjointBlocks (adjoint.cuh).
 template <class FL, class Real, int CT, class SP>
-__global__ void __launch_bounds__(kThreads, 5)
+__global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
     coupled_fluid_adjoint_kernel(const typename SP::elem* __restrict__ fn,
                                  const Real* __restrict__ lf_next, const Real* __restrict__ ubar_in,
                                  Real* __restrict__ lf, Grid g, AdjointParams ap, float rho0,

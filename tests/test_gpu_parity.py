@@ -86,6 +86,26 @@ def test_d3q27_mrt_nonfinite_cells(engine, dev, real):
     assert np.array_equal(got, want, equal_nan=True)
 
 
+@pytest.mark.parametrize("lat", LATS)
+@pytest.mark.parametrize("real", ["float", "double"])
+def test_rlbm_tiny_and_nonfinite_cells_bitwise(engine, dev, lat, real):
+    """RLBM on cells scaled to tiny and subnormal magnitudes (some products
+    underflow to zero, so signed zeros meet in the sums) and on cells holding
+    an infinite or NaN population (a blown-up run): bit-identical to the
+    reference, NaN where it has NaN."""
+    nx, ny, nz = SIZES[lat][0]
+    f0 = U.random_state(lat, nx, ny, nz, REALS[real], seed=41)
+    n = U.cells(lat, nx, ny, nz)
+    tiny = np.float32(1e-36) if real == "float" else np.float64(1e-300)
+    f0[:, 0:n:3] *= tiny
+    f0[2, 7] = np.inf
+    f0[0, 11] = -np.inf
+    f0[5, 13] = np.nan
+    got = _run_steps(engine, lat, real, "RLBM", f0, nx, ny, nz, 1 / 0.6, 1, dev)
+    want = O.step(f0, lat, "RLBM", nx, ny, nz, 1 / 0.6, steps=1)
+    assert np.array_equal(got, want, equal_nan=True)
+
+
 def test_tgv_d3q19_fp64_bgk_64cube(engine, dev):
     """The C1 workload shape: D3Q19 BGK FP64 64^3 Taylor-Green (u0 0.05, rho 1,
     tau 0.6), 100 steps, bit-identical; KE decays."""
