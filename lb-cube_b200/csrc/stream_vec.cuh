@@ -261,6 +261,11 @@ __device__ __forceinline__ void gather_vec(const typename S::elem* __restrict__ 
   const bool right_edge = lane == 31 || x0 + V == g.nx;
   const int xl = x0 == 0 ? g.nx - 1 : x0 - 1;
   const int xr = x0 + V == g.nx ? 0 : x0 + V;
+  // In-plane row offsets fit in 32 bits (a plane has at most 2^31 - 1 cells,
+  // checked at launch): 64-bit arithmetic only for the plane base cur + plane i,
+  // which is the same for every thread.
+  const int zoff[3] = {zm * g.ny, z * g.ny, zp * g.ny};
+  const int ysel[3] = {ym, y, yp};
   static_for<L::Q>([&](auto I) {
     constexpr int i = LB_I(I);
     constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
@@ -273,8 +278,8 @@ __device__ __forceinline__ void gather_vec(const typename S::elem* __restrict__ 
       row = z == g.nz - 1 ? slab.halo_hi + (size_t)(zslot<L>(i) * g.ny + sy) * g.nx
                           : cur + plane * i + (size_t)((z + 1) * g.ny + sy) * g.nx;
     } else {
-      const int sz = cz == 0 ? z : (cz > 0 ? zm : zp);
-      row = cur + plane * i + (size_t)(sz * g.ny + sy) * g.nx;
+      const int off = (zoff[cz > 0 ? 0 : (cz < 0 ? 2 : 1)] + ysel[cy > 0 ? 0 : (cy < 0 ? 2 : 1)]) * g.nx;
+      row = (cur + plane * i) + off;
     }
     using R = typename S::compute;
     R val[V];
@@ -311,7 +316,7 @@ __device__ __forceinline__ void store_vec(typename S::elem* __restrict__ nxt, co
   using E = typename S::elem;
   constexpr int V = S::V;
   const size_t plane = (size_t)g.plane;
-  const size_t cell = (size_t)(z * g.ny + y) * g.nx + x0;
+  const int cell = (z * g.ny + y) * g.nx + x0;  // < plane <= 2^31 - 1
   static_for<L::Q>([&](auto I) {
     constexpr int i = LB_I(I);
     constexpr int cz = L::c[i][2];
@@ -319,7 +324,7 @@ __device__ __forceinline__ void store_vec(typename S::elem* __restrict__ nxt, co
 #pragma unroll
     for (int j = 0; j < V; ++j) col[j] = f[j][i];
     const RowWord<E, V> w = S::template encode_word<L, i>(col, p);
-    store_word<E, V>(nxt + plane * i + cell, w);
+    store_word<E, V>((nxt + plane * i) + cell, w);
     if constexpr (SLAB && cz > 0) {  // leaves through the top face
       if (z == g.nz - 1) store_word<E, V>(slab.send_hi + (size_t)(zslot<L>(i) * g.ny + y) * g.nx + x0, w);
     } else if constexpr (SLAB && cz < 0) {  // leaves through the bottom face
