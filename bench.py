@@ -69,8 +69,9 @@ def parse():
                     help="launch every kernel family a few times at 128^3 (1024^2 for 2-D), time each with "
                          "CUDA events and print one JSON line; the command the per-kernel ncu summary captures")
     ap.add_argument("--adjoint-only", action="store_true",
-                    help="run only the adjoint cost measurement (D3Q19 BGK FP32, --size cube, --steps "
-                         "steps, checkpoint every min(100, steps)) and print it; for profiling captures")
+                    help="run only the adjoint cost measurements (KE: D3Q19 BGK FP32; reactive: D3Q19 TRT "
+                         "+ 2 D3Q7 with --storage in the forward; --size cube, --steps steps, checkpoint "
+                         "every min(100, steps)) and print them; for profiling captures")
     a = ap.parse_args()
     global NX, NY, NZ, OP
     NX = NY = NZ = a.size
@@ -981,7 +982,8 @@ def main():
         E.load()
         res = run_adjoint_cost(torch, E, dev, n=args.size, steps=args.steps, interval=min(100, args.steps))
         rres = run_reactive_adjoint_cost(torch, E, dev, n=args.size, steps=args.steps,
-                                         interval=min(60, args.steps))
+                                         interval=min(100, args.steps),
+                                         storage=None if args.storage == "fp32" else args.storage)
         print(json.dumps({"adjoint": res, "adjoint_reactive": rres}), flush=True)
         return
     if world > 1:

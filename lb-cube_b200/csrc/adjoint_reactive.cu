@@ -128,8 +128,12 @@ struct ShiftedState {
   }
 };
 
-// Per-block FP64 slots of the reactive adjoint: dJ/dk, dJ/dtau, dJ/domega_c.
+// FP64 slots of the reactive adjoint, one set per warp (kThreads / 32 per
+// block): dJ/dk, dJ/dtau, dJ/domega_c. Each warp adds its own sums to its own
+// slots, so no kernel waits on a block barrier, and the fixed slot order keeps
+// the totals identical from run to run.
 constexpr int kReactiveSlots = 3;
+constexpr int kWarpsPerBlock = kThreads / 32;
 
 // Reaction part of adjoint step n at every cell x: from the pulled A^n, B^n,
 // lambda_A^{n+1}, lambda_B^{n+1} at x and the advecting velocity u^{n+1}(x)
@@ -195,12 +199,10 @@ __global__ void __launch_bounds__(kThreads)
     scatter<SL>(la, g, n, x, y, z, ma);
     scatter<SL>(lb, g, n, x, y, z, mb);
   }
-  __shared__ double tot[2];
-  block_sum_to<2>(acc, tot);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    slots[block_linear() * kReactiveSlots + 0] += tot[0];
-    slots[block_linear() * kReactiveSlots + 2] += tot[1];
+  warp_sum<2>(acc);
+  if ((threadIdx.x & 31) == 0) {
+    slots[warp_slot() * kReactiveSlots + 0] += acc[0];
+    slots[warp_slot() * kReactiveSlots + 2] += acc[1];
   }
 }
 
@@ -237,10 +239,8 @@ __global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
     scatter<FL>(lf, g, n, x, y, z, mu);
   }
   double v[1] = {dtau};
-  __shared__ double tot;
-  block_sum_to<1>(v, &tot);
-  __syncthreads();
-  if (threadIdx.x == 0) slots[block_linear() * kReactiveSlots + 1] += tot;
+  warp_sum<1>(v);
+  if ((threadIdx.x & 31) == 0) slots[warp_slot() * kReactiveSlots + 1] += v[0];
 }
 
 // Seeds lambda^N = dJ/d(f^N, A^N, B^N) and writes the block's FP64 share of J.
@@ -417,7 +417,7 @@ inline ReactiveLayout reactive_layout(int FQ, int SQ, int D, size_t elem, size_t
   l.off_lam = l.off_seg + (size_t)interval * l.state;
   l.off_ubar = l.off_lam + 2 * l.lstate;
   l.off_slots = l.off_ubar + l.ufield;
-  l.off_j = l.off_slots + up((size_t)l.blocks * kReactiveSlots * sizeof(double));
+  l.off_j = l.off_slots + up((size_t)l.blocks * kWarpsPerBlock * kReactiveSlots * sizeof(double));
   l.off_part = l.off_j + up((size_t)l.blocks * sizeof(double));
   l.off_stats = l.off_part + up((size_t)l.blocks * kStatSums * sizeof(double));
   l.total = l.off_stats + 256;
@@ -563,8 +563,9 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
                                                 j_slots);
   }
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
-  if ((err = cudaMemsetAsync(slots, 0, (size_t)lay.blocks * kReactiveSlots * sizeof(double), s)) !=
-      cudaSuccess)
+  if ((err = cudaMemsetAsync(slots, 0,
+                             (size_t)lay.blocks * kWarpsPerBlock * kReactiveSlots * sizeof(double),
+                             s)) != cudaSuccess)
     return err;
 
   ReactiveParams rp{};
@@ -610,9 +611,10 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
   } else {
     sum_slots_kernel<<<1, 1024, 0, s>>>(j_slots, lay.blocks, 1, 1.0 / (double)g.plane, out);
   }
-  sum_slots_kernel<<<1, 1024, 0, s>>>(slots + 0, lay.blocks, kReactiveSlots, 1.0, out + 1);
-  sum_slots_kernel<<<1, 1024, 0, s>>>(slots + 1, lay.blocks, kReactiveSlots, 1.0, out + 2);
-  sum_slots_kernel<<<1, 1024, 0, s>>>(slots + 2, lay.blocks, kReactiveSlots, -omega_c * omega_c,
+  const long long nslots = lay.blocks * kWarpsPerBlock;
+  sum_slots_kernel<<<1, 1024, 0, s>>>(slots + 0, nslots, kReactiveSlots, 1.0, out + 1);
+  sum_slots_kernel<<<1, 1024, 0, s>>>(slots + 1, nslots, kReactiveSlots, 1.0, out + 2);
+  sum_slots_kernel<<<1, 1024, 0, s>>>(slots + 2, nslots, kReactiveSlots, -omega_c * omega_c,
                                       out + 3);
   return cudaGetLastError();
 }

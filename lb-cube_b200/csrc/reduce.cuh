@@ -41,4 +41,20 @@ __device__ __forceinline__ void block_sum_to(double (&v)[N], double* out) {
   }
 }
 
+// Sums v[0..N) over the warp (all 32 lanes must call it); lane 0 ends with
+// the totals. Fixed reduction tree, no block barrier.
+template <int N>
+__device__ __forceinline__ void warp_sum(double (&v)[N]) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+  }
+}
+
+// Index of this warp's accumulation slot: kThreads / 32 slots per block.
+__device__ __forceinline__ long long warp_slot() {
+  return (long long)block_linear() * (kThreads / 32) + (long long)(threadIdx.x >> 5);
+}
+
 }  // namespace lbcube
