@@ -201,6 +201,7 @@ __device__ __forceinline__ void store_word(E* __restrict__ p, const RowWord<E, V
 struct VecGrid {
   Grid g;
   int tx, ty, xblocks, yblocks;
+  int z0;  // first plane of the launch (grid.y planes from here); 0 for a whole box
 };
 
 inline VecGrid make_vec_grid(const Grid& g, int V) {
@@ -211,6 +212,7 @@ inline VecGrid make_vec_grid(const Grid& g, int V) {
   v.ty = kThreads / v.tx;
   v.xblocks = (g.nx / V + v.tx - 1) / v.tx;
   v.yblocks = (g.ny + v.ty - 1) / v.ty;
+  v.z0 = 0;
   return v;
 }
 
@@ -354,7 +356,7 @@ __device__ __forceinline__ void fluid_step_vec_body(const typename S::elem* __re
   const int xb = blockIdx.x - yb * vg.xblocks;
   const int x0 = (xb * vg.tx + (int)(threadIdx.x % vg.tx)) * V;
   const int y = yb * vg.ty + (int)(threadIdx.x / vg.tx);
-  const int z = SLAB ? slab.z_begin + (int)blockIdx.y : (int)blockIdx.y;
+  const int z = SLAB ? slab.z_begin + (int)blockIdx.y : vg.z0 + (int)blockIdx.y;
   const bool active = x0 < g.nx && y < g.ny;
   R f[V][L::Q];
   gather_vec<L, S, SLAB>(cur, g, x0, y < g.ny ? y : 0, z, active, p, f, slab);
