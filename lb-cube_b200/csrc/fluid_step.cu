@@ -70,11 +70,20 @@ __global__ void __launch_bounds__(kThreads)
 // 2 FP32 D2Q9 / D3Q19 cells (8-byte words; D3Q19 TRT 0.99 of the copy
 // bandwidth against 0.80 at V = 4 and 0.76 at V = 1), 1 D3Q27 FP32 cell (BGK
 // 0.86 against 0.75 at V = 2, TRT 0.80 against 0.58) and 1 FP64 cell.
-// Operators whose register footprint would spill use the one-cell kernel.
+// The plain step of native storage runs the vectorised kernel only for FP32
+// D3Q19 BGK and TRT, where it is level with the one-cell kernel; every other
+// lattice, operator and precision measured faster with the one-cell kernel
+// (A/B at 256^3 / 4096^2, bitwise-identical outputs, fraction of the copy
+// bandwidth): D3Q27 FP32 BGK 0.76 -> 0.97, TRT 0.74 -> 0.95, MRT 0.48 -> 0.56,
+// RLBM 0.59 -> 0.68; D3Q27 FP64 BGK 0.91 -> 1.03, TRT 0.88 -> 1.03; D3Q19 FP32
+// MRT 0.80 -> 0.87; D3Q19 FP64 MRT 0.86 -> 0.97, RLBM 0.74 -> 0.84; D2Q9 FP32
+// 2-5 % and FP64 4-18 %. The one-cell kernel keeps fewer values live across
+// the gather, so its warps hide the load latency without register pressure.
+// The 16-bit storage and the slab step keep the vectorised kernel.
 template <class L, class Real>
 constexpr int kVecCells = (sizeof(Real) == 4 && L::Q != 27) ? 2 : 1;
 template <class L, class Real, int CT>
-constexpr bool kUseVec = !(L::Q == 27 && sizeof(Real) == 8 && (CT == kMRT || CT == kRLBM));
+constexpr bool kUseVec = sizeof(Real) == 4 && L::Q == 19 && (CT == kBGK || CT == kTRT);
 
 template <class L, class Real, int CT>
 cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, size_t nz,
