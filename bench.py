@@ -620,7 +620,17 @@ def run_kernel_survey(torch, E, dev, n=128, reps=10):
     g27 = torch.empty_like(f27)
     for op in ("BGK", "TRT", "MRT", "RLBM"):
         timed(f"step D3Q27 f32 {op}", cells * 216, lambda op=op: E.step_async("D3Q27", "float", op, f27, g27, n, n, n, om))
-    del f27, g27
+    d27 = slab.SlabDomain(torch, "D3Q27", "float", "BGK", n, n, n, om, 0, 1, dev)
+    d27.pack(f27)
+    ex27 = slab.LocalExchange([d27])
+    ex27.exchange_all()
+
+    def slab_step27():
+        d27.compute(f27, g27)
+        ex27.exchange_all()
+        return 0
+    timed("slab step D3Q27 f32 BGK (3 launches + face copies)", cells * 216, slab_step27)
+    del d27, ex27, f27, g27
     h = torch.empty((19, n, n, n), dtype=torch.int16, device=dev)
     hg = torch.empty_like(h)
     timed("encode_shifted D3Q19 q15s", cells * (76 + 38), lambda: E.encode_shifted_async("D3Q19", "q15s", "float", f, h, n, n, n))

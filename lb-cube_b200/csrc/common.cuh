@@ -25,6 +25,7 @@ struct Grid {
   int xblocks;
   int bx;           // threads per block
   long long plane;  // cells per population plane, nx * ny * nz (< 2^31)
+  int z0 = 0;       // first z plane of the launch (blockIdx.y = z - z0)
 
   __host__ __device__ long long blocks() const { return (long long)xblocks * ny * nz; }
 };
@@ -34,7 +35,7 @@ __device__ __forceinline__ bool cell_of(const Grid& g, int& x, int& y, int& z) {
   const int xb = blockIdx.x - row * g.xblocks;
   x = xb * g.bx + threadIdx.x;
   y = row;
-  z = blockIdx.y;
+  z = g.z0 + blockIdx.y;
   return x < g.nx;
 }
 

@@ -20,6 +20,7 @@
 
 #include "collide.cuh"
 #include "common.cuh"
+#include "step_cell.cuh"
 #include "stream_vec.cuh"
 #include "../../include/lbcube_b200.h"
 
@@ -57,17 +58,27 @@ cudaError_t launch_slab_step(const Real* cur, Real* nxt, size_t nx, size_t ny, s
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
   VecGrid vg = make_vec_grid(g, S::V);
   // Interior planes [1, nz - 1) of the range pull only within the slab (no
-  // wrap) and send nothing: the periodic-box kernel steps them, from plane
-  // vg.z0 on. Only the face planes run the SLAB form (halo rows, face sends),
+  // wrap) and send nothing: the periodic-box kernel that the plain step uses
+  // for this lattice, operator and precision (kUseVec) steps them, from plane
+  // z0 on. Only the face planes run the SLAB form (halo rows, face sends),
   // whose extra addressing and stores cost about 30 % per plane.
   const size_t ib = std::max<size_t>(z_begin, 1), ie = std::min<size_t>(z_end, nz - 1);
   if (ib < ie) {
-    vg.z0 = (int)ib;
-    dim3 grid = vec_grid_dims(vg);
-    grid.y = (unsigned)(ie - ib);
-    fluid_step_vec_kernel<L, S, CT><<<grid, vec_block_threads(vg), 0, s>>>(
-        cur, nxt, vg, omega, omega_minus, typename S::Params{});
-    vg.z0 = 0;
+    if constexpr (kUseVec<L, Real, CT>) {
+      vg.z0 = (int)ib;
+      dim3 grid = vec_grid_dims(vg);
+      grid.y = (unsigned)(ie - ib);
+      launch_vec_step<L, S, CT>(vg, grid, vec_block_threads(vg), s, cur, nxt, omega, omega_minus,
+                                typename S::Params{});
+      vg.z0 = 0;
+    } else {
+      Grid gi = g;
+      gi.z0 = (int)ib;
+      dim3 grid = grid_dims(gi);
+      grid.y = (unsigned)(ie - ib);
+      fluid_step_kernel<L, Real, CT><<<grid, block_dims(gi), 0, s>>>(cur, nxt, gi, omega,
+                                                                     omega_minus);
+    }
   }
   auto face = [&](size_t z) {
     dim3 grid = vec_grid_dims(vg);

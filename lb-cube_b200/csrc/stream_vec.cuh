@@ -389,45 +389,18 @@ __global__ void __launch_bounds__(kThreads)
   fluid_step_vec_body<L, S, CT, DIAG, SLAB>(cur, nxt, vg, omega, omega_minus, p, partials, slab);
 }
 
-// The plain step with a register budget: at least MB resident blocks of
-// kThreads per SM (the launch bounds' second argument).
-template <class L, class S, int CT, int MB>
-__global__ void __launch_bounds__(kThreads, MB)
-    fluid_step_vec_kernel_mb(const typename S::elem* __restrict__ cur,
-                             typename S::elem* __restrict__ nxt, VecGrid vg,
-                             typename S::compute omega, typename S::compute omega_minus,
-                             typename S::Params p) {
-  fluid_step_vec_body<L, S, CT, false, false>(cur, nxt, vg, omega, omega_minus, p, nullptr, {});
-}
-
-// Register budget of the plain step per lattice, precision and operator: the
-// resident blocks per SM its allocation must allow, or 0 for the compiler's
-// own allocation (launch bounds without a block count; note that an explicit
-// count of 1 is not the same: it lets the allocation grow, e.g. 64 -> 94
-// registers for the FP32 D3Q19 TRT step). Chosen by timing the settings 4..8
-// against the compiler's allocation at 256^3 on B200; kept only where it won
-// by more than the run-to-run spread, spilling at most 8 bytes:
-//   FP32 D3Q19  MRT 0.75 -> 0.82 of the copy bandwidth (64 registers)
-//               RLBM 0.63 -> 0.72 (80)
-template <class L, class S, int CT>
-__host__ __device__ constexpr int vec_min_blocks() {
-  constexpr bool f32 = std::is_same_v<typename S::elem, float>;
-  if constexpr (L::Q == 19 && f32) return CT == kMRT ? 8 : (CT == kRLBM ? 6 : 0);
-  return 0;
-}
-
-// Launches the plain vectorised step with its register budget.
+// Launches the plain vectorised step. (Register budgets, i.e. launch bounds
+// with a minimum block count, were timed at 4..8 blocks per SM for every
+// lattice, precision and operator; where they won, for FP32 D3Q19 MRT and
+// RLBM, the one-cell kernel (step_cell.cuh) won by more and now runs those.
+// An explicit count of 1 is not the compiler's default: it lets the
+// allocation grow, e.g. 64 -> 94 registers for the FP32 D3Q19 TRT step.)
 template <class L, class S, int CT>
 inline void launch_vec_step(const VecGrid& vg, dim3 grid, unsigned threads, cudaStream_t stream,
                             const typename S::elem* cur, typename S::elem* nxt,
                             typename S::compute omega, typename S::compute omega_minus,
                             const typename S::Params& p) {
-  constexpr int mb = vec_min_blocks<L, S, CT>();
-  if constexpr (mb > 0)
-    fluid_step_vec_kernel_mb<L, S, CT, mb><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega,
-                                                                          omega_minus, p);
-  else
-    fluid_step_vec_kernel<L, S, CT><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega, omega_minus, p);
+  fluid_step_vec_kernel<L, S, CT><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega, omega_minus, p);
 }
 
 template <class S>

@@ -15,7 +15,8 @@ import slab
 pytestmark = pytest.mark.gpu
 
 CASES = [("D3Q19", "float", "TRT", (16, 6, 8)), ("D3Q19", "double", "BGK", (10, 5, 6)),
-         ("D3Q27", "float", "MRT", (8, 4, 4)), ("D3Q19", "float", "RLBM", (12, 3, 4))]
+         ("D3Q27", "float", "MRT", (8, 4, 4)), ("D3Q19", "float", "RLBM", (12, 3, 4)),
+         ("D3Q27", "double", "TRT", (6, 4, 8))]
 
 
 def whole_box(lat, dn, op, f, dims, steps, dev):
