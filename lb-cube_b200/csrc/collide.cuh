@@ -373,8 +373,12 @@ __host__ __device__ constexpr int tensor_slot27() {
   return t27(D3Q27::c[i][0] + 1, D3Q27::c[i][1] + 1, D3Q27::c[i][2] + 1);
 }
 
-// transform_to_moments_d3q27 (lattice_mrt.hpp:1023-1117).
-template <class Real>
+// transform_to_moments_d3q27 (lattice_mrt.hpp:1023-1117). DROP leaves out the
+// terms whose basis factor is 0 (the c = 0 term of each first-order sum): for
+// finite populations each is +-0, and adding +-0 to a sum that starts at +0
+// changes nothing (a round-to-nearest sum is -0 only when both addends are -0,
+// so such a sum is never -0). Callers pass DROP only for finite inputs.
+template <class Real, bool DROP = false>
 __device__ __forceinline__ void moments_d3q27(const Real (&f)[27], Real (&m)[27]) {
   Real p[27], xt[27], xyt[27], raw[27];
   static_for<27>([&](auto I) { p[tensor_slot27<LB_I(I)>()] = f[LB_I(I)]; });
@@ -383,7 +387,7 @@ __device__ __forceinline__ void moments_d3q27(const Real (&f)[27], Real (&m)[27]
     Real v = Real(0);
     static_for<3>([&](auto K) {
       constexpr int k = LB_I(K);
-      v += Real(p27_basis(a, k - 1)) * p[t27(k, b, c)];
+      if constexpr (!DROP || p27_basis(a, k - 1) != 0) v += Real(p27_basis(a, k - 1)) * p[t27(k, b, c)];
     });
     xt[t27(a, b, c)] = v;
   });
@@ -392,7 +396,7 @@ __device__ __forceinline__ void moments_d3q27(const Real (&f)[27], Real (&m)[27]
     Real v = Real(0);
     static_for<3>([&](auto K) {
       constexpr int k = LB_I(K);
-      v += Real(p27_basis(b, k - 1)) * xt[t27(a, k, c)];
+      if constexpr (!DROP || p27_basis(b, k - 1) != 0) v += Real(p27_basis(b, k - 1)) * xt[t27(a, k, c)];
     });
     xyt[t27(a, b, c)] = v;
   });
@@ -401,7 +405,7 @@ __device__ __forceinline__ void moments_d3q27(const Real (&f)[27], Real (&m)[27]
     Real v = Real(0);
     static_for<3>([&](auto K) {
       constexpr int k = LB_I(K);
-      v += Real(p27_basis(c, k - 1)) * xyt[t27(a, b, k)];
+      if constexpr (!DROP || p27_basis(c, k - 1) != 0) v += Real(p27_basis(c, k - 1)) * xyt[t27(a, b, k)];
     });
     raw[t27(a, b, c)] = v;
   });
@@ -497,7 +501,14 @@ struct Div27Const {
 // CHECK, `ok` is cleared when a dividend that Div::checked names is outside
 // the range Div::safe accepts. Each dividend is +-x or +-2x for a value x
 // checked here (|2x| >= |x|, and the sign does not matter).
-template <class Real, class Div, bool CHECK>
+//
+// DROP (fast transform only, whose result is used only when `ok` holds, i.e.
+// every intermediate is finite): leaves out the terms whose basis factor is 0
+// (+-0 added to a sum that starts at +0, see moments_d3q27) and forms
+// (x * -2) / 6 as -(x / 3). Both are the correctly rounded -x/3 (x * -2 is
+// exact), and the x = +-0 cases differ only in the sign of a zero term, which
+// the sum absorbs.
+template <class Real, class Div, bool CHECK, bool DROP = false>
 __device__ __forceinline__ void populations_d3q27_with(const Real (&m)[27], Real (&f)[27], bool& ok) {
   Real raw[27], zi[27], yzi[27], p[27];
   auto check = [&](auto n, Real x) {
@@ -549,7 +560,13 @@ __device__ __forceinline__ void populations_d3q27_with(const Real (&m)[27], Real
     Real v = Real(0);
     static_for<3>([&](auto K) {
       constexpr int k = LB_I(K);
-      v += Div::template div<p27_norm(k)>(raw[t27(a, b, k)] * Real(p27_basis(k, c - 1)));
+      constexpr int basis = p27_basis(k, c - 1);
+      if constexpr (DROP && basis == 0) {
+      } else if constexpr (DROP && basis == -2) {
+        v += -Div::template div<3>(raw[t27(a, b, k)]);
+      } else {
+        v += Div::template div<p27_norm(k)>(raw[t27(a, b, k)] * Real(basis));
+      }
     });
     zi[t27(a, b, c)] = v;
   });
@@ -562,7 +579,13 @@ __device__ __forceinline__ void populations_d3q27_with(const Real (&m)[27], Real
     Real v = Real(0);
     static_for<3>([&](auto K) {
       constexpr int k = LB_I(K);
-      v += Div::template div<p27_norm(k)>(zi[t27(a, k, c)] * Real(p27_basis(k, b - 1)));
+      constexpr int basis = p27_basis(k, b - 1);
+      if constexpr (DROP && basis == 0) {
+      } else if constexpr (DROP && basis == -2) {
+        v += -Div::template div<3>(zi[t27(a, k, c)]);
+      } else {
+        v += Div::template div<p27_norm(k)>(zi[t27(a, k, c)] * Real(basis));
+      }
     });
     yzi[t27(a, b, c)] = v;
   });
@@ -575,7 +598,13 @@ __device__ __forceinline__ void populations_d3q27_with(const Real (&m)[27], Real
     Real v = Real(0);
     static_for<3>([&](auto K) {
       constexpr int k = LB_I(K);
-      v += Div::template div<p27_norm(k)>(yzi[t27(k, b, c)] * Real(p27_basis(k, a - 1)));
+      constexpr int basis = p27_basis(k, a - 1);
+      if constexpr (DROP && basis == 0) {
+      } else if constexpr (DROP && basis == -2) {
+        v += -Div::template div<3>(yzi[t27(k, b, c)]);
+      } else {
+        v += Div::template div<p27_norm(k)>(yzi[t27(k, b, c)] * Real(basis));
+      }
     });
     p[t27(a, b, c)] = v;
   });
@@ -600,7 +629,7 @@ __device__ __forceinline__ void populations_d3q27(const Real (&m)[27], Real (&f)
   using Div = Div27Const<Real>;
   bool ok = true;
   static_for<27>([&](auto K) { ok = ok && Div::bounded(m[LB_I(K)]); });
-  populations_d3q27_with<Real, Div, true>(m, f, ok);
+  populations_d3q27_with<Real, Div, true, true>(m, f, ok);
   if (!ok) {
     // copies: passing m or f itself to the out-of-line call would make them
     // addressable and move them to local memory on the fast path as well
@@ -611,13 +640,9 @@ __device__ __forceinline__ void populations_d3q27(const Real (&m)[27], Real (&f)
   }
 }
 
-// collide_mrt_d3q27 (lattice_mrt.hpp:1284-1305) with the projected
-// equilibrium of :1242-1268 and MrtRelaxationRates_D3Q27 (:161-204).
+// Projected equilibrium populations of collide_mrt_d3q27 (lattice_mrt.hpp:1242-1268).
 template <class Real>
-__device__ __forceinline__ void collide_mrt_d3q27(Real (&f)[27], Real omega) {
-  Real rho, u[3], m[27], fe[27], eq[27];
-  macro_state<D3Q27>(f, rho, u);
-  moments_d3q27<Real>(f, m);
+__device__ __forceinline__ void equilibrium_d3q27(Real rho, const Real (&u)[3], Real (&fe)[27]) {
   const Real ux = u[0], uy = u[1], uz = u[2];
   const Real usq = ux * ux + uy * uy + uz * uz;
   static_for<27>([&](auto I) {
@@ -626,7 +651,11 @@ __device__ __forceinline__ void collide_mrt_d3q27(Real (&f)[27], Real omega) {
     const Real cu = c_dot<D3Q27, i>(u);
     fe[i] = Real(wd) * rho * (Real{1} + Real{3} * cu + Real{4.5} * cu * cu - Real{1.5} * usq);
   });
-  moments_d3q27<Real>(fe, eq);
+}
+
+// Moment relaxation with MrtRelaxationRates_D3Q27 (lattice_mrt.hpp:161-204).
+template <class Real>
+__device__ __forceinline__ void relax_d3q27(Real (&m)[27], const Real (&eq)[27], Real omega) {
   const Real s_b = Real(1.19), s_e = Real(1.1), s_eps = Real(1.2), s_q = Real(1.2);
   static_for<27>([&](auto I) {
     constexpr int i = LB_I(I);
@@ -635,6 +664,49 @@ __device__ __forceinline__ void collide_mrt_d3q27(Real (&f)[27], Real omega) {
       m[i] -= s * (m[i] - eq[i]);
     }
   });
+}
+
+// The reference's collision term for term, with IEEE divisions: the path of
+// every cell that the guard of collide_mrt_d3q27 sends away. Out of line, so
+// its code stays out of the kernel's instruction stream.
+template <class Real>
+static __device__ __noinline__ void collide_mrt_d3q27_full(Real (&f)[27], Real omega) {
+  Real rho, u[3], m[27], fe[27], eq[27];
+  macro_state<D3Q27>(f, rho, u);
+  moments_d3q27<Real>(f, m);
+  equilibrium_d3q27<Real>(rho, u, fe);
+  moments_d3q27<Real>(fe, eq);
+  relax_d3q27<Real>(m, eq, omega);
+  bool ok = true;
+  populations_d3q27_with<Real, Div27Ieee, false>(m, f, ok);
+}
+
+// collide_mrt_d3q27 (lattice_mrt.hpp:1284-1305) with the projected
+// equilibrium of :1242-1268 and MrtRelaxationRates_D3Q27 (:161-204).
+// Guard: |rho| <= 2^60 and every |u_d| <= 2^20 (false for NaN). A finite
+// density means every population is finite (a non-finite addend makes the
+// sum inf or NaN), and the bounds keep every equilibrium population below
+// 2^106, so both forward transforms may drop their zero-factor terms
+// (moments_d3q27). Other cells run the full expression out of line.
+template <class Real>
+__device__ __forceinline__ void collide_mrt_d3q27(Real (&f)[27], Real omega) {
+  Real rho, u[3];
+  macro_state<D3Q27>(f, rho, u);
+  const bool fast = fabs(rho) <= Real(0x1p60) && fabs(u[0]) <= Real(0x1p20) &&
+                    fabs(u[1]) <= Real(0x1p20) && fabs(u[2]) <= Real(0x1p20);
+  if (!fast) {
+    // a copy: passing f itself would make it addressable (local memory)
+    Real fc[27];
+    static_for<27>([&](auto K) { fc[LB_I(K)] = f[LB_I(K)]; });
+    collide_mrt_d3q27_full<Real>(fc, omega);
+    static_for<27>([&](auto K) { f[LB_I(K)] = fc[LB_I(K)]; });
+    return;
+  }
+  Real m[27], fe[27], eq[27];
+  moments_d3q27<Real, true>(f, m);
+  equilibrium_d3q27<Real>(rho, u, fe);
+  moments_d3q27<Real, true>(fe, eq);
+  relax_d3q27<Real>(m, eq, omega);
   populations_d3q27<Real>(m, f);
 }
 
