@@ -34,3 +34,17 @@ def rel_l2(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def same_bits(got, want):
+    """Bit-for-bit equality of two float arrays of one dtype, NaN payloads
+    aside: NaN exactly where the other has NaN, every other element the same
+    bit pattern (so +0 and -0 differ, unlike ==)."""
+    got, want = np.asarray(got), np.asarray(want)
+    if got.shape != want.shape or got.dtype != want.dtype:
+        return False
+    gn, wn = np.isnan(got), np.isnan(want)
+    if not np.array_equal(gn, wn):
+        return False
+    as_int = {2: np.uint16, 4: np.uint32, 8: np.uint64}[got.dtype.itemsize]
+    return np.array_equal(got.view(as_int)[~gn], want.view(as_int)[~wn])

@@ -40,7 +40,7 @@ def test_macro_fields_bitwise(engine, dev, lat, dn):
     got = device_macro(lat, dn, f, nx, ny, nz, dev)
     want = macro_real(f, lat, nx, ny, nz)
     for g, w in zip(got, want):
-        assert np.array_equal(g, w)
+        assert U.same_bits(g, w)
 
 
 @pytest.mark.parametrize("sl", ["D2Q5", "D3Q7"])

@@ -51,7 +51,7 @@ def test_step_bitwise(engine, dev, lat, real, op):
         f0 = U.random_state(lat, nx, ny, nz, REALS[real], seed=100 + k)
         got = _run_steps(engine, lat, real, op, f0, nx, ny, nz, 1 / 0.6, 5, dev)
         want = O.step(f0, lat, op, nx, ny, nz, 1 / 0.6, steps=5)
-        assert np.array_equal(got, want), f"{lat} {real} {op} {nx}x{ny}x{nz}: max |d| {np.abs(got - want).max()}"
+        assert U.same_bits(got, want), f"{lat} {real} {op} {nx}x{ny}x{nz}: max |d| {np.abs(got - want).max()}"
 
 
 @pytest.mark.parametrize("scale", [1e-24, 1e-33, 1e-38, 1e-42])
@@ -68,7 +68,7 @@ def test_d3q27_mrt_float_tiny_states_bitwise(engine, dev, scale):
     f0 = np.ascontiguousarray(f0.reshape(27, -1))
     got = _run_steps(engine, "D3Q27", "float", "MRT", f0, nx, ny, nz, 1 / 0.6, 5, dev)
     want = O.step(f0, "D3Q27", "MRT", nx, ny, nz, 1 / 0.6, steps=5)
-    assert np.array_equal(got, want), f"max |d| {np.abs(got - want).max()}"
+    assert U.same_bits(got, want), f"max |d| {np.abs(got - want).max()}"
 
 
 @pytest.mark.parametrize("real", ["float", "double"])
@@ -83,7 +83,7 @@ def test_d3q27_mrt_nonfinite_cells(engine, dev, real):
     f0[12, 77] = np.nan
     got = _run_steps(engine, "D3Q27", real, "MRT", f0, nx, ny, nz, 1 / 0.6, 1, dev)
     want = O.step(f0, "D3Q27", "MRT", nx, ny, nz, 1 / 0.6, steps=1)
-    assert np.array_equal(got, want, equal_nan=True)
+    assert U.same_bits(got, want)
 
 
 @pytest.mark.parametrize("lat", LATS)
@@ -103,7 +103,7 @@ def test_rlbm_tiny_and_nonfinite_cells_bitwise(engine, dev, lat, real):
     f0[5, 13] = np.nan
     got = _run_steps(engine, lat, real, "RLBM", f0, nx, ny, nz, 1 / 0.6, 1, dev)
     want = O.step(f0, lat, "RLBM", nx, ny, nz, 1 / 0.6, steps=1)
-    assert np.array_equal(got, want, equal_nan=True)
+    assert U.same_bits(got, want)
 
 
 def test_tgv_d3q19_fp64_bgk_64cube(engine, dev):
@@ -119,7 +119,7 @@ def test_tgv_d3q19_fp64_bgk_64cube(engine, dev):
     f0 = O.init_equilibrium("D3Q19", np.ones(n ** 3), u, n, n, n)
     got = _run_steps(engine, "D3Q19", "double", "BGK", f0, n, n, n, 1 / 0.6, 100, dev)
     want = O.step(f0, "D3Q19", "BGK", n, n, n, 1 / 0.6, steps=100)
-    assert np.array_equal(got, want)
+    assert U.same_bits(got, want)
     _, u1 = O.macro_fields(got, "D3Q19", n, n, n)
     assert (u1 ** 2).sum() < (u ** 2).sum()
 
@@ -149,7 +149,7 @@ def test_2d_z_extent_forced_to_one(engine, dev):
         nxt = torch.empty_like(cur)
         assert engine.launch_step_gpu("D2Q9", "double", "TRT", cur, nxt, nx, ny, nz, 1.3) == 0
         torch.cuda.synchronize()
-        assert np.array_equal(nxt.cpu().numpy(), want)
+        assert U.same_bits(nxt.cpu().numpy(), want)
 
 
 @pytest.mark.parametrize("lat", LATS)
@@ -167,7 +167,7 @@ def test_scalar_step_bitwise(engine, dev, lat, real):
         cur, nxt = nxt, cur
     torch.cuda.synchronize()
     want = O.scalar_step(g0, f, lat, nx, ny, nz, 1 / 0.8, 2e-3, steps=4)
-    assert np.array_equal(cur.cpu().numpy(), want)
+    assert U.same_bits(cur.cpu().numpy(), want)
 
 
 def _reaction_tol(real):
@@ -210,7 +210,7 @@ def test_reaction_equal_species_branch_bitwise(engine, dev):
         ta, na, tb, nb = na, ta, nb, tb
     torch.cuda.synchronize()
     wa, _ = O.reaction_ab(g, g, fl, "D2Q9", nx, ny, 1, 1 / 0.8, 0.005, steps=200)
-    assert np.array_equal(ta.cpu().numpy(), wa)
+    assert U.same_bits(ta.cpu().numpy(), wa)
     assert abs(ta[:, 0].sum().item() - 1.0 / (1.0 + 0.005 * 200)) <= 1e-4
 
 
@@ -248,7 +248,7 @@ def test_fused_fluid_reaction(engine, dev, lat, real, op, size):
     torch.cuda.synchronize()
     assert torch.equal(tf, sf) and torch.equal(ta, sa) and torch.equal(tb, sb)
     wf, wa, wb = O.coupled_reaction(f0, a0, b0, lat, op, nx, ny, nz, om, omc, k, steps=steps)
-    assert np.array_equal(tf.cpu().numpy(), wf)
+    assert U.same_bits(tf.cpu().numpy(), wf)
     assert U.rel_l2(ta.cpu().numpy(), wa) <= _reaction_tol(real)
     assert U.rel_l2(tb.cpu().numpy(), wb) <= _reaction_tol(real)
 
@@ -315,4 +315,4 @@ def test_init_equilibrium_bitwise(engine, dev, lat, real):
                                                torch.from_numpy(u).to(dev), out, nx, ny, nz))
     torch.cuda.synchronize()
     want = O.init_equilibrium(lat, rho.astype(np.float64), u.astype(np.float64), nx, ny, nz, dt)
-    assert np.array_equal(out.cpu().numpy(), want)
+    assert U.same_bits(out.cpu().numpy(), want)
