@@ -18,15 +18,21 @@
 
 namespace lbcube {
 
-// Cells per thread of the 16-bit kernels (8-byte words).
-constexpr int kShiftedCells = 4;
+// Cells per thread of the 16-bit kernels: four (8-byte words), except two
+// (4-byte words) for E3M12, whose software codec makes the step arithmetic-
+// bound. D3Q19 at 256^3, fraction of the copy bandwidth at 4 / 2 cells: F16
+// TRT 0.83 / 0.58, MRT 0.74 / 0.66, Q15 TRT 0.74 / 0.52, BF16 TRT 0.79 / 0.57,
+// E3M12 TRT 0.25 / 0.31.
+template <int FMT>
+constexpr int kShiftedCells = FMT == kE3M12S ? 2 : 4;
 
 // BGK, TRT and the D2Q9 / D3Q19 MRT collide on the stored deviations; D3Q27
 // MRT and RLBM decode to f and run the reference operator.
 template <class L, int FMT, int CT>
 using ShiftedPolicy =
     std::conditional_t<CT == kBGK || CT == kTRT || (CT == kMRT && L::Q != 27),
-                       DevStorage<FMT, kShiftedCells>, ShiftedStorage<FMT, kShiftedCells>>;
+                       DevStorage<FMT, kShiftedCells<FMT>>,
+                       ShiftedStorage<FMT, kShiftedCells<FMT>>>;
 
 template <class L, int FMT, int CT>
 cudaError_t launch_shifted_step(const void* cur, void* nxt, size_t nx, size_t ny, size_t nz,
@@ -39,6 +45,10 @@ cudaError_t launch_shifted_step(const void* cur, void* nxt, size_t nx, size_t ny
   const Span reads[1] = {{cur, bytes}};
   const Span writes[1] = {{nxt, bytes}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  // the public contract for every format: x_extent a multiple of 4, buffers
+  // 8-byte aligned (covers the word shape of both cell counts)
+  if (g.nx % 4 != 0 || (uintptr_t)cur % 8 != 0 || (uintptr_t)nxt % 8 != 0)
+    return cudaErrorInvalidValue;
   if (!vec_eligible<S>(g, cur, nxt)) return cudaErrorInvalidValue;  // nx % V, word alignment
   const float omega_minus = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
   const VecGrid vg = make_vec_grid(g, S::V);
