@@ -2,8 +2,8 @@
 //
 // No reference counterpart (the reference runs one domain on one device). The
 // box is cut into slabs along z; each rank owns nz_local planes in the
-// reference's [Q, Z, Y, X] layout and steps them with the same kernel as the
-// periodic box (fluid_step_vec_kernel), except that the populations crossing
+// reference's [Q, Z, Y, X] layout and steps them with the same kernels as the
+// periodic box (kUseVec, step_cell.cuh), except that the populations crossing
 // a slab face are pulled from halo planes (SlabArgs, stream_vec.cuh) and the
 // ones leaving through a face are also stored, in the same pass, into send
 // planes for the neighbour. One exchange per step moves the send planes into
@@ -26,10 +26,6 @@
 
 namespace lbcube {
 
-// Cells per thread, as the periodic step (fluid_step.cu kVecCells).
-template <class L, class Real>
-constexpr int kSlabCells = (sizeof(Real) == 4 && L::Q != 27) ? 2 : 1;
-
 template <class L, class Real, int CT>
 cudaError_t launch_slab_step(const Real* cur, Real* nxt, size_t nx, size_t ny, size_t nz,
                              Real omega, const Real* halo_lo, const Real* halo_hi, Real* send_lo,
@@ -45,7 +41,7 @@ cudaError_t launch_slab_step(const Real* cur, Real* nxt, size_t nx, size_t ny, s
   // a face plane reads both halos when nz == 1
   if (nz == 1 && (halo_lo == nullptr || halo_hi == nullptr || send_lo == nullptr || send_hi == nullptr))
     return cudaErrorInvalidDevicePointer;
-  using S = NativeStorage<Real, kSlabCells<L, Real>>;
+  using S = NativeStorage<Real, kVecCells<L, Real>>;  // as the periodic step
   if (!vec_eligible<S>(g, cur, nxt)) return cudaErrorInvalidValue;
   const size_t bytes = (size_t)L::Q * g.plane * sizeof(Real);
   const size_t hbytes = (size_t)zcount<L>() * g.ny * g.nx * sizeof(Real);
