@@ -27,15 +27,17 @@ cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, 
   const Span writes[1] = {{nxt, bytes}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
-  using S = NativeStorage<Real, kVecCells<L, Real>>;
-  if (kUseVec<L, Real, CT> && vec_eligible<S>(g, cur, nxt)) {
-    const VecGrid vg = make_vec_grid(g, S::V);
-    launch_vec_step<L, S, CT>(vg, vec_grid_dims(vg), vec_block_threads(vg), stream, cur, nxt, omega,
-                              omega_minus, typename S::Params{});
-  } else {
-    fluid_step_kernel<L, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(cur, nxt, g, omega,
-                                                                           omega_minus);
+  if constexpr (kUseVec<L, Real, CT>) {
+    using S = NativeStorage<Real, kVecCells<L, Real>>;
+    if (vec_eligible<S>(g, cur, nxt)) {
+      const VecGrid vg = make_vec_grid(g, S::V);
+      launch_vec_step<L, S, CT>(vg, vec_grid_dims(vg), vec_block_threads(vg), stream, cur, nxt,
+                                omega, omega_minus, typename S::Params{});
+      return cudaGetLastError();
+    }
   }
+  fluid_step_kernel<L, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(cur, nxt, g, omega,
+                                                                         omega_minus);
   return cudaGetLastError();
 }
 
@@ -57,15 +59,18 @@ cudaError_t launch_fluid_step_diag(const Real* cur, Real* nxt, size_t nx, size_t
   const Span writes[3] = {{nxt, bytes}, {partials, need}, {out, kDiagOut * sizeof(double)}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
-  using S = NativeStorage<Real, kVecCells<L, Real>>;
-  long long count;
-  if (kUseVec<L, Real, CT> && vec_eligible<S>(g, cur, nxt)) {
-    const VecGrid vg = make_vec_grid(g, S::V);
-    const dim3 grid = vec_grid_dims(vg);
-    count = (long long)grid.x * grid.y;  // <= g.blocks(): a vector block spans >= one row block
-    fluid_step_vec_kernel<L, S, CT, true><<<grid, vec_block_threads(vg), 0, stream>>>(
-        cur, nxt, vg, omega, omega_minus, typename S::Params{}, partials);
-  } else {
+  long long count = -1;
+  if constexpr (kUseVec<L, Real, CT>) {
+    using S = NativeStorage<Real, kVecCells<L, Real>>;
+    if (vec_eligible<S>(g, cur, nxt)) {
+      const VecGrid vg = make_vec_grid(g, S::V);
+      const dim3 grid = vec_grid_dims(vg);
+      count = (long long)grid.x * grid.y;  // <= g.blocks(): a vector block spans >= one row block
+      fluid_step_vec_kernel<L, S, CT, true><<<grid, vec_block_threads(vg), 0, stream>>>(
+          cur, nxt, vg, omega, omega_minus, typename S::Params{}, partials);
+    }
+  }
+  if (count < 0) {
     count = g.blocks();
     fluid_step_kernel<L, Real, CT, true><<<grid_dims(g), block_dims(g), 0, stream>>>(
         cur, nxt, g, omega, omega_minus, partials);

@@ -79,8 +79,12 @@ __global__ void __launch_bounds__(kThreads)
 // bandwidth): D3Q27 FP32 BGK 0.76 -> 0.97, TRT 0.74 -> 0.95, MRT 0.48 -> 0.56,
 // RLBM 0.59 -> 0.68; D3Q27 FP64 BGK 0.91 -> 1.03, TRT 0.88 -> 1.03; D3Q19 FP32
 // MRT 0.80 -> 0.87; D3Q19 FP64 MRT 0.86 -> 0.97, RLBM 0.74 -> 0.84; D2Q9 FP32
-// 2-5 % and FP64 4-18 %. The one-cell kernel keeps fewer values live across
-// the gather, so its warps hide the load latency without register pressure.
+// 2-5 % and FP64 4-18 %. Two cells per thread double the live populations
+// (D3Q19 FP32 MRT: 80 registers against 40); at one cell per thread (D3Q27
+// FP32, FP64) both kernels hold the same values, and they differ in the
+// gather: the vectorised kernel exchanges x-neighbours by warp shuffles with
+// extra loads at the warp edges, the one-cell kernel loads every neighbour
+// directly (overlapping row segments, served by L1).
 // The slab step follows the same rule on its interior planes; its face planes
 // and the 16-bit storage keep the vectorised kernel.
 template <class L, class Real>
