@@ -173,35 +173,28 @@ extern "C" int lbm_reactive_stats_finalize_async(int fluid_lattice, int precisio
 // array of fixed size, reserved on every GPU that loads the library until the
 // process exits; nothing is allocated per call.
 // ----------------------------------------------------------------------------
-#include <mutex>
-
 namespace lbcube {
 
 // Partial sums for up to this many 128-cell row segments (blocks):
 // ceil(nx / 128) * ny * nz <= 131072, e.g. 256^3 or 1024^2. 5 MiB per GPU.
 constexpr long long kNoAllocMaxBlocks = 131072;
+static_assert(kNoAllocMaxBlocks == LBM_STATS_NOALLOC_MAX_BLOCKS,
+              "the array size and the limit the header publishes must agree");
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxBlocks * kStatSums];
 
-constexpr int kNoAllocMaxDevices = 64;
-static std::mutex g_noalloc_mutex;
-static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of g_noalloc_partials on the current device. In host code
-// the array's name only stands in for the symbol, so the address is looked up
-// once per device (with that device current) and cached.
+// Device address of g_noalloc_partials in the calling thread's current
+// context. In host code the array's name only stands in for the symbol. The
+// address belongs to the context the library's device code is loaded in, not
+// to the device ordinal: a host that creates or switches contexts itself
+// (cuCtxCreate, cuCtxSetCurrent), or resets the device, gets the array at
+// another address. So it is looked up on every call (a host-side query, no
+// device work); the first lookup in a context may load the library's device
+// code into it.
 static cudaError_t noalloc_scratch(double** out) {
-  int dev = 0;
-  cudaError_t err = cudaGetDevice(&dev);
+  void* p = nullptr;
+  const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_partials);
   if (err != cudaSuccess) return err;
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_ptr[dev] == nullptr) {
-    void* p = nullptr;
-    err = cudaGetSymbolAddress(&p, g_noalloc_partials);
-    if (err != cudaSuccess) return err;
-    g_noalloc_ptr[dev] = static_cast<double*>(p);
-  }
-  *out = g_noalloc_ptr[dev];
+  *out = static_cast<double*>(p);
   return cudaSuccess;
 }
 

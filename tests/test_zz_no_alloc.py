@@ -6,8 +6,9 @@ scalar fields, so it cannot provide the partial-sum scratch that
 lbm_reactive_stats_async takes. lbm_reactive_stats_noalloc_async keeps that
 scratch in a fixed array inside the library. Called through the C ABI, it must
 give the same diagnostics as the scratch-taking entry point (within the 1e-12
-relative tolerance of the statistics tests) on two calls in a row, and reject a
-domain larger than its array. This file is collected last on purpose.
+relative tolerance of the statistics tests) on two calls in a row, accept the
+largest domain its array holds and reject a larger one. This file is
+collected last on purpose.
 """
 import ctypes as C
 
@@ -54,12 +55,46 @@ def test_noalloc_stats_match_scratch_entry(lat, real, shape):
             assert abs(g - w) <= 1e-12 * max(abs(w), 1e-6), f"call {call}: {name}"
 
 
-def test_noalloc_rejects_domains_beyond_its_array():
+def _fields(lat, nx, ny, nz, seed):
+    """Two scalar fields of the declared extent in separate device buffers, so
+    that no overlap check can reject the call."""
     dev = torch.device("cuda:0")
-    out = torch.empty(8, dtype=torch.float64, device=dev)
-    fn = _noalloc()
-    # ceil(129 / 128) * 256 * 257 = 131584 row segments > 131072; the call is
-    # rejected before any kernel runs, so the (never read) field addresses can be fake.
-    rc = fn(E.LATTICES["D3Q7"], E.REALS["float"], 0x10000000, 0x90000000, 129, 256, 257, 0.02,
-            out.data_ptr(), None)
+    q = E.Q_OF[lat]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    a = torch.rand((q, nz, ny, nx), generator=gen, device=dev) * 0.2
+    b = torch.rand((q, nz, ny, nx), generator=gen, device=dev) * 0.2
+    return a, b
+
+
+def test_noalloc_accepts_the_largest_domain_its_array_holds():
+    # ceil(256 / 128) * 256 * 256 = 131072 row segments: exactly the array's capacity
+    assert E.stats_partials_bytes("D3Q19", 256, 256, 256) == 131072 * 5 * 8
+    a, b = _fields("D3Q7", 256, 256, 256, seed=83)
+    nbytes = E.stats_partials_bytes("D3Q19", 256, 256, 256)
+    part = torch.empty(nbytes // 8, dtype=torch.float64, device=a.device)
+    want = torch.empty(8, dtype=torch.float64, device=a.device)
+    E.check(E.reactive_stats_async("D3Q7", "float", a, b, 256, 256, 256, 0.02, part, nbytes, want))
+    got = torch.full((8,), float("nan"), dtype=torch.float64, device=a.device)
+    rc = _noalloc()(E.LATTICES["D3Q7"], E.REALS["float"], a.data_ptr(), b.data_ptr(), 256, 256, 256, 0.02,
+                    got.data_ptr(), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    for name, g, w in zip(E.STATS_FIELDS, got.cpu().tolist(), want.cpu().tolist()):
+        assert abs(g - w) <= 1e-12 * max(abs(w), 1e-6), name
+
+
+def test_noalloc_rejects_domains_beyond_its_array():
+    # ceil(129 / 128) * 256 * 257 = 131584 row segments > 131072. Real, disjoint
+    # fields of the declared size: the scratch-taking entry accepts them, so the
+    # only reason left to reject the call is the array's capacity.
+    nx, ny, nz = 129, 256, 257
+    a, b = _fields("D3Q7", nx, ny, nz, seed=84)
+    nbytes = E.stats_partials_bytes("D3Q19", nx, ny, nz)
+    assert nbytes == 131584 * 5 * 8
+    part = torch.empty(nbytes // 8, dtype=torch.float64, device=a.device)
+    out = torch.empty(8, dtype=torch.float64, device=a.device)
+    E.check(E.reactive_stats_async("D3Q7", "float", a, b, nx, ny, nz, 0.02, part, nbytes, out))
+    rc = _noalloc()(E.LATTICES["D3Q7"], E.REALS["float"], a.data_ptr(), b.data_ptr(), nx, ny, nz, 0.02,
+                    out.data_ptr(), None)
     assert rc == E.cudaErrorInvalidValue
