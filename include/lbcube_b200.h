@@ -308,18 +308,30 @@ int lbm_reactive_stats_async(int scalar_lattice, int precision, const void* curr
  *              for |v| = 2^(E-6) (1 + m/4096) - 2^-6: uniform 2^-18 grid near
  *              zero, 13-bit relative precision above ~1/64, |v| < 3.98,
  *              saturating
- *   LBM_Q15S   16-bit two's-complement fixed point (code = round(v)),
- *              S = 32768: uniform 2^-15 grid over |f/w - rho0| < 1,
- *              saturating (NaN gives 0)
- * Half the bytes of FP32 storage; collision in FP32 registers (BGK and TRT on
- * the deviations v, MRT and RLBM on the decoded f with the FP32 operator
- * code). Buffers are uint16 [Q, Z, Y, X]; x_extent must be a multiple of 4
- * and buffers 8-byte aligned (else cudaErrorInvalidValue). rho0 is the
- * reference density of the shift.
+ *   LBM_Q15S   16-bit fixed point, v rounded to an integer, S = 32768:
+ *              uniform 2^-15 grid over |f/w - rho0| < 1; stored offset
+ *              binary (code = round(v) + 32768), saturating (NaN gives the
+ *              lower bound)
+ * Half the bytes of FP32 storage; collision in FP32 registers (BGK, TRT and
+ * D2Q9 / D3Q19 MRT on the deviations v, D3Q27 MRT and RLBM on the decoded f
+ * with the FP32 operator code). Buffers are uint16 [Q, Z, Y, X]; x_extent
+ * must be a multiple of 4 and buffers 8-byte aligned (else
+ * cudaErrorInvalidValue). rho0 is the reference density of the shift. With
+ * x_extent a multiple of 8 (at most 1024) and 16-byte aligned buffers, the
+ * D2Q9 / D3Q19 BGK, TRT and MRT steps stage each row's source rows in shared
+ * memory with bulk copies (see lbm_stage_timeouts).
  * ------------------------------------------------------------------------- */
 int lbm_step_shifted_async(int lattice, int format, int collision,
     const void* current_populations, void* next_populations, size_t x_extent,
     size_t y_extent, size_t z_extent, float omega, float rho0, void* stream);
+
+/* Blocks of the row-staged 16-bit step (no reference counterpart) that gave
+ * up waiting for a shared-memory row copy, since the count was last reset, on
+ * the current device; every wait in that kernel is bounded, so a copy that
+ * never lands ends the launch with this count raised instead of hanging it.
+ * `reset` non-zero clears the count. Synchronous; returns 0xFFFFFFFF if the
+ * count cannot be read. */
+unsigned int lbm_stage_timeouts(int reset);
 
 /* FP32/FP64 populations (`precision`) -> shifted 16-bit form, any lattice
  * (fluid or scalar; scalars shift by w_i * rho0 with rho0 a reference
@@ -399,10 +411,13 @@ int lbm_reactive_gradient_async(int fluid_lattice, int precision, int storage, f
  * a fixed array inside the library (5 MiB, reserved on every GPU that loads
  * the library until the process exits) instead of caller scratch. Limit:
  * ceil(x_extent / 128) * y_extent * z_extent <= LBM_STATS_NOALLOC_MAX_BLOCKS
- * (e.g. 256^3 or 1024^2); larger domains return cudaErrorInvalidValue. The
- * first call on a device looks up the array's device address for that device
- * (make it before any stream capture). All calls share the array: calls that
- * overlap on the GPU (other streams, other threads) race, so serialise them. */
+ * (e.g. 256^3 or 1024^2); larger domains return cudaErrorInvalidValue. Each
+ * call looks up the array's address in the calling thread's current CUDA
+ * context (host-side; the address belongs to the context, so contexts the host
+ * creates or switches itself, and device resets, are handled). The first call
+ * in a context may load the library's device code into it: make it before any
+ * stream capture. All calls in a context share the array: calls that overlap
+ * on the GPU (other streams, other threads) race, so serialise them. */
 #define LBM_STATS_NOALLOC_MAX_BLOCKS 131072
 int lbm_reactive_stats_noalloc_async(int scalar_lattice, int precision, const void* current_a,
     const void* current_b, size_t x_extent, size_t y_extent, size_t z_extent, double k_react,

@@ -66,7 +66,8 @@ def _stale(target, deps):
 
 def _compile(src, verbose):
     obj = _obj(src)
-    cmd = [NVCC, *COMMON, *ARCH, *UNITS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
+    extra = os.environ.get("LBCUBE_NVCC_FLAGS", "").split()  # e.g. -D overrides of tuning constants
+    cmd = [NVCC, *COMMON, *ARCH, *UNITS.get(src, []), *extra, "-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)

@@ -13,18 +13,25 @@
 
 #include "collide.cuh"
 #include "common.cuh"
+#include "stream_staged.cuh"
 #include "stream_vec.cuh"
 #include "../../include/lbcube_b200.h"
 
 namespace lbcube {
 
-// Cells per thread of the 16-bit kernels: four (8-byte words), except two
-// (4-byte words) for E3M12, whose software codec makes the step arithmetic-
-// bound. D3Q19 at 256^3, fraction of the copy bandwidth at 4 / 2 cells: F16
-// TRT 0.83 / 0.58, MRT 0.74 / 0.66, Q15 TRT 0.74 / 0.52, BF16 TRT 0.79 / 0.57,
-// E3M12 TRT 0.25 / 0.31.
+// Cells per thread of the 16-bit kernels: four (8-byte words of codes).
+#ifndef LBCUBE_SHIFTED_CELLS
+#define LBCUBE_SHIFTED_CELLS 4
+#endif
 template <int FMT>
-constexpr int kShiftedCells = FMT == kE3M12S ? 2 : 4;
+constexpr int kShiftedCells = LBCUBE_SHIFTED_CELLS;
+
+// The plain step on the deviation-collision formats goes through the
+// row-staged kernel (stream_staged.cuh) wherever its requirements hold.
+#ifndef LBCUBE_SHIFTED_STAGED
+#define LBCUBE_SHIFTED_STAGED 1
+#endif
+constexpr bool kShiftedStaged = LBCUBE_SHIFTED_STAGED != 0;
 
 // BGK, TRT and the D2Q9 / D3Q19 MRT collide on the stored deviations; D3Q27
 // MRT and RLBM decode to f and run the reference operator.
@@ -51,6 +58,12 @@ cudaError_t launch_shifted_step(const void* cur, void* nxt, size_t nx, size_t ny
     return cudaErrorInvalidValue;
   if (!vec_eligible<S>(g, cur, nxt)) return cudaErrorInvalidValue;  // nx % V, word alignment
   const float omega_minus = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
+  if constexpr (kShiftedStaged && S::kBudgeted && S::V == 4 && L::Q <= 19) {
+    if (staged_eligible<L>(g, cur, nxt))
+      return launch_staged_step<L, S, CT>(g, stream, static_cast<const unsigned short*>(cur),
+                                          static_cast<unsigned short*>(nxt), omega, omega_minus,
+                                          typename S::Params{rho0});
+  }
   const VecGrid vg = make_vec_grid(g, S::V);
   launch_vec_step<L, S, CT>(vg, vec_grid_dims(vg), vec_block_threads(vg), stream,
                             static_cast<const unsigned short*>(cur),
@@ -213,6 +226,16 @@ extern "C" int lbm_step_shifted_async(int lattice, int format, int collision,
                                           next_populations, x_extent, y_extent, z_extent, omega,
                                           rho0, s);
   return (int)cudaErrorInvalidValue;
+}
+
+extern "C" unsigned int lbm_stage_timeouts(int reset) {
+  unsigned int n = 0;
+  if (cudaMemcpyFromSymbol(&n, g_stage_timeouts, sizeof(n)) != cudaSuccess) return ~0u;
+  if (reset) {
+    const unsigned int zero = 0;
+    if (cudaMemcpyToSymbol(g_stage_timeouts, &zero, sizeof(zero)) != cudaSuccess) return ~0u;
+  }
+  return n;
 }
 
 extern "C" int lbm_encode_shifted_async(int lattice, int format, int precision,

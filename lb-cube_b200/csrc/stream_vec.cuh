@@ -48,6 +48,7 @@ struct NativeStorage {
   using elem = Real;
   using compute = Real;
   static constexpr int V = VEC;
+  static constexpr bool kBudgeted = false;
   struct Params {};
   template <class L, int i>
   __device__ __forceinline__ static compute decode(elem v, const Params&) { return v; }
@@ -86,6 +87,7 @@ struct ShiftedStorage {
   using elem = unsigned short;
   using compute = float;
   static constexpr int V = VEC;  // cells per thread, decoded to FP32 in registers
+  static constexpr bool kBudgeted = false;
   struct Params {
     float rho0;
   };
@@ -127,6 +129,7 @@ struct DevStorage {
   using elem = unsigned short;
   using compute = float;
   static constexpr int V = VEC;
+  static constexpr bool kBudgeted = true;
   struct Params {
     float rho0;
   };
@@ -160,6 +163,10 @@ struct DevStorage {
     RowWord<elem, V> w;
     memcpy(&w, u, sizeof(u));
     return w;
+  }
+  __device__ __forceinline__ static float2 decode_pair(unsigned int w) { return Codec<FMT>::decode2(w); }
+  __device__ __forceinline__ static unsigned int encode_pair(float a, float b) {
+    return Codec<FMT>::encode2(a, b);
   }
   template <class L, int CT>
   __device__ __forceinline__ static void collide_cell(compute (&v)[L::Q], compute omega,
@@ -389,18 +396,42 @@ __global__ void __launch_bounds__(kThreads)
   fluid_step_vec_body<L, S, CT, DIAG, SLAB>(cur, nxt, vg, omega, omega_minus, p, partials, slab);
 }
 
+// The plain step on 16-bit storage with a register budget: at least
+// kShiftedMinBlocks blocks of kThreads per SM. Four cells of 19 populations per
+// thread leave the compiler free to interleave the cells' collisions up to
+// 128 registers (4 blocks per SM), which an issue-bound kernel pays for in
+// latency it cannot hide.
+#ifndef LBCUBE_SHIFTED_MIN_BLOCKS
+#define LBCUBE_SHIFTED_MIN_BLOCKS 5
+#endif
+constexpr int kShiftedMinBlocks = LBCUBE_SHIFTED_MIN_BLOCKS;
+
+template <class L, class S, int CT>
+__global__ void __launch_bounds__(kThreads, kShiftedMinBlocks)
+    fluid_step_vec16_kernel(const typename S::elem* __restrict__ cur,
+                            typename S::elem* __restrict__ nxt, VecGrid vg,
+                            typename S::compute omega, typename S::compute omega_minus,
+                            typename S::Params p) {
+  fluid_step_vec_body<L, S, CT, false, false>(cur, nxt, vg, omega, omega_minus, p, nullptr, {});
+}
+
 // Launches the plain vectorised step. (Register budgets, i.e. launch bounds
 // with a minimum block count, were timed at 4..8 blocks per SM for every
-// lattice, precision and operator; where they won, for FP32 D3Q19 MRT and
-// RLBM, the one-cell kernel (step_cell.cuh) won by more and now runs those.
-// An explicit count of 1 is not the compiler's default: it lets the
-// allocation grow, e.g. 64 -> 94 registers for the FP32 D3Q19 TRT step.)
+// lattice, precision and operator of the native storage; where they won, for
+// FP32 D3Q19 MRT and RLBM, the one-cell kernel (step_cell.cuh) won by more and
+// now runs those. An explicit count of 1 is not the compiler's default: it
+// lets the allocation grow, e.g. 64 -> 94 registers for the FP32 D3Q19 TRT
+// step.) 16-bit storage colliding on the deviations runs the budgeted kernel
+// above for D2Q9 and D3Q19 (D3Q27 and the decoded RLBM spill under it).
 template <class L, class S, int CT>
 inline void launch_vec_step(const VecGrid& vg, dim3 grid, unsigned threads, cudaStream_t stream,
                             const typename S::elem* cur, typename S::elem* nxt,
                             typename S::compute omega, typename S::compute omega_minus,
                             const typename S::Params& p) {
-  fluid_step_vec_kernel<L, S, CT><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega, omega_minus, p);
+  if constexpr (S::kBudgeted && L::Q <= 19)
+    fluid_step_vec16_kernel<L, S, CT><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega, omega_minus, p);
+  else
+    fluid_step_vec_kernel<L, S, CT><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega, omega_minus, p);
 }
 
 template <class S>

@@ -132,6 +132,8 @@ def _declare(lib):
     lib.lbm_diagnostics_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
     lib.lbm_ke_gradient_workspace_bytes.restype = C.c_size_t
     lib.lbm_ke_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, _sz, _sz, _sz, C.c_int, C.c_int]
+    lib.lbm_stage_timeouts.restype = C.c_uint
+    lib.lbm_stage_timeouts.argtypes = [C.c_int]
 
 
 def _ptr(buf):
@@ -288,6 +290,12 @@ def step_shifted_async(lattice, fmt, collision, cur, nxt, nx, ny, nz, omega, rho
                                          _ptr(cur), _ptr(nxt), nx, ny, nz, float(omega),
                                          float(rho0), _stream(stream))
 
+
+
+def stage_timeouts(reset: bool = False) -> int:
+    """Blocks of the row-staged 16-bit step that gave up waiting for a row copy
+    (0 in a healthy run); `reset` clears the count."""
+    return int(load().lbm_stage_timeouts(1 if reset else 0))
 
 def encode_shifted_async(lattice, fmt, real, populations, shifted, nx, ny, nz, rho0=1.0,
                          stream=None) -> int:
