@@ -1,10 +1,12 @@
-"""Generates tests/golden/reference_steps.npz from LB-Cube's own CPU path.
+"""Generates the golden fixtures under tests/golden/ from LB-Cube's own CPU path.
 
 Runs the reference build (oracle/_ref/libref.so: the unmodified reference
 headers compiled in place by `make -C oracle ref`) on small seeded states and
 stores inputs and outputs, so the oracle and the engine can be checked against
 the reference where its sources are not available. Regenerate with
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # the small fixtures (a minute)
+    python tests/golden/make_golden.py --c3     # the 1024^2 reactive-mixing run
+                                                # (about an hour on one core)
 """
 import os
 import sys
@@ -14,9 +16,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
 sys.path.insert(0, os.path.join(HERE, ".."))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "lb-cube_b200"))
 
 import _util as U  # noqa: E402
 import oracle as O  # noqa: E402
+import workloads as W  # noqa: E402
 
 SIZES = {"D2Q9": (7, 5, 1), "D3Q19": (6, 5, 4), "D3Q27": (5, 4, 3)}
 OMEGA, OMEGA_C, K, STEPS = 1 / 0.6, 1 / 0.8, 0.07, 3
@@ -73,7 +77,73 @@ def make_vtk_golden():
     np.savez_compressed(os.path.join(HERE, "vtk_inputs.npz"), **inputs)
 
 
+C3_FILE = os.path.join(HERE, "c3_shear1024_mrt.npz")
+
+
+def concentration(g, q):
+    """C = sum of the scalar populations, in ascending order (FP64)."""
+    g = np.asarray(g, np.float64).reshape(q, -1)
+    c = g[0].copy()
+    for i in range(1, q):
+        c += g[i]
+    return c
+
+
+def c3_reactive_mixing(n=1024, steps=20000, every=10, out=C3_FILE):
+    """The reactive-mixing configuration on the reference CPU path: D2Q9 MRT
+    fluid (tau 0.6) on the double shear layer of workloads.reactive_shear_layer
+    and two D2Q5 species reacting A + B -> C (Pe 1000, Da 1, L = n), stepped
+    as src/simulate_reaction.cpp:515-555 steps it (step_cpu, then
+    step_reaction_AB with the post-step fluid), with compute_reactive_stats
+    (lattice_io.hpp:256-338) at step 0 and every `every` steps, as
+    log_reactive_diagnostics records it.
+
+    Stores: the workload's 1-D tables; the statistics rows as the reference
+    computes them (sums in FP32) and the same rows with FP64 sums over the
+    reference's fields; SHA-256 of the final fluid, A and B populations; the
+    final concentrations' FP64 row and column sums and a stride-8 subsample."""
+    import hashlib
+    import time
+
+    w = W.reactive_shear_layer(n)
+    omega, omega_c, k = 1.0 / w["tau"], 1.0 / w["tau_c"], w["k"]
+    f = O.init_equilibrium("D2Q9", w["rho"], w["u"], n, n, 1, np.float32)
+    a = O.init_equilibrium("D2Q5", w["a0"], w["u"], n, n, 1, np.float32)
+    b = O.init_equilibrium("D2Q5", w["b0"], w["u"], n, n, 1, np.float32)
+    init_sha = hashlib.sha256(f.tobytes() + a.tobytes() + b.tobytes()).hexdigest()
+
+    def stats_rows(a_, b_):
+        return (O.reactive_stats(a_, b_, "D2Q5", n, n, 1, k, lib=O.REF),
+                O.reactive_stats(a_, b_, "D2Q5", n, n, 1, k, accumulate_f64=True))
+
+    r32, r64 = stats_rows(a, b)
+    rows_ref, rows_f64 = [r32], [r64]
+    t0 = time.time()
+    for s in range(steps // every):
+        f, a, b = O.coupled_reaction(f, a, b, "D2Q9", "MRT", n, n, 1, omega, omega_c, k, steps=every,
+                                     lib=O.REF)
+        r32, r64 = stats_rows(a, b)
+        rows_ref.append(r32)
+        rows_f64.append(r64)
+        if (s + 1) % 100 == 0:
+            print(f"C3: step {(s + 1) * every} of {steps}, {time.time() - t0:.0f} s", flush=True)
+    ca, cb = concentration(a, 5).reshape(n, n), concentration(b, 5).reshape(n, n)
+    np.savez_compressed(
+        out, n=n, steps=steps, every=every, tau=w["tau"], tau_c=w["tau_c"], k=k, seed=W.SHEAR_SEED,
+        ux_row=w["tables"]["ux_row"], cos_col=w["tables"]["cos_col"], init_sha256=init_sha,
+        stats_reference=np.array(rows_ref), stats_f64=np.array(rows_f64),
+        fluid_sha256=hashlib.sha256(f.tobytes()).hexdigest(),
+        a_sha256=hashlib.sha256(a.tobytes()).hexdigest(), b_sha256=hashlib.sha256(b.tobytes()).hexdigest(),
+        ca_rows=ca.sum(axis=1), ca_cols=ca.sum(axis=0), cb_rows=cb.sum(axis=1), cb_cols=cb.sum(axis=0),
+        ca_sub=ca[::8, ::8].astype(np.float32), cb_sub=cb[::8, ::8].astype(np.float32),
+        ca_l2=np.linalg.norm(ca), cb_l2=np.linalg.norm(cb))
+    print(f"wrote {out}: {len(rows_ref)} statistics rows in {time.time() - t0:.0f} s")
+
+
 def main():
+    if "--c3" in sys.argv:
+        steps = int(sys.argv[sys.argv.index("--c3") + 1]) if len(sys.argv) > sys.argv.index("--c3") + 1 else 20000
+        return c3_reactive_mixing(steps=steps)
     if not O.REF.available:
         raise SystemExit("reference build oracle/_ref/libref.so missing: run make -C oracle ref")
     out = {}
