@@ -310,11 +310,14 @@ int lbm_reactive_stats_async(int scalar_lattice, int precision, const void* curr
  *              saturating
  *   LBM_Q15S   16-bit fixed point, v rounded to an integer, S = 32768:
  *              uniform 2^-15 grid over |f/w - rho0| < 1; stored offset
- *              binary (code = round(v) + 32768), saturating (NaN gives the
- *              lower bound)
+ *              binary (code = round(v) + 32768), saturating (NaN to one
+ *              of the bounds)
  * Half the bytes of FP32 storage; collision in FP32 registers (BGK, TRT and
  * D2Q9 / D3Q19 MRT on the deviations v, D3Q27 MRT and RLBM on the decoded f
- * with the FP32 operator code). Buffers are uint16 [Q, Z, Y, X]; x_extent
+ * with the FP32 operator code). Where the step collides on the deviations it
+ * rounds FP16 and BF16 stochastically (unbiased; the random bits come from
+ * the values themselves, so the step is deterministic); conversions and the
+ * other paths round to nearest. Buffers are uint16 [Q, Z, Y, X]; x_extent
  * must be a multiple of 4 and buffers 8-byte aligned (else
  * cudaErrorInvalidValue). rho0 is the reference density of the shift. With
  * x_extent a multiple of 8 (at most 1024) and 16-byte aligned buffers, the

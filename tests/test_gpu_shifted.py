@@ -7,17 +7,19 @@
   deviations; the FP32 path works on f ~ w and carries a few FP32 ulps of 1 of
   absolute error in f/w after cancelling rho0, more for D3Q27's 1/216 weights
   and 27-term MRT sums), so every value is within one 16-bit step plus 2e-6
-  of the other and at least 95 % of the codes agree;
+  of the other; with nearest rounding at least 95 % of the codes agree, and
+  where FP16 / BF16 round stochastically every value is one of the two 16-bit
+  neighbours of the FP32 result with an average signed error of 0;
 * Q15 covers |f/w - rho0| < 1 only, so its round trip uses a state inside
   that range (|u| ~ 0.03) and out-of-range values saturate;
 * 2000 steps of the D3Q19 256^3 Taylor-Green + noise case (tau 0.55): the
   velocity rel-L2 against the FP64 run (the FP64 kernel is bit-identical to
-  the reference CPU path, tests/test_gpu_parity.py). Bars: E3M12 <= 1e-3 for
-  TRT and MRT; IEEE FP16 <= 1e-3 for MRT and <= 3e-3 for TRT (1.9e-3 measured:
-  TRT's odd modes relax at omega- ~ 0.18 at tau 0.55 and keep the rounding
-  noise); Q15 <= 1e-3 for TRT and <= 3e-3 for MRT (2.6e-4 and 1.4e-3
-  measured); BF16 <= 0.15 (8-bit significand: ~8e-2 measured, not usable at
-  this tolerance).
+  the reference CPU path, tests/test_gpu_parity.py), held to the 1e-3 target
+  for every format that meets it: E3M12 (1.0e-4 / 8.4e-5 measured), IEEE FP16
+  with stochastic rounding (3.7e-4 TRT, 3.5e-4 MRT; 1.96e-3 TRT with nearest
+  rounding, whose correlated errors TRT's slowly relaxed odd modes keep) and
+  Q15 for TRT (2.6e-4); Q15 MRT <= 3e-3 (1.45e-3 measured); BF16 <= 0.15
+  (8-bit significand).
 """
 import math
 
@@ -34,7 +36,7 @@ FMTS = ("f16s", "bf16s", "e3m12s", "q15s")
 ULP = {"f16s": 2.0 ** -10, "bf16s": 2.0 ** -7, "e3m12s": 2.0 ** -12, "q15s": 0.0}  # relative spacing
 ABS_FLOOR = {"f16s": 0.0, "bf16s": 0.0, "e3m12s": 2.0 ** -18, "q15s": 2.0 ** -16}  # half the uniform grid
 BARS = {("e3m12s", "TRT"): 1e-3, ("e3m12s", "MRT"): 1e-3, ("f16s", "MRT"): 1e-3,
-        ("f16s", "TRT"): 3e-3, ("bf16s", "TRT"): 0.15, ("bf16s", "MRT"): 0.15,
+        ("f16s", "TRT"): 1e-3, ("bf16s", "TRT"): 0.15, ("bf16s", "MRT"): 0.15,
         ("q15s", "TRT"): 1e-3, ("q15s", "MRT"): 3e-3}
 
 
@@ -122,7 +124,24 @@ def test_shifted_step_is_rounded_fp32_step(engine, dev, fmt, lat, op):
     dv = (got_f.double() - want_f.double()).abs() / w
     step = ULP[fmt] * (want_f.double() / w - 1.0).abs() * 2 + 2 * ABS_FLOOR[fmt] + 2e-6
     assert bool((dv <= step).all()), float((dv - step).max())
-    assert float((h1 == want).double().mean()) >= 0.95
+    if _stochastic(fmt, lat, op):
+        # each value one of the two 16-bit neighbours of the FP32 result, and
+        # no bias: the signed error, in units of the local spacing, averages 0.
+        # Checked where the spacing is 10x the FP32 paths' 2e-6 disagreement.
+        exact = f1.double() / w - 1.0
+        spacing = ULP[fmt] * torch.exp2(torch.floor(torch.log2(exact.abs().clamp_min(1e-30))))
+        e = ((got_f.double() / w - 1.0 - exact) / spacing)[spacing >= 2e-5]
+        assert e.numel() >= 500
+        assert float(e.abs().max()) <= 1.2
+        assert abs(float(e.mean())) <= 0.05, float(e.mean())
+    else:
+        assert float((h1 == want).double().mean()) >= 0.95
+
+
+def _stochastic(fmt, lat, op):
+    """The step rounds FP16 / BF16 stochastically wherever it collides on the
+    deviations (BGK, TRT; MRT on D2Q9 / D3Q19)."""
+    return fmt in ("f16s", "bf16s") and (op in ("BGK", "TRT") or (op == "MRT" and lat != "D3Q27"))
 
 
 def test_shifted_rejects_unaligned_extent(engine, dev):
