@@ -903,12 +903,12 @@ def _reference_lib():
     return O, O.ORACLE, "port"
 
 
-def cpu_sample(nz_sample, steps):
-    """Time `steps` serial step_cpu<D3Q19, float, TRT> calls on a 256 x 256 x
-    nz_sample periodic slab of the benchmark state (same per-cell work)."""
+def workload_slab(O, nz_sample):
+    """FP32 equilibrium populations of planes 0 .. nz_sample-1 of the benchmark
+    field (Taylor-Green u0 = 0.05 with wavenumber 2 pi / 256 in each axis plus
+    seeded N(0, 1e-3) velocity noise, rho = 1), as a periodic slab."""
     import numpy as np
 
-    O, lib, kind = _reference_lib()
     n = NX * NY * nz_sample
     rng = np.random.default_rng(SEED)
     k = 2 * math.pi / NX
@@ -916,7 +916,15 @@ def cpu_sample(nz_sample, steps):
     z, y, x = np.meshgrid(np.arange(nz_sample) * k, ax, ax, indexing="ij")
     u = np.stack([U0 * np.sin(x) * np.cos(y) * np.cos(z), -U0 * np.cos(x) * np.sin(y) * np.cos(z),
                   np.zeros_like(x)]).reshape(3, -1) + NOISE * rng.standard_normal((3, n))
-    f = O.init_equilibrium("D3Q19", np.ones(n), u, NX, NY, nz_sample, np.float32)
+    return O.init_equilibrium("D3Q19", np.ones(n), u, NX, NY, nz_sample, np.float32)
+
+
+def cpu_sample(nz_sample, steps):
+    """Time `steps` serial step_cpu<D3Q19, float, TRT> calls on a 256 x 256 x
+    nz_sample periodic slab of the benchmark state (same per-cell work)."""
+    O, lib, kind = _reference_lib()
+    n = NX * NY * nz_sample
+    f = workload_slab(O, nz_sample)
     t = time.perf_counter()
     O.step(f, "D3Q19", "TRT", NX, NY, nz_sample, 1 / TAU, steps=steps, lib=lib)
     dt = time.perf_counter() - t
@@ -938,12 +946,8 @@ def run_reference(args):
     total = max(1, args.steps + args.warmup)
     nz_s = int(max(1, min(64, budget_s * rate * 1e6 / total / (NX * NY))))
     O, lib, kind = _reference_lib()
-    import numpy as np
-
     n = NX * NY * nz_s
-    rng = np.random.default_rng(SEED)
-    u = 0.05 * rng.standard_normal((3, n))
-    f = O.init_equilibrium("D3Q19", np.ones(n), u, NX, NY, nz_s, np.float32)
+    f = workload_slab(O, nz_s)
     for _ in range(args.warmup):
         f = O.step(f, "D3Q19", "TRT", NX, NY, nz_s, 1 / TAU, steps=1, lib=lib)
     t = time.perf_counter()
@@ -951,12 +955,13 @@ def run_reference(args):
         f = O.step(f, "D3Q19", "TRT", NX, NY, nz_s, 1 / TAU, steps=1, lib=lib)
     dt = time.perf_counter() - t
     value = n * args.steps / dt / 1e6
-    sample = (f"each step: step_cpu<D3Q19,float,TRT> on a 256x256x{nz_s} periodic slab of the "
-              f"256^3 workload (serial reference CPU path, 1 thread of {os.cpu_count()})")
+    sample = (f"each step: step_cpu<D3Q19,float,TRT> on planes 0..{nz_s - 1} of the 256^3 workload field as "
+              f"a 256x256x{nz_s} periodic slab (serial reference CPU path, 1 thread of {os.cpu_count()})")
     return {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": config_dict(), "impl": "reference",
+            "data": "synthetic", "config": dict(config_dict(), slab=f"{NX}x{NY}x{nz_s} (planes 0..{nz_s - 1})"),
+            "impl": "reference",
             "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": 1, "kind": kind,
                              "sample": sample},
             "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0,

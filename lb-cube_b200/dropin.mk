@@ -5,9 +5,10 @@
 # is installed here; a user with real Eigen drops SHIM.
 #
 #   make -f lb-cube_b200/dropin.mk REF=/path/to/LB-Cube
-REF     ?= /root/reference
-CUDA    ?= /usr/local/cuda
+# (default: a checkout named reference next to this repository)
 HERE    := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
+REF     ?= $(abspath $(HERE)../../reference)
+CUDA    ?= /usr/local/cuda
 OUT     := $(HERE)_build/dropin
 SHIM    := -I$(HERE)../oracle/shim
 CXXFLAGS := -std=c++23 -O2 -ffp-contract=off -w -DLB_CUBE_ENABLE_CUDA=1 \

@@ -7,7 +7,8 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference"
+# LB-Cube's source tree: LBCUBE_REFERENCE, else a checkout next to this repository
+REF = os.environ.get("LBCUBE_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "src", "main.cpp")), reason="reference sources absent")
