@@ -407,6 +407,19 @@ int lbm_reactive_gradient_async(int fluid_lattice, int precision, int storage, f
     double k_react, int steps, int checkpoint_interval, void* workspace, size_t workspace_bytes,
     double* result, void* grad_a0, void* grad_b0, void* grad_u0, void* stream);
 
+/* Statistics of a domain split across ranks (no reference counterpart): each
+ * rank reduces its partials (from a statistics launch over its cells) to the
+ * five FP64 sums of C_A, C_B, C_A^2, C_B^2, C_A C_B (device, 5 doubles); the
+ * ranks add their sums (an all-reduce of five doubles); then
+ * lbm_reactive_stats_from_sums_async forms the 8 diagnostics of the totals
+ * over `cells` cells (k_react in `precision`, as compute_reactive_stats takes
+ * it). On one rank the two calls give the bits of
+ * lbm_reactive_stats_finalize_async. */
+int lbm_reactive_stats_sums_async(int fluid_lattice, size_t x_extent, size_t y_extent,
+    size_t z_extent, const double* partials, size_t partials_bytes, double* sums, void* stream);
+int lbm_reactive_stats_from_sums_async(int precision, const double* sums, double cells,
+    double k_react, double* diagnostics, void* stream);
+
 /* Allocation-free form of lbm_reactive_stats_async. No counterpart in the
  * reference. For callers that cannot allocate device memory, e.g. a plugin or
  * FFI binding inside an application that owns every device allocation and
@@ -495,6 +508,30 @@ int lbm_step_slab_async(int lattice, int precision, int collision,
     void* send_hi, size_t z_begin, size_t z_end, void* stream);
 int lbm_slab_pack_async(int lattice, int precision, const void* populations, size_t x_extent,
     size_t y_extent, size_t z_extent, void* send_lo, void* send_hi, void* stream);
+
+/* The coupled fluid + A + B -> C step of lbm_fluid_reaction_ab_async on a
+ * z-slab (D3Q19 or D3Q27 fluid with two D3Q7 species). One face buffer per
+ * side of lbm_fluid_reaction_slab_face_elems() elements: the fluid's crossing
+ * populations as for lbm_step_slab_async, then species A's and then B's (one
+ * [Y, X] plane each: c_z = +1 in send_hi / halo_lo, c_z = -1 in send_lo /
+ * halo_hi). All four face buffers are required for every plane range. With
+ * stats_partials non-null the launch writes the statistics partials of its
+ * planes' new scalar fields at their places in a buffer of
+ * lbm_stats_partials_bytes(fluid_lattice, x, y, z_extent) bytes, so a step
+ * split into several plane ranges fills it once; lbm_reactive_stats_sums_async
+ * then gives the rank's five sums. A box stepped as slabs is bit-identical to
+ * the box stepped whole. lbm_fluid_reaction_slab_pack_async fills the send
+ * buffers from a state (before the first exchange). */
+size_t lbm_fluid_reaction_slab_face_elems(int fluid_lattice, size_t x_extent, size_t y_extent);
+int lbm_fluid_reaction_slab_async(int fluid_lattice, int precision, int collision,
+    const void* current_fluid, void* next_fluid, const void* current_a, void* next_a,
+    const void* current_b, void* next_b, size_t x_extent, size_t y_extent, size_t z_extent,
+    double omega, double omega_c, double k_react, const void* halo_lo, const void* halo_hi,
+    void* send_lo, void* send_hi, size_t z_begin, size_t z_end, double* stats_partials,
+    size_t stats_partials_bytes, void* stream);
+int lbm_fluid_reaction_slab_pack_async(int fluid_lattice, int precision, const void* fluid,
+    const void* a, const void* b, size_t x_extent, size_t y_extent, size_t z_extent,
+    void* send_lo, void* send_hi, void* stream);
 
 /* ---- output ----------------------------------------------------------------
  * Macroscopic fields for output, computed on the device from the populations

@@ -6,6 +6,8 @@
 //                       the reaction driver sequences them
 //                       (src/simulate_reaction.cpp:518-543), optionally with
 //                       the reactive-statistics partial sums of the new fields.
+#include <algorithm>
+
 #include "adr.cuh"
 #include "cells.cuh"
 #include "collide.cuh"
@@ -97,6 +99,223 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   if constexpr (STATS) block_sum_to<kStatSums>(sums, partials + block_linear() * kStatSums);
+}
+
+// ---- z-slab form of the coupled step ----------------------------------------
+// A rank owns planes [0, nz) of a box cut along z (see slab.cu for the fluid
+// alone). One face buffer per side holds, per crossing population in
+// ascending i, an ny x nx plane: first the fluid's (5 of 19 for D3Q19, 9 of
+// 27 for D3Q27), then species A's and B's (1 of 7 each for D3Q7). Populations
+// with c_z = +1 at plane 0 are pulled from halo_lo (the lower neighbour's
+// top-plane sends), c_z = -1 at plane nz - 1 from halo_hi; the populations
+// leaving through a face are also stored into send_lo / send_hi. Every cell
+// does the arithmetic of fluid_reaction_kernel, so a box stepped as slabs is
+// bit-identical to the box stepped whole.
+template <class L>
+__host__ __device__ constexpr int face_planes() {
+  return zcount_of<L>();
+}
+template <class FL>
+__host__ __device__ constexpr int coupled_face_planes() {
+  using SL = typename ScalarOf<FL>::type;
+  return face_planes<FL>() + 2 * face_planes<SL>();
+}
+
+// Pull-gather with the slab's halos in place of the periodic z wrap.
+template <class L, class Real>
+__device__ __forceinline__ void gather_slab(const Real* __restrict__ cur, const Grid& g,
+                                            const Neighbours& n, int x, int y, int z,
+                                            const Real* __restrict__ halo_lo,
+                                            const Real* __restrict__ halo_hi, Real (&f)[L::Q]) {
+  const size_t plane = (size_t)g.plane;
+  const size_t n2 = (size_t)g.ny * g.nx;
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    const int sx = cx == 0 ? x : (cx > 0 ? n.xm : n.xp);
+    const int sy = cy == 0 ? y : (cy > 0 ? n.ym : n.yp);
+    const size_t row = (size_t)sy * g.nx + sx;
+    if constexpr (cz > 0) {
+      f[i] = z == 0 ? __ldg(halo_lo + zslot_of<L>(i) * n2 + row)
+                    : __ldg(cur + plane * i + (size_t)(z - 1) * n2 + row);
+    } else if constexpr (cz < 0) {
+      f[i] = z == g.nz - 1 ? __ldg(halo_hi + zslot_of<L>(i) * n2 + row)
+                           : __ldg(cur + plane * i + (size_t)(z + 1) * n2 + row);
+    } else {
+      f[i] = __ldg(cur + plane * i + (size_t)z * n2 + row);
+    }
+  });
+}
+
+// Stores the populations of a face cell that leave the slab.
+template <class L, class Real>
+__device__ __forceinline__ void send_slab(const Grid& g, int x, int y, int z, const Real (&f)[L::Q],
+                                          Real* __restrict__ send_lo, Real* __restrict__ send_hi) {
+  const size_t n2 = (size_t)g.ny * g.nx;
+  const size_t row = (size_t)y * g.nx + x;
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr int cz = L::c[i][2];
+    if constexpr (cz > 0) {
+      if (z == g.nz - 1) send_hi[zslot_of<L>(i) * n2 + row] = f[i];
+    } else if constexpr (cz < 0) {
+      if (z == 0) send_lo[zslot_of<L>(i) * n2 + row] = f[i];
+    }
+  });
+}
+
+// Launch over planes [g.z0, g.z0 + gridDim.y); statistics partials indexed by
+// the absolute plane, so a step split into several plane ranges writes every
+// block's partial once.
+template <class FL, class Real, int CT, bool STATS>
+__global__ void __launch_bounds__(kThreads)
+    fluid_reaction_slab_kernel(const Real* __restrict__ cur_f, Real* __restrict__ nxt_f,
+                               const Real* __restrict__ cur_a, Real* __restrict__ nxt_a,
+                               const Real* __restrict__ cur_b, Real* __restrict__ nxt_b, Grid g,
+                               Real omega, Real omega_minus, Real omega_c, Real k,
+                               const Real* __restrict__ halo_lo, const Real* __restrict__ halo_hi,
+                               Real* __restrict__ send_lo, Real* __restrict__ send_hi,
+                               double* __restrict__ partials) {
+  using SL = typename ScalarOf<FL>::type;
+  const size_t n2 = (size_t)g.ny * g.nx;
+  const size_t a_off = (size_t)face_planes<FL>() * n2;
+  const size_t b_off = a_off + (size_t)face_planes<SL>() * n2;
+  int x, y, z;
+  const bool active = cell_of(g, x, y, z);
+  double sums[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (active) {
+    const int cell = (z * g.ny + y) * g.nx + x;
+    const Neighbours n = neighbours(g, x, y, z);
+    Real f[FL::Q], u[FL::D];
+    gather_slab<FL>(cur_f, g, n, x, y, z, halo_lo, halo_hi, f);
+    collide<FL, Real, CT>(f, omega, omega_minus);
+    store_cell<FL>(nxt_f, g, cell, f);
+    send_slab<FL>(g, x, y, z, f, send_lo, send_hi);
+    fluid_velocity<FL>(f, u);
+    Real a[SL::Q], b[SL::Q];
+    gather_slab<SL>(cur_a, g, n, x, y, z, halo_lo + a_off, halo_hi + a_off, a);
+    gather_slab<SL>(cur_b, g, n, x, y, z, halo_lo + b_off, halo_hi + b_off, b);
+    react_pair<SL>(a, b, u, omega_c, k);
+    store_cell<SL>(nxt_a, g, cell, a);
+    store_cell<SL>(nxt_b, g, cell, b);
+    send_slab<SL>(g, x, y, z, a, send_lo + a_off, send_hi + a_off);
+    send_slab<SL>(g, x, y, z, b, send_lo + b_off, send_hi + b_off);
+    if constexpr (STATS) {
+      const double ca = (double)concentration<SL>(a);
+      const double cb = (double)concentration<SL>(b);
+      sums[0] = ca;
+      sums[1] = cb;
+      sums[2] = ca * ca;
+      sums[3] = cb * cb;
+      sums[4] = ca * cb;
+    }
+  }
+  if constexpr (STATS) {
+    const long long blk = ((long long)g.z0 + blockIdx.y) * gridDim.x + blockIdx.x;
+    block_sum_to<kStatSums>(sums, partials + blk * kStatSums);
+  }
+}
+
+// The face populations of a coupled state (fluid, A, B) into the send
+// buffers: the exchange that precedes the first slab step.
+template <class FL, class Real>
+__global__ void __launch_bounds__(256)
+    fluid_reaction_slab_pack_kernel(const Real* __restrict__ f, const Real* __restrict__ a,
+                                    const Real* __restrict__ b, Real* __restrict__ send_lo,
+                                    Real* __restrict__ send_hi, Grid g) {
+  using SL = typename ScalarOf<FL>::type;
+  const size_t n2 = (size_t)g.ny * g.nx;
+  const size_t a_off = (size_t)face_planes<FL>() * n2;
+  const size_t b_off = a_off + (size_t)face_planes<SL>() * n2;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)(2 * n2);
+       e += (long long)gridDim.x * blockDim.x) {
+    const int z = e < (long long)n2 ? 0 : g.nz - 1;
+    const size_t row = (size_t)(e < (long long)n2 ? e : e - (long long)n2);
+    const int y = (int)(row / g.nx), x = (int)(row - (size_t)y * g.nx);
+    const int cell = (z * g.ny + y) * g.nx + x;
+    Real ff[FL::Q], fa[SL::Q], fb[SL::Q];
+    load_cell<FL>(f, g, cell, ff);
+    load_cell<SL>(a, g, cell, fa);
+    load_cell<SL>(b, g, cell, fb);
+    auto send = [&](auto& vals, auto lat, size_t off) {
+      using LL = decltype(lat);
+      static_for<LL::Q>([&](auto I) {
+        constexpr int i = LB_I(I);
+        constexpr int cz = LL::c[i][2];
+        if constexpr (cz > 0) {
+          if (z == g.nz - 1) send_hi[off + zslot_of<LL>(i) * n2 + row] = vals[i];
+        } else if constexpr (cz < 0) {
+          if (z == 0) send_lo[off + zslot_of<LL>(i) * n2 + row] = vals[i];
+        }
+      });
+    };
+    send(ff, FL{}, 0);
+    send(fa, SL{}, a_off);
+    send(fb, SL{}, b_off);
+  }
+}
+
+template <class FL, class Real, int CT>
+cudaError_t launch_fluid_reaction_slab(const Real* cur_f, Real* nxt_f, const Real* cur_a,
+                                       Real* nxt_a, const Real* cur_b, Real* nxt_b, size_t nx,
+                                       size_t ny, size_t nz, Real omega, Real omega_c, Real k,
+                                       const Real* halo_lo, const Real* halo_hi, Real* send_lo,
+                                       Real* send_hi, size_t z_begin, size_t z_end,
+                                       double* partials, size_t partials_bytes,
+                                       cudaStream_t stream) {
+  using SL = typename ScalarOf<FL>::type;
+  Grid g;
+  cudaError_t err = validate_domain(cur_f == nullptr || nxt_f == nullptr || cur_a == nullptr ||
+                                        nxt_a == nullptr || cur_b == nullptr || nxt_b == nullptr ||
+                                        halo_lo == nullptr || halo_hi == nullptr ||
+                                        send_lo == nullptr || send_hi == nullptr,
+                                    1, 1, 1, 3, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  if (z_begin >= z_end || z_end > (size_t)g.nz) return cudaErrorInvalidValue;
+  const size_t sb = (size_t)SL::Q * g.plane * sizeof(Real);
+  const size_t fb = (size_t)FL::Q * g.plane * sizeof(Real);
+  const size_t hb = (size_t)coupled_face_planes<FL>() * g.ny * g.nx * sizeof(Real);
+  const size_t need = (size_t)g.blocks() * kStatSums * sizeof(double);
+  if (partials != nullptr && partials_bytes < need) return cudaErrorInvalidValue;
+  const Span reads[5] = {{cur_f, fb}, {cur_a, sb}, {cur_b, sb}, {halo_lo, hb}, {halo_hi, hb}};
+  const Span writes[6] = {{nxt_f, fb}, {nxt_a, sb}, {nxt_b, sb}, {send_lo, hb}, {send_hi, hb},
+                          {partials, partials != nullptr ? need : 0}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
+  g.z0 = (int)z_begin;
+  dim3 grid = grid_dims(g);
+  grid.y = (unsigned)(z_end - z_begin);
+  if (partials != nullptr)
+    fluid_reaction_slab_kernel<FL, Real, CT, true><<<grid, block_dims(g), 0, stream>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, halo_lo,
+        halo_hi, send_lo, send_hi, partials);
+  else
+    fluid_reaction_slab_kernel<FL, Real, CT, false><<<grid, block_dims(g), 0, stream>>>(
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, halo_lo,
+        halo_hi, send_lo, send_hi, nullptr);
+  return cudaGetLastError();
+}
+
+template <class FL, class Real>
+cudaError_t launch_fluid_reaction_slab_pack(const Real* f, const Real* a, const Real* b, size_t nx,
+                                            size_t ny, size_t nz, Real* send_lo, Real* send_hi,
+                                            cudaStream_t stream) {
+  using SL = typename ScalarOf<FL>::type;
+  Grid g;
+  cudaError_t err = validate_domain(f == nullptr || a == nullptr || b == nullptr ||
+                                        send_lo == nullptr || send_hi == nullptr,
+                                    1, 1, 1, 3, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  const size_t hb = (size_t)coupled_face_planes<FL>() * g.ny * g.nx * sizeof(Real);
+  const Span reads[3] = {{f, (size_t)FL::Q * g.plane * sizeof(Real)},
+                         {a, (size_t)SL::Q * g.plane * sizeof(Real)},
+                         {b, (size_t)SL::Q * g.plane * sizeof(Real)}};
+  const Span writes[2] = {{send_lo, hb}, {send_hi, hb}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  const long long total = 2LL * g.ny * g.nx;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+  fluid_reaction_slab_pack_kernel<FL, Real><<<blocks, 256, 0, stream>>>(f, a, b, send_lo, send_hi, g);
+  return cudaGetLastError();
 }
 
 template <class FL, class Real>
@@ -344,5 +563,65 @@ extern "C" int lbm_fluid_reaction_ab_async(int fluid_lattice, int precision, int
     if (fluid_lattice == LBM_D3Q27) LBCUBE_CASE(D3Q27, double);
   }
 #undef LBCUBE_CASE
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" size_t lbm_fluid_reaction_slab_face_elems(int fluid_lattice, size_t x_extent,
+                                                    size_t y_extent) {
+  if (fluid_lattice == LBM_D3Q19) return (size_t)coupled_face_planes<D3Q19>() * x_extent * y_extent;
+  if (fluid_lattice == LBM_D3Q27) return (size_t)coupled_face_planes<D3Q27>() * x_extent * y_extent;
+  return 0;
+}
+
+extern "C" int lbm_fluid_reaction_slab_async(
+    int fluid_lattice, int precision, int collision, const void* current_fluid, void* next_fluid,
+    const void* current_a, void* next_a, const void* current_b, void* next_b, size_t x_extent,
+    size_t y_extent, size_t z_extent, double omega, double omega_c, double k_react,
+    const void* halo_lo, const void* halo_hi, void* send_lo, void* send_hi, size_t z_begin,
+    size_t z_end, double* stats_partials, size_t stats_partials_bytes, void* stream) {
+  const cudaStream_t s = as_stream(stream);
+#define LBCUBE_SLAB(FL, R, CT)                                                                    \
+  return (int)launch_fluid_reaction_slab<FL, R, CT>(                                             \
+      static_cast<const R*>(current_fluid), static_cast<R*>(next_fluid),                         \
+      static_cast<const R*>(current_a), static_cast<R*>(next_a), static_cast<const R*>(current_b), \
+      static_cast<R*>(next_b), x_extent, y_extent, z_extent, R(omega), R(omega_c), R(k_react),   \
+      static_cast<const R*>(halo_lo), static_cast<const R*>(halo_hi), static_cast<R*>(send_lo),  \
+      static_cast<R*>(send_hi), z_begin, z_end, stats_partials, stats_partials_bytes, s)
+#define LBCUBE_SLAB_OP(FL, R)                       \
+  switch (collision) {                              \
+    case kBGK: LBCUBE_SLAB(FL, R, kBGK);            \
+    case kTRT: LBCUBE_SLAB(FL, R, kTRT);            \
+    case kMRT: LBCUBE_SLAB(FL, R, kMRT);            \
+    default: return (int)cudaErrorInvalidValue;     \
+  }
+  if (precision == LBM_FLOAT) {
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_SLAB_OP(D3Q19, float)
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_SLAB_OP(D3Q27, float)
+  } else if (precision == LBM_DOUBLE) {
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_SLAB_OP(D3Q19, double)
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_SLAB_OP(D3Q27, double)
+  }
+#undef LBCUBE_SLAB_OP
+#undef LBCUBE_SLAB
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int lbm_fluid_reaction_slab_pack_async(int fluid_lattice, int precision,
+                                                  const void* fluid, const void* a, const void* b,
+                                                  size_t x_extent, size_t y_extent, size_t z_extent,
+                                                  void* send_lo, void* send_hi, void* stream) {
+  const cudaStream_t s = as_stream(stream);
+#define LBCUBE_PACK(FL, R)                                                                       \
+  return (int)launch_fluid_reaction_slab_pack<FL, R>(                                           \
+      static_cast<const R*>(fluid), static_cast<const R*>(a), static_cast<const R*>(b), x_extent, \
+      y_extent, z_extent, static_cast<R*>(send_lo), static_cast<R*>(send_hi), s)
+  if (precision == LBM_FLOAT) {
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_PACK(D3Q19, float);
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_PACK(D3Q27, float);
+  } else if (precision == LBM_DOUBLE) {
+    if (fluid_lattice == LBM_D3Q19) LBCUBE_PACK(D3Q19, double);
+    if (fluid_lattice == LBM_D3Q27) LBCUBE_PACK(D3Q27, double);
+  }
+#undef LBCUBE_PACK
   return (int)cudaErrorInvalidValue;
 }

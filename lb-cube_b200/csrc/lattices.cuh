@@ -100,4 +100,20 @@ template <> struct ScalarOf<D3Q27> { using type = D3Q7; };
 
 enum Collision : int { kBGK = 0, kTRT = 1, kMRT = 2, kRLBM = 3 };
 
+// Populations that cross a z face of a slab: zcount_of<L>() of them per face
+// (c_z = +1 and c_z = -1 each); zslot_of<L>(i) is population i's place among
+// those with the same c_z, in ascending i.
+template <class L>
+__host__ __device__ constexpr int zslot_of(int i) {
+  int k = 0;
+  for (int j = 0; j < i; ++j) k += L::c[j][2] == L::c[i][2] ? 1 : 0;
+  return k;
+}
+template <class L>
+__host__ __device__ constexpr int zcount_of() {
+  int k = 0;
+  for (int j = 0; j < L::Q; ++j) k += L::c[j][2] > 0 ? 1 : 0;
+  return k;
+}
+
 }  // namespace lbcube

@@ -41,11 +41,12 @@ __global__ void __launch_bounds__(kThreads)
 
 constexpr int kFinalThreads = 1024;
 
-__global__ void __launch_bounds__(kFinalThreads)
-    stats_finalize_kernel(const double* __restrict__ partials, long long blocks, long long cells,
-                          double k, double* __restrict__ out) {
+// Adds the partials in a fixed order; thread 0 returns the five sums in s.
+__device__ __forceinline__ void sum_partials(const double* __restrict__ partials, long long blocks,
+                                             double (&s)[kStatSums]) {
   __shared__ double sh[kFinalThreads][kStatSums];
-  double s[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int q = 0; q < kStatSums; ++q) s[q] = 0.0;
   for (long long blk = threadIdx.x; blk < blocks; blk += kFinalThreads) {
 #pragma unroll
     for (int q = 0; q < kStatSums; ++q) s[q] += partials[blk * kStatSums + q];
@@ -60,22 +61,55 @@ __global__ void __launch_bounds__(kFinalThreads)
     }
     __syncthreads();
   }
+#pragma unroll
+  for (int q = 0; q < kStatSums; ++q) s[q] = sh[0][q];
+}
+
+// The eight ReactiveDiagnostics fields from the five sums over `cells` cells
+// (the reference's formulas, lattice_io.hpp:318-337, in FP64).
+__device__ __forceinline__ void diagnostics_from_sums(const double (&s)[kStatSums], double cells,
+                                                      double k, double* __restrict__ out) {
+  const double inv = 1.0 / cells;
+  const double ma = s[0] * inv, mb = s[1] * inv;
+  const double ma2 = s[2] * inv, mb2 = s[3] * inv, mab = s[4] * inv;
+  const double cov = mab - ma * mb;
+  const double mp = ma * mb;
+  const double eps = 2.220446049250313080847e-16;
+  out[0] = ma;
+  out[1] = mb;
+  out[2] = ma2 - ma * ma;
+  out[3] = mb2 - mb * mb;
+  out[4] = cov;
+  out[5] = fabs(mp) > eps ? cov / mp : 0.0;
+  out[6] = k * mab;
+  out[7] = k * ma * mb;
+}
+
+__global__ void __launch_bounds__(kFinalThreads)
+    stats_finalize_kernel(const double* __restrict__ partials, long long blocks, long long cells,
+                          double k, double* __restrict__ out) {
+  double s[kStatSums];
+  sum_partials(partials, blocks, s);
+  if (threadIdx.x == 0) diagnostics_from_sums(s, (double)cells, k, out);
+}
+
+// The five sums alone: a rank's share of the statistics of a decomposed domain.
+__global__ void __launch_bounds__(kFinalThreads)
+    stats_sums_kernel(const double* __restrict__ partials, long long blocks, double* __restrict__ out) {
+  double s[kStatSums];
+  sum_partials(partials, blocks, s);
   if (threadIdx.x == 0) {
-    const double inv = 1.0 / (double)cells;
-    const double ma = sh[0][0] * inv, mb = sh[0][1] * inv;
-    const double ma2 = sh[0][2] * inv, mb2 = sh[0][3] * inv, mab = sh[0][4] * inv;
-    const double cov = mab - ma * mb;
-    const double mp = ma * mb;
-    const double eps = 2.220446049250313080847e-16;
-    out[0] = ma;
-    out[1] = mb;
-    out[2] = ma2 - ma * ma;
-    out[3] = mb2 - mb * mb;
-    out[4] = cov;
-    out[5] = fabs(mp) > eps ? cov / mp : 0.0;
-    out[6] = k * mab;
-    out[7] = k * ma * mb;
+#pragma unroll
+    for (int q = 0; q < kStatSums; ++q) out[q] = s[q];
   }
+}
+
+__global__ void stats_from_sums_kernel(const double* __restrict__ sums, double cells, double k,
+                                       double* __restrict__ out) {
+  double s[kStatSums];
+#pragma unroll
+  for (int q = 0; q < kStatSums; ++q) s[q] = sums[q];
+  diagnostics_from_sums(s, cells, k, out);
 }
 
 cudaError_t launch_finalize(const Grid& g, double k, const double* partials, double* out,
@@ -160,6 +194,35 @@ extern "C" int lbm_reactive_stats_finalize_async(int fluid_lattice, int precisio
   if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return (int)cudaErrorInvalidValue;
   const double k = precision == LBM_FLOAT ? (double)(float)k_react : k_react;
   return (int)launch_finalize(g, k, partials, diagnostics, as_stream(stream));
+}
+
+// Statistics of a domain split across ranks: each rank reduces its partials
+// to the five sums (lbm_reactive_stats_sums_async), the ranks add the sums
+// (an all-reduce of five doubles), and lbm_reactive_stats_from_sums_async
+// forms the diagnostics from the totals. On one rank the two calls give the
+// bits of lbm_reactive_stats_finalize_async.
+extern "C" int lbm_reactive_stats_sums_async(int fluid_lattice, size_t x_extent, size_t y_extent,
+                                             size_t z_extent, const double* partials,
+                                             size_t partials_bytes, double* sums, void* stream) {
+  Grid g;
+  const int dims = fluid_lattice == LBM_D2Q9 || fluid_lattice == LBM_D2Q5 ? 2 : 3;
+  cudaError_t err = validate_domain(partials == nullptr || sums == nullptr, 1, 1, 1, dims,
+                                    x_extent, y_extent, z_extent, g);
+  if (err != cudaSuccess) return (int)err;
+  if (partials_bytes < (size_t)g.blocks() * kStatSums * sizeof(double)) return (int)cudaErrorInvalidValue;
+  stats_sums_kernel<<<1, kFinalThreads, 0, as_stream(stream)>>>(partials, g.blocks(), sums);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int lbm_reactive_stats_from_sums_async(int precision, const double* sums, double cells,
+                                                  double k_react, double* diagnostics,
+                                                  void* stream) {
+  if (sums == nullptr || diagnostics == nullptr) return (int)cudaErrorInvalidDevicePointer;
+  if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return (int)cudaErrorInvalidValue;
+  if (!(cells >= 1.0)) return (int)cudaErrorInvalidValue;
+  const double k = precision == LBM_FLOAT ? (double)(float)k_react : k_react;
+  stats_from_sums_kernel<<<1, 1, 0, as_stream(stream)>>>(sums, cells, k, diagnostics);
+  return (int)cudaGetLastError();
 }
 
 // ----------------------------------------------------------------------------

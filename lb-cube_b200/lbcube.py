@@ -109,6 +109,11 @@ def _declare(lib):
         "lbm_step_slab_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp, _vp, _vp, _sz,
                                 _sz, _vp],
         "lbm_slab_pack_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
+        "lbm_fluid_reaction_slab_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz,
+                                          _sz, d, d, d, _vp, _vp, _vp, _vp, _sz, _sz, _vp, _sz, _vp],
+        "lbm_fluid_reaction_slab_pack_async": [C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
+        "lbm_reactive_stats_sums_async": [C.c_int, _sz, _sz, _sz, _vp, _sz, _vp, _vp],
+        "lbm_reactive_stats_from_sums_async": [C.c_int, _vp, d, d, _vp, _vp],
         "lbm_macro_fields_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp, _vp],
         "lbm_write_vtk_legacy": [C.c_char_p, C.c_int, _sz, _sz, _sz, _sz, C.c_int, _vp, _vp, _vp],
         "lbm_write_populations": [C.c_char_p, C.c_int, C.c_int, _sz, _sz, _sz, _sz, _vp],
@@ -125,6 +130,8 @@ def _declare(lib):
     lib.lbm_stats_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
     lib.lbm_slab_face_elems.restype = C.c_size_t
     lib.lbm_slab_face_elems.argtypes = [C.c_int, _sz, _sz]
+    lib.lbm_fluid_reaction_slab_face_elems.restype = C.c_size_t
+    lib.lbm_fluid_reaction_slab_face_elems.argtypes = [C.c_int, _sz, _sz]
     lib.lbm_reactive_gradient_workspace_bytes.restype = C.c_size_t
     lib.lbm_reactive_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, C.c_int, _sz, _sz, _sz, C.c_int,
                                                           C.c_int]

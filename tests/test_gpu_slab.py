@@ -2,8 +2,10 @@
 process (LocalExchange copies the face buffers between slabs, standing in for
 the point-to-point transfers); stepping the slabs is bit-identical to
 stepping the whole periodic box with lbm_step_async, for W = 1..4 including
-one-plane slabs. The single-rank path of SlabDomain.step (exchange on a second
-stream, overlapped with the interior planes) is bit-identical too."""
+one-plane slabs, and the same holds for the coupled fluid + A + B -> C step
+with its statistics. The single-rank path of SlabDomain.step (exchange on a
+second stream, overlapped with the interior planes) is bit-identical too.
+tests/test_gpu_slab_mp.py runs the ranks as separate processes."""
 import numpy as np
 import pytest
 import torch
@@ -115,3 +117,72 @@ def test_slab_validation(engine, dev):
     assert args(1, 2, None, None, None, None) == 0             # interior plane: no face buffer needed
     assert args(0, 1, p[0], p[1], b.data_ptr(), p[3]) == E.cudaErrorInvalidValue  # send overlaps the output
     torch.cuda.synchronize()
+
+
+REACTIVE_CASES = [("D3Q19", "float", "TRT", (16, 6, 6)), ("D3Q19", "double", "MRT", (8, 4, 6)),
+                  ("D3Q27", "float", "BGK", (8, 4, 6))]
+
+
+def _reactive_state(lat, dt, dims, seed):
+    nx, ny, nz = dims
+    f = U.random_state(lat, nx, ny, nz, dt, seed=seed)
+    a = U.random_scalar("D3Q7", nx, ny, nz, dt, seed=seed + 1)
+    b = U.random_scalar("D3Q7", nx, ny, nz, dt, seed=seed + 2)
+    return f, a, b
+
+
+@pytest.mark.parametrize("lat,dn,op,dims", REACTIVE_CASES)
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_coupled_slabs_match_whole_box(engine, dev, lat, dn, op, dims, world):
+    """The coupled fluid + A + B -> C step as slabs (face buffers carrying the
+    fluid's crossing populations and one D3Q7 plane per species) is
+    bit-identical to the whole box stepped with lbm_fluid_reaction_ab_async, and
+    the statistics from the ranks' summed partials equal the whole box's: bit
+    for bit on one rank, to 1e-12 across ranks (the sums are added in another
+    order)."""
+    nx, ny, nz = dims
+    dt = np.float32 if dn == "float" else np.float64
+    steps, omega, omega_c, k = 6, 1 / 0.6, 1 / 0.8, 0.3
+    f, a, b = _reactive_state(lat, dt, dims, seed=31)
+    whole = [torch.from_numpy(x).to(dev) for x in (f, a, b)]
+    wnext = [torch.empty_like(x) for x in whole]
+    pb = E.stats_partials_bytes(lat, nx, ny, nz)
+    part = torch.empty(pb // 8, dtype=torch.float64, device=dev)
+    want_stats = torch.empty(8, dtype=torch.float64, device=dev)
+    for s in range(steps):
+        last = s == steps - 1
+        E.check(E.fluid_reaction_ab_async(lat, dn, op, whole[0], wnext[0], whole[1], wnext[1], whole[2], wnext[2],
+                                          nx, ny, nz, omega, omega_c, k, part if last else None, pb if last else 0))
+        whole, wnext = wnext, whole
+    E.check(E.reactive_stats_finalize_async(lat, dn, nx, ny, nz, k, part, pb, want_stats))
+
+    doms = [slab.ReactiveSlabDomain(torch, lat, dn, op, nx, ny, nz, omega, omega_c, k, r, world, dev)
+            for r in range(world)]
+    q = E.Q_OF[lat]
+
+    def split(x, qq):
+        x4 = x.reshape(qq, nz, ny, nx)
+        return [torch.from_numpy(np.ascontiguousarray(x4[:, d.z0:d.z0 + d.nz])).to(dev) for d in doms]
+
+    cur = list(zip(split(f, q), split(a, 7), split(b, 7)))
+    nxt = [tuple(torch.empty_like(t) for t in c) for c in cur]
+    ex = slab.LocalExchange(doms)
+    for d, c in zip(doms, cur):
+        d.pack(c)
+    ex.exchange_all()
+    for s in range(steps):
+        for d, c, n in zip(doms, cur, nxt):
+            d.compute(c, n, stats=s == steps - 1)
+        ex.exchange_all()
+        cur, nxt = nxt, cur
+    sums = sum(d.rank_sums() for d in doms) if world > 1 else doms[0].rank_sums()
+    got_stats = slab.diagnostics_from_sums(torch, dn, sums, nx * ny * nz, k)
+    torch.cuda.synchronize()
+    for idx, (qq, ref) in enumerate(((q, whole[0]), (7, whole[1]), (7, whole[2]))):
+        got = np.concatenate([c[idx].cpu().numpy() for c in cur], axis=1).reshape(qq, -1)
+        assert U.same_bits(got, ref.cpu().numpy().reshape(qq, -1)), ("fluid", "A", "B")[idx]
+    g, w = got_stats.cpu().numpy(), want_stats.cpu().numpy()
+    if world == 1:
+        assert U.same_bits(g, w)
+    else:
+        assert np.all(np.abs(g - w) <= 1e-12 * np.maximum(np.abs(w), 1e-300)), (g, w)
