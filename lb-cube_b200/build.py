@@ -76,6 +76,34 @@ def _compile(src, verbose):
     return obj, (res.stdout + res.stderr)
 
 
+DRIVERS = os.path.join(HERE, "drivers")
+BIN = os.path.join(HERE, "bin")
+CUDA_HOME = os.path.dirname(os.path.dirname(os.path.realpath(NVCC)))
+
+
+def build_drivers(force: bool = False) -> list:
+    """The ports of the reference's two drivers (drivers/*.cpp): host C++23
+    executables on the C ABI, linked to the library next to them (bin/)."""
+    os.makedirs(BIN, exist_ok=True)
+    cxx = os.environ.get("CXX", shutil.which("g++") or "g++")
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    out = []
+    for name in ("lbm_sim", "lbm_reaction_sim"):
+        src = os.path.join(DRIVERS, name + ".cpp")
+        exe = os.path.join(BIN, name)
+        deps = [src, os.path.join(DRIVERS, "driver_common.hpp"), os.path.join(inc, "lbcube_b200.h"), LIB]
+        if force or _stale(exe, deps):
+            cmd = [cxx, "-std=c++23", "-O2", "-ffp-contract=off", "-Wall", "-Wextra", f"-I{inc}",
+                   f"-I{os.path.join(CUDA_HOME, 'include')}", src, "-o", exe, f"-L{HERE}", "-llbcube_b200",
+                   "-Wl,-rpath,$ORIGIN/..", f"-L{os.path.join(CUDA_HOME, 'lib64')}", "-lcudart",
+                   f"-Wl,-rpath,{os.path.join(CUDA_HOME, 'lib64')}"]
+            res = subprocess.run(cmd, capture_output=True, text=True)
+            if res.returncode != 0:
+                raise RuntimeError(f"driver build failed:\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+        out.append(exe)
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     """Compile (if stale) and link the engine library; returns its path."""
     os.makedirs(BUILD, exist_ok=True)
@@ -98,6 +126,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
         os.replace(tmp, LIB)
+    build_drivers(force)
     return LIB
 
 
