@@ -507,75 +507,88 @@ def run_reactive_adjoint_cost(torch, E, dev, n=192, steps=3000, interval=100, ta
     return out
 
 
-def run_reactive_mixing(torch, E, dev, n=1024, steps=20000, every=10, tau=0.6):
-    """2-D reactive mixing: D2Q9 MRT double shear layer (u = 0.04 tanh, delta = 8
-    cells, the periodic form of turbulent_shear_layer.cpp:61-63, plus a
-    seeded sinusoidal + random u_y perturbation of relative amplitude 1e-3)
-    coupled to two D2Q5 scalars (A = 1 in the top half, B = 1 in the bottom
-    half) reacting A + B -> C with Pe = U L / D = 1000 and Da = k C0 L / U = 1
-    for L = n. Every step is one fused fluid + reaction launch; every `every`
-    steps that launch also writes the statistics partials and a finalize
-    launch appends the eight ReactiveDiagnostics fields to a device table, so
-    the loop never synchronises with the host."""
-    u0, delta = 0.04, 8.0
-    tau_c = 0.5 + 3.0 * (u0 * n / 1000.0)  # D = cs2 (tau_c - 1/2), cs2 = 1/3
-    k = u0 / n
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(SEED)
-    ax = torch.arange(n, device=dev, dtype=torch.float64) / n
-    y, x = torch.meshgrid(ax, ax, indexing="ij")
-    ux = torch.where(y <= 0.5, u0 * torch.tanh((n / delta) * (y - 0.25)), u0 * torch.tanh((n / delta) * (0.75 - y)))
-    uy = u0 * 1e-3 * (torch.sin(2 * math.pi * (x + 0.25)) +
-                      torch.randn((n, n), generator=gen, device=dev, dtype=torch.float64))
-    u = torch.stack([ux, uy]).float().contiguous()
-    rho = torch.ones((n, n), device=dev, dtype=torch.float32)
-    a0 = (y > 0.5).float().contiguous()
-    b0 = (y <= 0.5).float().contiguous()
+def run_reactive_mixing(torch, E, dev, n=1024, steps=20000, every=10):
+    """2-D reactive mixing: D2Q9 MRT double shear layer coupled to two D2Q5
+    scalars reacting A + B -> C (workloads.reactive_shear_layer: u = 0.04 tanh
+    with delta = 8 cells, the periodic form of turbulent_shear_layer.cpp:61-63,
+    seeded transverse perturbation; A = 1 in the top half, B = 1 in the bottom
+    half; Pe = 1000, Da = 1 for L = n; tau 0.6). Every step is one fused fluid +
+    reaction launch; every `every` steps that launch also writes the statistics
+    partials and lbm_reactive_stats_append_async writes the eight
+    ReactiveDiagnostics fields to the next row of a device table. The `every`
+    steps plus the append are captured once in a CUDA graph and replayed
+    steps / every times: no host work and no synchronisation in the loop.
+    The same workload and sequence is held to the reference CPU run in
+    tests/test_gpu_c3.py."""
+    import workloads as W
+
+    w = W.reactive_shear_layer(n)
+    tau, tau_c, k = w["tau"], w["tau_c"], w["k"]
+    rho = torch.from_numpy(w["rho"]).to(dev)
+    u = torch.from_numpy(w["u"]).to(dev)
+    a0 = torch.from_numpy(w["a0"]).to(dev)
+    b0 = torch.from_numpy(w["b0"]).to(dev)
     f = [torch.empty((9, n, n), device=dev, dtype=torch.float32) for _ in range(2)]
     A = [torch.empty((5, n, n), device=dev, dtype=torch.float32) for _ in range(2)]
     B = [torch.empty((5, n, n), device=dev, dtype=torch.float32) for _ in range(2)]
     pb = E.stats_partials_bytes("D2Q9", n, n, 1)
     part = torch.empty(pb, dtype=torch.uint8, device=dev)
-    table = torch.zeros((steps // every, 8), dtype=torch.float64, device=dev)
+    rows = steps // every
+    table = torch.zeros((rows, 8), dtype=torch.float64, device=dev)
+    row = torch.zeros(1, dtype=torch.int64, device=dev)
+    assert every % 2 == 0  # a chunk returns the ping-pong buffers to their places
 
     def init():
         E.check(E.init_equilibrium_async("D2Q9", "float", rho, u, f[0], n, n, 1))
         E.check(E.init_equilibrium_async("D2Q5", "float", a0, u, A[0], n, n, 1))
         E.check(E.init_equilibrium_async("D2Q5", "float", b0, u, B[0], n, n, 1))
+        row.zero_()
 
-    def run(nsteps):
-        for s_ in range(nsteps):
+    def chunk(stream):
+        for s_ in range(every):
             i, j = s_ % 2, (s_ + 1) % 2
-            stats = (s_ + 1) % every == 0
+            last = s_ == every - 1
             E.check(E.fluid_reaction_ab_async("D2Q9", "float", "MRT", f[i], f[j], A[i], A[j], B[i], B[j], n, n, 1,
-                                              1.0 / tau, 1.0 / tau_c, k, part if stats else None,
-                                              pb if stats else 0))
-            if stats:
-                E.check(E.reactive_stats_finalize_async("D2Q9", "float", n, n, 1, k, part, pb,
-                                                        table[(s_ + 1) // every - 1]))
+                                              1.0 / tau, 1.0 / tau_c, k, part if last else None, pb if last else 0,
+                                              stream=stream))
+        E.check(E.reactive_stats_append_async("D2Q9", "float", n, n, 1, k, part, pb, table, rows, row,
+                                              stream=stream))
 
+    s = torch.cuda.Stream(device=dev)
     init()
-    run(2 * every)  # warm-up
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        chunk(s)  # warm-up outside the graph
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        chunk(s)
+    init()
+    for _ in range(2):  # warm-up replays
+        graph.replay()
     init()
     torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
-    t0.record()
-    run(steps)
-    t1.record()
+    t0.record(s)
+    with torch.cuda.stream(s):
+        for _ in range(rows):
+            graph.replay()
+    t1.record(s)
     torch.cuda.synchronize()
     ms = t0.elapsed_time(t1)
+    assert int(row.item()) == rows
     cells = n * n
     mlups = cells * steps / (ms * 1e-3) / 1e6
     last = table[-1].tolist()
     out = {"config": f"D2Q9 MRT + 2 x D2Q5 (A + B -> C) FP32 {n}^2 double shear layer (u0 0.04, delta 8), "
                      f"tau {tau}, tau_c {tau_c:.5f} (Pe 1000), k {k:.6g} (Da 1), {steps} steps, statistics "
-                     f"every {every} steps in FP64 on the device",
+                     f"every {every} steps in FP64 on the device; {every}-step chunks replayed as one CUDA graph",
            "ms_total": round(ms, 2), "mlups": round(mlups, 1), "bytes_per_lu": 152,
            "achieved_gbs": round(152 * cells * steps / (ms * 1e-3) / 1e9, 1),
            "stats_rows": int(table.shape[0]), "final_mean_a": last[0], "final_mean_b": last[1],
            "final_segregation_intensity": last[5], "final_true_rate": last[6], "final_mixed_rate": last[7]}
-    del f, A, B, part, table
+    del graph, f, A, B, part, table
     torch.cuda.empty_cache()
     return out
 

@@ -407,6 +407,18 @@ int lbm_reactive_gradient_async(int fluid_lattice, int precision, int storage, f
     double k_react, int steps, int checkpoint_interval, void* workspace, size_t workspace_bytes,
     double* result, void* grad_a0, void* grad_b0, void* grad_u0, void* stream);
 
+/* The same second pass writing into row *row_counter of a device table of
+ * table_rows x 8 doubles (rows at or past table_rows are not written), then
+ * advancing *row_counter (device). No reference counterpart: the destination
+ * row is read on the device, so a sequence of steps with this call at its end
+ * can be captured once in a CUDA graph and replayed to fill successive rows
+ * (the reference driver logs a row every output_frequency steps,
+ * simulate_reaction.cpp:557-580). */
+int lbm_reactive_stats_append_async(int fluid_lattice, int precision, size_t x_extent,
+    size_t y_extent, size_t z_extent, double k_react, const double* partials,
+    size_t partials_bytes, double* table, size_t table_rows, unsigned long long* row_counter,
+    void* stream);
+
 /* Statistics of a domain split across ranks (no reference counterpart): each
  * rank reduces its partials (from a statistics launch over its cells) to the
  * five FP64 sums of C_A, C_B, C_A^2, C_B^2, C_A C_B (device, 5 doubles); the

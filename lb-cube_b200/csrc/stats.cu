@@ -93,6 +93,23 @@ __global__ void __launch_bounds__(kFinalThreads)
   if (threadIdx.x == 0) diagnostics_from_sums(s, (double)cells, k, out);
 }
 
+// Finalize into the next row of a device table: row *row_counter (if below
+// rows), then the counter advances. The destination is read on the device, so
+// a captured sequence of steps plus this launch can be replayed to fill
+// successive rows.
+__global__ void __launch_bounds__(kFinalThreads)
+    stats_append_kernel(const double* __restrict__ partials, long long blocks, long long cells,
+                        double k, double* __restrict__ table, unsigned long long rows,
+                        unsigned long long* __restrict__ row_counter) {
+  double s[kStatSums];
+  sum_partials(partials, blocks, s);
+  if (threadIdx.x == 0) {
+    const unsigned long long row = *row_counter;
+    if (row < rows) diagnostics_from_sums(s, (double)cells, k, table + row * 8);
+    *row_counter = row + 1;
+  }
+}
+
 // The five sums alone: a rank's share of the statistics of a decomposed domain.
 __global__ void __launch_bounds__(kFinalThreads)
     stats_sums_kernel(const double* __restrict__ partials, long long blocks, double* __restrict__ out) {
@@ -194,6 +211,28 @@ extern "C" int lbm_reactive_stats_finalize_async(int fluid_lattice, int precisio
   if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return (int)cudaErrorInvalidValue;
   const double k = precision == LBM_FLOAT ? (double)(float)k_react : k_react;
   return (int)launch_finalize(g, k, partials, diagnostics, as_stream(stream));
+}
+
+extern "C" int lbm_reactive_stats_append_async(int fluid_lattice, int precision, size_t x_extent,
+                                               size_t y_extent, size_t z_extent, double k_react,
+                                               const double* partials, size_t partials_bytes,
+                                               double* table, size_t table_rows,
+                                               unsigned long long* row_counter, void* stream) {
+  Grid g;
+  const int dims = fluid_lattice == LBM_D2Q9 || fluid_lattice == LBM_D2Q5 ? 2 : 3;
+  cudaError_t err = validate_domain(partials == nullptr || table == nullptr || row_counter == nullptr,
+                                    1, 1, 1, dims, x_extent, y_extent, z_extent, g);
+  if (err != cudaSuccess) return (int)err;
+  const size_t need = (size_t)g.blocks() * kStatSums * sizeof(double);
+  if (partials_bytes < need || table_rows == 0) return (int)cudaErrorInvalidValue;
+  if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return (int)cudaErrorInvalidValue;
+  const Span reads[1] = {{partials, need}};
+  const Span writes[2] = {{table, table_rows * 8 * sizeof(double)}, {row_counter, sizeof(unsigned long long)}};
+  if (any_overlap(reads, writes)) return (int)cudaErrorInvalidValue;
+  const double k = precision == LBM_FLOAT ? (double)(float)k_react : k_react;
+  stats_append_kernel<<<1, kFinalThreads, 0, as_stream(stream)>>>(partials, g.blocks(), g.plane, k, table,
+                                                                  table_rows, row_counter);
+  return (int)cudaGetLastError();
 }
 
 // Statistics of a domain split across ranks: each rank reduces its partials

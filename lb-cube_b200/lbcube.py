@@ -113,6 +113,7 @@ def _declare(lib):
                                           _sz, d, d, d, _vp, _vp, _vp, _vp, _sz, _sz, _vp, _sz, _vp],
         "lbm_fluid_reaction_slab_pack_async": [C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
         "lbm_reactive_stats_sums_async": [C.c_int, _sz, _sz, _sz, _vp, _sz, _vp, _vp],
+        "lbm_reactive_stats_append_async": [C.c_int, C.c_int, _sz, _sz, _sz, d, _vp, _sz, _vp, _sz, _vp, _vp],
         "lbm_reactive_stats_from_sums_async": [C.c_int, _vp, d, d, _vp, _vp],
         "lbm_macro_fields_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp, _vp],
         "lbm_write_vtk_legacy": [C.c_char_p, C.c_int, _sz, _sz, _sz, _sz, C.c_int, _vp, _vp, _vp],
@@ -274,6 +275,14 @@ def reactive_stats_async(scalar_lattice, real, a, b, nx, ny, nz, k_react, partia
     return load().lbm_reactive_stats_async(LATTICES[scalar_lattice], REALS[real_name(real)], _ptr(a),
                                            _ptr(b), nx, ny, nz, float(k_react), _ptr(partials),
                                            int(partials_bytes), _ptr(diagnostics), _stream(stream))
+
+
+def reactive_stats_append_async(fluid_lattice, real, nx, ny, nz, k_react, partials, partials_bytes, table,
+                                table_rows, row_counter, stream=None) -> int:
+    return load().lbm_reactive_stats_append_async(LATTICES[fluid_lattice], REALS[real_name(real)], nx, ny, nz,
+                                                  float(k_react), _ptr(partials), int(partials_bytes),
+                                                  _ptr(table), int(table_rows), _ptr(row_counter),
+                                                  _stream(stream))
 
 
 def reactive_stats_finalize_async(fluid_lattice, real, nx, ny, nz, k_react, partials, partials_bytes,
