@@ -545,6 +545,72 @@ int lbm_fluid_reaction_slab_pack_async(int fluid_lattice, int precision, const v
     const void* a, const void* b, size_t x_extent, size_t y_extent, size_t z_extent,
     void* send_lo, void* send_hi, void* stream);
 
+/* The gradient of lbm_reactive_gradient_async on a z-slab (no reference
+ * counterpart): native FP32 / FP64 states, D3Q19 (BGK, TRT, MRT) or D3Q27
+ * (BGK, TRT) fluid with two D3Q7 species. Every rank runs the whole-box
+ * sequence on its slab (z_extent = its own planes, total_cells = cells of the
+ * whole box); the face buffers have the layout above, and each exchange moves
+ * send_hi(r) into halo_lo(r + 1) and send_lo(r) into halo_hi(r - 1):
+ *   forward step  lbm_reactive_slab_forward_async (velocity, [3, Z, Y, X],
+ *                 may be null for states the backward sweep recomputes), then
+ *                 an exchange;
+ *   adjoint step  n (state n and u^{n+1} stored): lbm_fluid_reaction_slab_pack_async
+ *                 of state n + exchange (its halos), then
+ *                 lbm_reactive_slab_adjoint_step_async (lambda^{n+1} ->
+ *                 lambda^n; velocity_adjoint is [3, Z, Y, X] scratch; adds to
+ *                 the per-warp slots of lbm_reactive_slab_slots_bytes, zeroed
+ *                 by the caller before the first step), an exchange of the
+ *                 scatter sends it wrote, and
+ *                 lbm_reactive_slab_adjoint_unpack_async(halo_lo, halo_hi) into
+ *                 lambda^n;
+ *   seed          lbm_reactive_slab_seed_async of the final state (segregation:
+ *                 the whole box's eight diagnostics, e.g. from
+ *                 lbm_reactive_stats_sums_async over ranks and
+ *                 lbm_reactive_stats_from_sums_async); objective partials of
+ *                 lbm_reactive_slab_objective_bytes;
+ *   end           lbm_reactive_slab_init_gradients_async (grad_b0, grad_u0
+ *                 may be null), lbm_reactive_slab_sums_async (the rank's four
+ *                 FP64 sums), an all-reduce (sum) of those four doubles, and
+ *                 lbm_reactive_slab_result_async -> result[4] = J, dJ/dk,
+ *                 dJ/dtau, dJ/dtau_c.
+ * A slab's adjoint fields and initial-state gradients are bit-identical to the
+ * whole box's given the same seed; the four scalars differ from the whole
+ * box's only in the order of the FP64 sums. */
+size_t lbm_reactive_slab_slots_bytes(int fluid_lattice, size_t x_extent, size_t y_extent,
+    size_t z_extent);
+size_t lbm_reactive_slab_objective_bytes(int fluid_lattice, size_t x_extent, size_t y_extent,
+    size_t z_extent);
+int lbm_reactive_slab_forward_async(int fluid_lattice, int precision, int collision,
+    const void* current_fluid, void* next_fluid, const void* current_a, void* next_a,
+    const void* current_b, void* next_b, void* velocity, size_t x_extent, size_t y_extent,
+    size_t z_extent, double tau, double tau_c, double k_react, const void* halo_lo,
+    const void* halo_hi, void* send_lo, void* send_hi, void* stream);
+int lbm_reactive_slab_adjoint_step_async(int fluid_lattice, int precision, int collision,
+    const void* fluid_n, const void* a_n, const void* b_n, const void* halo_lo,
+    const void* halo_hi, const void* velocity_next, const void* lambda_fluid_next,
+    const void* lambda_a_next, const void* lambda_b_next, void* lambda_fluid, void* lambda_a,
+    void* lambda_b, void* velocity_adjoint, void* send_lo, void* send_hi, size_t x_extent,
+    size_t y_extent, size_t z_extent, double tau, double tau_c, double k_react, double* slots,
+    size_t slots_bytes, void* stream);
+int lbm_reactive_slab_adjoint_unpack_async(int fluid_lattice, int precision,
+    const void* recv_lo, const void* recv_hi, void* lambda_fluid, void* lambda_a,
+    void* lambda_b, size_t x_extent, size_t y_extent, size_t z_extent, void* stream);
+int lbm_reactive_slab_seed_async(int fluid_lattice, int precision, int objective,
+    const void* a_final, const void* b_final, const void* a0, const double* diagnostics,
+    void* lambda_fluid, void* lambda_a, void* lambda_b, size_t x_extent, size_t y_extent,
+    size_t z_extent, double total_cells, double* objective_partials, size_t partials_bytes,
+    void* stream);
+int lbm_reactive_slab_init_gradients_async(int fluid_lattice, int precision, int objective,
+    const void* rho0, const void* u0, const void* a0, const void* b0, const void* lambda_fluid,
+    const void* lambda_a, const void* lambda_b, size_t x_extent, size_t y_extent,
+    size_t z_extent, double total_cells, void* grad_a0, void* grad_b0, void* grad_u0,
+    void* stream);
+int lbm_reactive_slab_sums_async(int fluid_lattice, size_t x_extent, size_t y_extent,
+    size_t z_extent, const double* slots, size_t slots_bytes, const double* objective_partials,
+    size_t partials_bytes, double* sums, void* stream);
+int lbm_reactive_slab_result_async(int precision, int objective, const double* sums,
+    const double* diagnostics, double total_cells, double tau_c, double* result, void* stream);
+
 /* ---- output ----------------------------------------------------------------
  * Macroscopic fields for output, computed on the device from the populations
  * as the reference's VTK writer computes them on the host (write_vtk,

@@ -36,6 +36,7 @@
 //   LBM_OBJECTIVE_SEGREGATION   I_s = cov(C_A, C_B) / (<C_A> <C_B>) of
 //                               compute_reactive_stats (lattice_io.hpp:318-337)
 #include <algorithm>
+#include <type_traits>
 
 #include "adjoint.cuh"
 #include "adr.cuh"
@@ -44,6 +45,7 @@
 #include "collide.cuh"
 #include "common.cuh"
 #include "reduce.cuh"
+#include "slab_faces.cuh"
 #include "stream_vec.cuh"
 #include "../../include/lbcube_b200.h"
 
@@ -135,20 +137,36 @@ struct ShiftedState {
 constexpr int kReactiveSlots = 3;
 constexpr int kWarpsPerBlock = kThreads / 32;
 
+// The face buffers of a z-slab (slab_faces.cuh): halos of the stored state the
+// step pulls from, and sends of the adjoint scatter. Unused on the whole box.
+template <class Real>
+struct SlabFaces {
+  const Real* halo_lo;
+  const Real* halo_hi;
+  Real* send_lo;
+  Real* send_hi;
+};
+
 // Reaction part of adjoint step n at every cell x: from the pulled A^n, B^n,
 // lambda_A^{n+1}, lambda_B^{n+1} at x and the advecting velocity u^{n+1}(x)
 // (stored by the forward pass), scatter abar and bbar to lambda^n_A, lambda^n_B,
 // write ubar(x) = dJ/du^{n+1}(x) for the fluid part, and add the block's
 // dJ/dk and dJ/domega_c to its slots.
-template <class FL, class Real, class SP>
+// SLAB: the pulls and scatters cross the z faces through `faces` (native
+// states only).
+template <class FL, class Real, class SP, bool SLAB = false>
 __global__ void __launch_bounds__(kThreads)
     reaction_adjoint_kernel(const typename SP::elem* __restrict__ an,
                             const typename SP::elem* __restrict__ bn,
                             const Real* __restrict__ u_next, const Real* __restrict__ la_next,
                             const Real* __restrict__ lb_next, Real* __restrict__ la,
                             Real* __restrict__ lb, Real* __restrict__ ubar_out, Grid g,
-                            ReactiveParams rp, double* __restrict__ slots) {
+                            ReactiveParams rp, double* __restrict__ slots,
+                            SlabFaces<Real> faces = {}) {
   using SL = typename ScalarOf<FL>::type;
+  static_assert(!SLAB || std::is_same_v<SP, NativeState<Real>>);
+  const size_t a_off = (size_t)face_planes<FL>() * g.ny * g.nx;
+  const size_t b_off = a_off + (size_t)face_planes<SL>() * g.ny * g.nx;
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double acc[2] = {0.0, 0.0};
@@ -159,8 +177,13 @@ __global__ void __launch_bounds__(kThreads)
     Real u[FL::D];
     static_for<FL::D>([&](auto D) { u[LB_I(D)] = __ldg(u_next + plane * LB_I(D) + cell); });
     Real ga[SL::Q], gb[SL::Q], lA[SL::Q], lB[SL::Q];
-    SP::template pulled<SL>(an, g, n, x, y, z, rp.c0, ga);
-    SP::template pulled<SL>(bn, g, n, x, y, z, rp.c0, gb);
+    if constexpr (SLAB) {
+      gather_slab<SL>(an, g, n, x, y, z, faces.halo_lo + a_off, faces.halo_hi + a_off, ga);
+      gather_slab<SL>(bn, g, n, x, y, z, faces.halo_lo + b_off, faces.halo_hi + b_off, gb);
+    } else {
+      SP::template pulled<SL>(an, g, n, x, y, z, rp.c0, ga);
+      SP::template pulled<SL>(bn, g, n, x, y, z, rp.c0, gb);
+    }
     load_cell<SL>(la_next, g, cell, lA);
     load_cell<SL>(lb_next, g, cell, lB);
     const Real ca = concentration<SL>(ga), cb = concentration<SL>(gb);
@@ -196,8 +219,13 @@ __global__ void __launch_bounds__(kThreads)
       ma[j] = (Real(1) - oc) * lA[j] + oc * ea + sa;
       mb[j] = (Real(1) - oc) * lB[j] + oc * eb + sb;
     });
-    scatter<SL>(la, g, n, x, y, z, ma);
-    scatter<SL>(lb, g, n, x, y, z, mb);
+    if constexpr (SLAB) {
+      scatter_slab<SL>(la, g, n, x, y, z, ma, faces.send_lo + a_off, faces.send_hi + a_off);
+      scatter_slab<SL>(lb, g, n, x, y, z, mb, faces.send_lo + b_off, faces.send_hi + b_off);
+    } else {
+      scatter<SL>(la, g, n, x, y, z, ma);
+      scatter<SL>(lb, g, n, x, y, z, mb);
+    }
   }
   warp_sum<2>(acc);
   if ((threadIdx.x & 31) == 0) {
@@ -210,12 +238,13 @@ __global__ void __launch_bounds__(kThreads)
 // (c_k - u) . ubar(x) / rho (u = j / rho of the cell), then the fluid adjoint
 // of adjoint.cuh; dJ/dtau to the block's slot.
 // Register budget kAdjointBlocks (adjoint.cuh).
-template <class FL, class Real, int CT, class SP>
+template <class FL, class Real, int CT, class SP, bool SLAB = false>
 __global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
     coupled_fluid_adjoint_kernel(const typename SP::elem* __restrict__ fn,
                                  const Real* __restrict__ lf_next, const Real* __restrict__ ubar_in,
                                  Real* __restrict__ lf, Grid g, AdjointParams ap, float rho0,
-                                 double* __restrict__ slots) {
+                                 double* __restrict__ slots, SlabFaces<Real> faces = {}) {
+  static_assert(!SLAB || std::is_same_v<SP, NativeState<Real>>);
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double dtau = 0.0;
@@ -224,7 +253,8 @@ __global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
     const int cell = (z * g.ny + y) * g.nx + x;
     const size_t plane = (size_t)g.plane;
     Real gv[FL::Q], lv[FL::Q], mu[FL::Q], rho, u[FL::D], ub[FL::D];
-    SP::template pulled<FL>(fn, g, n, x, y, z, rho0, gv);
+    if constexpr (SLAB) gather_slab<FL>(fn, g, n, x, y, z, faces.halo_lo, faces.halo_hi, gv);
+    else SP::template pulled<FL>(fn, g, n, x, y, z, rho0, gv);
     load_cell<FL>(lf_next, g, cell, lv);
     static_for<FL::D>([&](auto D) { ub[LB_I(D)] = __ldg(ubar_in + plane * LB_I(D) + cell); });
     macro_state<FL>(gv, rho, u);
@@ -236,7 +266,8 @@ __global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
       lv[k] += (c_dot<FL, k>(ub) - uub) * inv_rho;
     });
     dtau = fluid_adjoint_cell<FL, Real, CT>(gv, lv, rho, u, ap, mu);
-    scatter<FL>(lf, g, n, x, y, z, mu);
+    if constexpr (SLAB) scatter_slab<FL>(lf, g, n, x, y, z, mu, faces.send_lo, faces.send_hi);
+    else scatter<FL>(lf, g, n, x, y, z, mu);
   }
   double v[1] = {dtau};
   warp_sum<1>(v);
@@ -255,7 +286,7 @@ __global__ void __launch_bounds__(kThreads)
                          const typename SP::elem* __restrict__ bN, const Real* __restrict__ a0,
                          const double* __restrict__ stats, Real* __restrict__ lf,
                          Real* __restrict__ la, Real* __restrict__ lb, Grid g, float c0,
-                         double* __restrict__ j_slots) {
+                         double inv_n, double* __restrict__ j_slots) {
   using SL = typename ScalarOf<FL>::type;
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
@@ -263,7 +294,6 @@ __global__ void __launch_bounds__(kThreads)
   if (active) {
     const int cell = (z * g.ny + y) * g.nx + x;
     const size_t plane = (size_t)g.plane;
-    const double inv_n = 1.0 / (double)g.plane;
     Real va[SL::Q], vb[SL::Q];
     SP::template local<SL>(aN, g, cell, c0, va);
     SP::template local<SL>(bN, g, cell, c0, vb);
@@ -556,11 +586,11 @@ cudaError_t reactive_gradient(int collision, int objective, const Real* rho0, co
     if (err != cudaSuccess) return err;
     reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_SEGREGATION, SP>
         <<<grid_dims(g), block_dims(g), 0, s>>>(cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, c0,
-                                                j_slots);
+                                                1.0 / (double)g.plane, j_slots);
   } else {
     reactive_seed_kernel<FL, Real, LBM_OBJECTIVE_MEAN_PRODUCT, SP>
         <<<grid_dims(g), block_dims(g), 0, s>>>(cur.a, cur.b, a0, stats, lN.f, lN.a, lN.b, g, c0,
-                                                j_slots);
+                                                1.0 / (double)g.plane, j_slots);
   }
   if ((err = cudaGetLastError()) != cudaSuccess) return err;
   if ((err = cudaMemsetAsync(slots, 0,
@@ -679,6 +709,115 @@ cudaError_t reactive_dispatch(int lattice, int storage, float c0, int collision,
 #undef LBCUBE_REACTIVE
 }
 
+// ---- z-slab form -------------------------------------------------------------
+// The same gradient over a box cut along z into slabs, one per rank
+// (slab_faces.cuh for the face layout). The host sequence of reactive_gradient
+// runs on every rank with its own slab; the per-step pieces are entries of
+// their own because a face exchange or an all-reduce sits between them:
+//   forward step   lbm_reactive_slab_forward_async (the coupled slab step,
+//                  storing the advecting velocity), then a face exchange;
+//   adjoint step   pack of the stored state's faces + exchange (the pulled
+//                  halos), lbm_reactive_slab_adjoint_step_async (the two
+//                  kernels above with slab pulls and scatters), exchange of the
+//                  scatter sends, lbm_reactive_slab_adjoint_unpack_async;
+//   seed / end     lbm_reactive_slab_seed_async, ..._init_gradients_async,
+//                  the rank's FP64 sums (..._sums_async), an all-reduce of
+//                  those four doubles, lbm_reactive_slab_result_async.
+// Every cell does the whole box's arithmetic on the same inputs, so the
+// adjoint fields and initial-state gradients of a slab are bit-identical to
+// the whole box's (given the same seed); the four scalars differ only in the
+// order of the FP64 sums.
+
+// The neighbours' scatter sends into the slab's lambda^n (slab_faces.cuh).
+template <class FL, class Real>
+__global__ void __launch_bounds__(256)
+    reactive_slab_unpack_kernel(const Real* __restrict__ recv_lo, const Real* __restrict__ recv_hi,
+                                Real* __restrict__ lf, Real* __restrict__ la, Real* __restrict__ lb,
+                                Grid g) {
+  using SL = typename ScalarOf<FL>::type;
+  const size_t n2 = (size_t)g.ny * g.nx;
+  const size_t a_off = (size_t)face_planes<FL>() * n2;
+  const size_t b_off = a_off + (size_t)face_planes<SL>() * n2;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)(2 * n2);
+       e += (long long)gridDim.x * blockDim.x) {
+    const int side = e < (long long)n2 ? 0 : 1;
+    const size_t row = (size_t)(side == 0 ? e : e - (long long)n2);
+    unscatter_slab<FL>(lf, g, side, row, recv_lo, recv_hi);
+    unscatter_slab<SL>(la, g, side, row, recv_lo + a_off, recv_hi + a_off);
+    unscatter_slab<SL>(lb, g, side, row, recv_lo + b_off, recv_hi + b_off);
+  }
+}
+
+// J, dJ/dk, dJ/dtau, dJ/dtau_c from the all-reduced sums (objective partials,
+// slots 0..2): the scaling of reactive_gradient's last four reductions.
+static __global__ void reactive_slab_result_kernel(const double* __restrict__ sums,
+                                                   const double* __restrict__ stats, int objective,
+                                                   double inv_n, double omega_c,
+                                                   double* __restrict__ out) {
+  out[0] = objective == LBM_OBJECTIVE_SEGREGATION ? stats[5] : sums[0] * inv_n;
+  out[1] = sums[1];
+  out[2] = sums[2];
+  out[3] = sums[3] * (-omega_c * omega_c);
+}
+
+// Checks shared by the slab entries; fills g (a 3-D slab of a D3Q19 / D3Q27
+// fluid lattice).
+inline cudaError_t slab_domain(int fluid_lattice, int precision, bool any_null, size_t nx,
+                               size_t ny, size_t nz, Grid& g) {
+  if (fluid_lattice != kD3Q19 && fluid_lattice != kD3Q27) return cudaErrorInvalidValue;
+  if (precision != LBM_FLOAT && precision != LBM_DOUBLE) return cudaErrorInvalidValue;
+  return validate_domain(any_null, 1, 1, 1, 3, nx, ny, nz, g);
+}
+
+inline bool slab_collision_ok(int fluid_lattice, int collision) {
+  return collision == kBGK || collision == kTRT || (collision == kMRT && fluid_lattice != kD3Q27);
+}
+
+inline size_t slab_slots_bytes(const Grid& g) {
+  return (size_t)g.blocks() * kWarpsPerBlock * kReactiveSlots * sizeof(double);
+}
+
+template <class FL, class Real>
+cudaError_t slab_adjoint_step(int collision, const Real* fn, const Real* an, const Real* bn,
+                              const Real* halo_lo, const Real* halo_hi, const Real* u_next,
+                              const Real* lf_next, const Real* la_next, const Real* lb_next,
+                              Real* lf, Real* la, Real* lb, Real* ubar, Real* send_lo,
+                              Real* send_hi, const Grid& g, double tau, double tau_c, double k,
+                              double* slots, cudaStream_t s) {
+  using SL = typename ScalarOf<FL>::type;
+  using SP = NativeState<Real>;
+  const size_t fb = (size_t)FL::Q * g.plane * sizeof(Real);
+  const size_t sb = (size_t)SL::Q * g.plane * sizeof(Real);
+  const size_t ub = (size_t)FL::D * g.plane * sizeof(Real);
+  const size_t hb = (size_t)coupled_face_planes<FL>() * g.ny * g.nx * sizeof(Real);
+  const Span reads[9] = {{fn, fb},      {an, sb},     {bn, sb},      {halo_lo, hb}, {halo_hi, hb},
+                         {u_next, ub},  {lf_next, fb}, {la_next, sb}, {lb_next, sb}};
+  const Span writes[7] = {{lf, fb}, {la, sb}, {lb, sb}, {ubar, ub}, {send_lo, hb}, {send_hi, hb},
+                          {slots, slab_slots_bytes(g)}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  ReactiveParams rp{};
+  rp.fluid = make_params<Real>(collision, tau);
+  rp.omega_c = (double)(Real(1) / Real(tau_c));
+  rp.k = (double)Real(k);
+  rp.rho0 = 1.0f;
+  rp.c0 = 0.0f;
+  const SlabFaces<Real> faces{halo_lo, halo_hi, send_lo, send_hi};
+  reaction_adjoint_kernel<FL, Real, SP, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+      an, bn, u_next, la_next, lb_next, la, lb, ubar, g, rp, slots, faces);
+  if (collision == kBGK)
+    coupled_fluid_adjoint_kernel<FL, Real, kBGK, SP, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots, faces);
+  else if (collision == kTRT)
+    coupled_fluid_adjoint_kernel<FL, Real, kTRT, SP, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots, faces);
+  else if constexpr (FL::Q != 27)
+    coupled_fluid_adjoint_kernel<FL, Real, kMRT, SP, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots, faces);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
 }  // namespace lbcube
 
 using namespace lbcube;
@@ -725,3 +864,217 @@ extern "C" int lbm_reactive_gradient_async(int fluid_lattice, int precision, int
                                           workspace_bytes, result, grad_a0, grad_b0, grad_u0, s);
   return (int)cudaErrorInvalidValue;
 }
+
+// ---- z-slab entries -----------------------------------------------------------
+
+extern "C" size_t lbm_reactive_slab_slots_bytes(int fluid_lattice, size_t x_extent,
+                                                size_t y_extent, size_t z_extent) {
+  Grid g;
+  if (slab_domain(fluid_lattice, LBM_DOUBLE, false, x_extent, y_extent, z_extent, g) != cudaSuccess)
+    return 0;
+  return slab_slots_bytes(g);
+}
+
+extern "C" size_t lbm_reactive_slab_objective_bytes(int fluid_lattice, size_t x_extent,
+                                                    size_t y_extent, size_t z_extent) {
+  Grid g;
+  if (slab_domain(fluid_lattice, LBM_DOUBLE, false, x_extent, y_extent, z_extent, g) != cudaSuccess)
+    return 0;
+  return (size_t)g.blocks() * sizeof(double);
+}
+
+#define LBCUBE_SLAB_DISPATCH(...)                                                                 \
+  if (fluid_lattice == kD3Q19 && precision == LBM_FLOAT) { using FL = D3Q19; using R = float; __VA_ARGS__; } \
+  if (fluid_lattice == kD3Q19 && precision == LBM_DOUBLE) { using FL = D3Q19; using R = double; __VA_ARGS__; } \
+  if (fluid_lattice == kD3Q27 && precision == LBM_FLOAT) { using FL = D3Q27; using R = float; __VA_ARGS__; } \
+  if (fluid_lattice == kD3Q27 && precision == LBM_DOUBLE) { using FL = D3Q27; using R = double; __VA_ARGS__; } \
+  return (int)cudaErrorInvalidValue;
+
+extern "C" int lbm_reactive_slab_forward_async(
+    int fluid_lattice, int precision, int collision, const void* current_fluid, void* next_fluid,
+    const void* current_a, void* next_a, const void* current_b, void* next_b, void* velocity,
+    size_t x_extent, size_t y_extent, size_t z_extent, double tau, double tau_c, double k_react,
+    const void* halo_lo, const void* halo_hi, void* send_lo, void* send_hi, void* stream) {
+  Grid g;
+  cudaError_t err = slab_domain(fluid_lattice, precision,
+                                current_fluid == nullptr || next_fluid == nullptr ||
+                                    current_a == nullptr || next_a == nullptr ||
+                                    current_b == nullptr || next_b == nullptr ||
+                                    halo_lo == nullptr || halo_hi == nullptr ||
+                                    send_lo == nullptr || send_hi == nullptr,
+                                x_extent, y_extent, z_extent, g);
+  if (err != cudaSuccess) return (int)err;
+  if (!slab_collision_ok(fluid_lattice, collision) || !(tau > 0.5) || !(tau_c > 0.5))
+    return (int)cudaErrorInvalidValue;
+  const size_t real = precision == LBM_DOUBLE ? 8 : 4;
+  const size_t fq = fluid_lattice == kD3Q19 ? 19 : 27;
+  const size_t fb = fq * g.plane * real, sb = 7 * g.plane * real, ub = 3 * g.plane * real;
+  const size_t hb = lbm_fluid_reaction_slab_face_elems(fluid_lattice, x_extent, y_extent) * real;
+  const Span reads[5] = {{current_fluid, fb}, {current_a, sb}, {current_b, sb}, {halo_lo, hb},
+                         {halo_hi, hb}};
+  const Span writes[6] = {{next_fluid, fb}, {next_a, sb},   {next_b, sb},
+                          {send_lo, hb},    {send_hi, hb},  {velocity, velocity ? ub : 0}};
+  if (any_overlap(reads, writes)) return (int)cudaErrorInvalidValue;
+  const cudaStream_t s = as_stream(stream);
+  // the relaxation rates as the whole-box gradient forms them
+  LBCUBE_SLAB_DISPATCH(return (int)fluid_reaction_slab_with_velocity<FL, R>(
+      collision, (const R*)current_fluid, (R*)next_fluid, (const R*)current_a, (R*)next_a,
+      (const R*)current_b, (R*)next_b, (R*)velocity, g, R(1) / R(tau), R(1) / R(tau_c), R(k_react),
+      (const R*)halo_lo, (const R*)halo_hi, (R*)send_lo, (R*)send_hi, s))
+}
+
+extern "C" int lbm_reactive_slab_adjoint_step_async(
+    int fluid_lattice, int precision, int collision, const void* fluid_n, const void* a_n,
+    const void* b_n, const void* halo_lo, const void* halo_hi, const void* velocity_next,
+    const void* lambda_fluid_next, const void* lambda_a_next, const void* lambda_b_next,
+    void* lambda_fluid, void* lambda_a, void* lambda_b, void* velocity_adjoint, void* send_lo,
+    void* send_hi, size_t x_extent, size_t y_extent, size_t z_extent, double tau, double tau_c,
+    double k_react, double* slots, size_t slots_bytes, void* stream) {
+  Grid g;
+  cudaError_t err = slab_domain(
+      fluid_lattice, precision,
+      fluid_n == nullptr || a_n == nullptr || b_n == nullptr || halo_lo == nullptr ||
+          halo_hi == nullptr || velocity_next == nullptr || lambda_fluid_next == nullptr ||
+          lambda_a_next == nullptr || lambda_b_next == nullptr || lambda_fluid == nullptr ||
+          lambda_a == nullptr || lambda_b == nullptr || velocity_adjoint == nullptr ||
+          send_lo == nullptr || send_hi == nullptr || slots == nullptr,
+      x_extent, y_extent, z_extent, g);
+  if (err != cudaSuccess) return (int)err;
+  if (!slab_collision_ok(fluid_lattice, collision) || !(tau > 0.5) || !(tau_c > 0.5) ||
+      slots_bytes < slab_slots_bytes(g))
+    return (int)cudaErrorInvalidValue;
+  const cudaStream_t s = as_stream(stream);
+  LBCUBE_SLAB_DISPATCH(return (int)slab_adjoint_step<FL, R>(
+      collision, (const R*)fluid_n, (const R*)a_n, (const R*)b_n, (const R*)halo_lo,
+      (const R*)halo_hi, (const R*)velocity_next, (const R*)lambda_fluid_next,
+      (const R*)lambda_a_next, (const R*)lambda_b_next, (R*)lambda_fluid, (R*)lambda_a,
+      (R*)lambda_b, (R*)velocity_adjoint, (R*)send_lo, (R*)send_hi, g, tau, tau_c, k_react, slots,
+      s))
+}
+
+extern "C" int lbm_reactive_slab_adjoint_unpack_async(int fluid_lattice, int precision,
+                                                      const void* recv_lo, const void* recv_hi,
+                                                      void* lambda_fluid, void* lambda_a,
+                                                      void* lambda_b, size_t x_extent,
+                                                      size_t y_extent, size_t z_extent,
+                                                      void* stream) {
+  Grid g;
+  cudaError_t err = slab_domain(fluid_lattice, precision,
+                                recv_lo == nullptr || recv_hi == nullptr ||
+                                    lambda_fluid == nullptr || lambda_a == nullptr ||
+                                    lambda_b == nullptr,
+                                x_extent, y_extent, z_extent, g);
+  if (err != cudaSuccess) return (int)err;
+  const size_t real = precision == LBM_DOUBLE ? 8 : 4;
+  const size_t fq = fluid_lattice == kD3Q19 ? 19 : 27;
+  const size_t hb = lbm_fluid_reaction_slab_face_elems(fluid_lattice, x_extent, y_extent) * real;
+  const Span reads[2] = {{recv_lo, hb}, {recv_hi, hb}};
+  const Span writes[3] = {{lambda_fluid, fq * g.plane * real},
+                          {lambda_a, 7 * g.plane * real},
+                          {lambda_b, 7 * g.plane * real}};
+  if (any_overlap(reads, writes)) return (int)cudaErrorInvalidValue;
+  const cudaStream_t s = as_stream(stream);
+  const long long total = 2LL * g.ny * g.nx;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+  LBCUBE_SLAB_DISPATCH(reactive_slab_unpack_kernel<FL, R><<<blocks, 256, 0, s>>>(
+                           (const R*)recv_lo, (const R*)recv_hi, (R*)lambda_fluid, (R*)lambda_a,
+                           (R*)lambda_b, g);
+                       return (int)cudaGetLastError())
+}
+
+extern "C" int lbm_reactive_slab_seed_async(int fluid_lattice, int precision, int objective,
+                                            const void* a_final, const void* b_final,
+                                            const void* a0, const double* diagnostics,
+                                            void* lambda_fluid, void* lambda_a, void* lambda_b,
+                                            size_t x_extent, size_t y_extent, size_t z_extent,
+                                            double total_cells, double* objective_partials,
+                                            size_t partials_bytes, void* stream) {
+  Grid g;
+  cudaError_t err = slab_domain(
+      fluid_lattice, precision,
+      a_final == nullptr || b_final == nullptr || a0 == nullptr || lambda_fluid == nullptr ||
+          lambda_a == nullptr || lambda_b == nullptr || objective_partials == nullptr ||
+          (objective == LBM_OBJECTIVE_SEGREGATION && diagnostics == nullptr),
+      x_extent, y_extent, z_extent, g);
+  if (err != cudaSuccess) return (int)err;
+  if ((objective != LBM_OBJECTIVE_MEAN_PRODUCT && objective != LBM_OBJECTIVE_SEGREGATION) ||
+      !(total_cells >= (double)g.plane) || partials_bytes < (size_t)g.blocks() * sizeof(double))
+    return (int)cudaErrorInvalidValue;
+  const cudaStream_t s = as_stream(stream);
+  const double inv_n = 1.0 / total_cells;
+#define LBCUBE_SEED(OBJ)                                                                           \
+  reactive_seed_kernel<FL, R, OBJ, NativeState<R>><<<grid_dims(g), block_dims(g), 0, s>>>(         \
+      (const R*)a_final, (const R*)b_final, (const R*)a0, diagnostics, (R*)lambda_fluid,           \
+      (R*)lambda_a, (R*)lambda_b, g, 0.0f, inv_n, objective_partials)
+  LBCUBE_SLAB_DISPATCH(if (objective == LBM_OBJECTIVE_SEGREGATION) LBCUBE_SEED(LBM_OBJECTIVE_SEGREGATION);
+                       else LBCUBE_SEED(LBM_OBJECTIVE_MEAN_PRODUCT);
+                       return (int)cudaGetLastError())
+#undef LBCUBE_SEED
+}
+
+extern "C" int lbm_reactive_slab_init_gradients_async(
+    int fluid_lattice, int precision, int objective, const void* rho0, const void* u0,
+    const void* a0, const void* b0, const void* lambda_fluid, const void* lambda_a,
+    const void* lambda_b, size_t x_extent, size_t y_extent, size_t z_extent, double total_cells,
+    void* grad_a0, void* grad_b0, void* grad_u0, void* stream) {
+  Grid g;
+  cudaError_t err = slab_domain(fluid_lattice, precision,
+                                u0 == nullptr || lambda_a == nullptr || grad_a0 == nullptr ||
+                                    (grad_b0 != nullptr && lambda_b == nullptr) ||
+                                    (grad_u0 != nullptr &&
+                                     (rho0 == nullptr || a0 == nullptr || b0 == nullptr ||
+                                      lambda_fluid == nullptr || lambda_b == nullptr)),
+                                x_extent, y_extent, z_extent, g);
+  if (err != cudaSuccess) return (int)err;
+  if ((objective != LBM_OBJECTIVE_MEAN_PRODUCT && objective != LBM_OBJECTIVE_SEGREGATION) ||
+      !(total_cells >= (double)g.plane))
+    return (int)cudaErrorInvalidValue;
+  const cudaStream_t s = as_stream(stream);
+  LBCUBE_SLAB_DISPATCH(
+      const R direct = objective == LBM_OBJECTIVE_MEAN_PRODUCT ? R(1.0 / total_cells) : R(0);
+      scalar_init_gradient_kernel<FL, R><<<grid_dims(g), block_dims(g), 0, s>>>(
+          (const R*)u0, (const R*)lambda_a, direct, (R*)grad_a0, g);
+      if (grad_b0 != nullptr) scalar_init_gradient_kernel<FL, R><<<grid_dims(g), block_dims(g), 0, s>>>(
+          (const R*)u0, (const R*)lambda_b, R(0), (R*)grad_b0, g);
+      if (grad_u0 != nullptr) reactive_velocity_gradient_kernel<FL, R><<<grid_dims(g), block_dims(g), 0, s>>>(
+          (const R*)rho0, (const R*)u0, (const R*)a0, (const R*)b0, (const R*)lambda_fluid,
+          (const R*)lambda_a, (const R*)lambda_b, (R*)grad_u0, g);
+      return (int)cudaGetLastError())
+}
+
+extern "C" int lbm_reactive_slab_sums_async(int fluid_lattice, size_t x_extent, size_t y_extent,
+                                            size_t z_extent, const double* slots,
+                                            size_t slots_bytes, const double* objective_partials,
+                                            size_t partials_bytes, double* sums, void* stream) {
+  Grid g;
+  cudaError_t err = slab_domain(fluid_lattice, LBM_DOUBLE,
+                                slots == nullptr || objective_partials == nullptr || sums == nullptr,
+                                x_extent, y_extent, z_extent, g);
+  if (err != cudaSuccess) return (int)err;
+  if (slots_bytes < slab_slots_bytes(g) || partials_bytes < (size_t)g.blocks() * sizeof(double))
+    return (int)cudaErrorInvalidValue;
+  const cudaStream_t s = as_stream(stream);
+  const long long nslots = g.blocks() * kWarpsPerBlock;
+  sum_slots_kernel<<<1, 1024, 0, s>>>(objective_partials, g.blocks(), 1, 1.0, sums);
+  for (int k = 0; k < kReactiveSlots; ++k)
+    sum_slots_kernel<<<1, 1024, 0, s>>>(slots + k, nslots, kReactiveSlots, 1.0, sums + 1 + k);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int lbm_reactive_slab_result_async(int precision, int objective, const double* sums,
+                                              const double* diagnostics, double total_cells,
+                                              double tau_c, double* result, void* stream) {
+  if (sums == nullptr || result == nullptr ||
+      (objective == LBM_OBJECTIVE_SEGREGATION && diagnostics == nullptr))
+    return (int)cudaErrorInvalidDevicePointer;
+  if ((precision != LBM_FLOAT && precision != LBM_DOUBLE) ||
+      (objective != LBM_OBJECTIVE_MEAN_PRODUCT && objective != LBM_OBJECTIVE_SEGREGATION) ||
+      !(total_cells >= 1.0) || !(tau_c > 0.5))
+    return (int)cudaErrorInvalidValue;
+  const double omega_c = precision == LBM_FLOAT ? (double)(1.0f / (float)tau_c) : 1.0 / tau_c;
+  reactive_slab_result_kernel<<<1, 1, 0, as_stream(stream)>>>(sums, diagnostics, objective,
+                                                              1.0 / total_cells, omega_c, result);
+  return (int)cudaGetLastError();
+}
+
+#undef LBCUBE_SLAB_DISPATCH

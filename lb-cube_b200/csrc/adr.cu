@@ -9,6 +9,7 @@
 #include <algorithm>
 
 #include "adr.cuh"
+#include "slab_faces.cuh"
 #include "cells.cuh"
 #include "collide.cuh"
 #include "common.cuh"
@@ -102,72 +103,16 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---- z-slab form of the coupled step ----------------------------------------
-// A rank owns planes [0, nz) of a box cut along z (see slab.cu for the fluid
-// alone). One face buffer per side holds, per crossing population in
-// ascending i, an ny x nx plane: first the fluid's (5 of 19 for D3Q19, 9 of
-// 27 for D3Q27), then species A's and B's (1 of 7 each for D3Q7). Populations
-// with c_z = +1 at plane 0 are pulled from halo_lo (the lower neighbour's
-// top-plane sends), c_z = -1 at plane nz - 1 from halo_hi; the populations
-// leaving through a face are also stored into send_lo / send_hi. Every cell
+// Face layout and the halo gather / face sends: slab_faces.cuh. Every cell
 // does the arithmetic of fluid_reaction_kernel, so a box stepped as slabs is
 // bit-identical to the box stepped whole.
-template <class L>
-__host__ __device__ constexpr int face_planes() {
-  return zcount_of<L>();
-}
-template <class FL>
-__host__ __device__ constexpr int coupled_face_planes() {
-  using SL = typename ScalarOf<FL>::type;
-  return face_planes<FL>() + 2 * face_planes<SL>();
-}
-
-// Pull-gather with the slab's halos in place of the periodic z wrap.
-template <class L, class Real>
-__device__ __forceinline__ void gather_slab(const Real* __restrict__ cur, const Grid& g,
-                                            const Neighbours& n, int x, int y, int z,
-                                            const Real* __restrict__ halo_lo,
-                                            const Real* __restrict__ halo_hi, Real (&f)[L::Q]) {
-  const size_t plane = (size_t)g.plane;
-  const size_t n2 = (size_t)g.ny * g.nx;
-  static_for<L::Q>([&](auto I) {
-    constexpr int i = LB_I(I);
-    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
-    const int sx = cx == 0 ? x : (cx > 0 ? n.xm : n.xp);
-    const int sy = cy == 0 ? y : (cy > 0 ? n.ym : n.yp);
-    const size_t row = (size_t)sy * g.nx + sx;
-    if constexpr (cz > 0) {
-      f[i] = z == 0 ? __ldg(halo_lo + zslot_of<L>(i) * n2 + row)
-                    : __ldg(cur + plane * i + (size_t)(z - 1) * n2 + row);
-    } else if constexpr (cz < 0) {
-      f[i] = z == g.nz - 1 ? __ldg(halo_hi + zslot_of<L>(i) * n2 + row)
-                           : __ldg(cur + plane * i + (size_t)(z + 1) * n2 + row);
-    } else {
-      f[i] = __ldg(cur + plane * i + (size_t)z * n2 + row);
-    }
-  });
-}
-
-// Stores the populations of a face cell that leave the slab.
-template <class L, class Real>
-__device__ __forceinline__ void send_slab(const Grid& g, int x, int y, int z, const Real (&f)[L::Q],
-                                          Real* __restrict__ send_lo, Real* __restrict__ send_hi) {
-  const size_t n2 = (size_t)g.ny * g.nx;
-  const size_t row = (size_t)y * g.nx + x;
-  static_for<L::Q>([&](auto I) {
-    constexpr int i = LB_I(I);
-    constexpr int cz = L::c[i][2];
-    if constexpr (cz > 0) {
-      if (z == g.nz - 1) send_hi[zslot_of<L>(i) * n2 + row] = f[i];
-    } else if constexpr (cz < 0) {
-      if (z == 0) send_lo[zslot_of<L>(i) * n2 + row] = f[i];
-    }
-  });
-}
 
 // Launch over planes [g.z0, g.z0 + gridDim.y); statistics partials indexed by
 // the absolute plane, so a step split into several plane ranges writes every
 // block's partial once.
-template <class FL, class Real, int CT, bool STATS>
+// UOUT: also store the advecting velocity (the reactive adjoint keeps it with
+// each stored state).
+template <class FL, class Real, int CT, bool STATS, bool UOUT = false>
 __global__ void __launch_bounds__(kThreads)
     fluid_reaction_slab_kernel(const Real* __restrict__ cur_f, Real* __restrict__ nxt_f,
                                const Real* __restrict__ cur_a, Real* __restrict__ nxt_a,
@@ -175,7 +120,7 @@ __global__ void __launch_bounds__(kThreads)
                                Real omega, Real omega_minus, Real omega_c, Real k,
                                const Real* __restrict__ halo_lo, const Real* __restrict__ halo_hi,
                                Real* __restrict__ send_lo, Real* __restrict__ send_hi,
-                               double* __restrict__ partials) {
+                               double* __restrict__ partials, Real* __restrict__ u_out = nullptr) {
   using SL = typename ScalarOf<FL>::type;
   const size_t n2 = (size_t)g.ny * g.nx;
   const size_t a_off = (size_t)face_planes<FL>() * n2;
@@ -192,6 +137,9 @@ __global__ void __launch_bounds__(kThreads)
     store_cell<FL>(nxt_f, g, cell, f);
     send_slab<FL>(g, x, y, z, f, send_lo, send_hi);
     fluid_velocity<FL>(f, u);
+    if constexpr (UOUT) {
+      static_for<FL::D>([&](auto D) { u_out[(size_t)g.plane * LB_I(D) + cell] = u[LB_I(D)]; });
+    }
     Real a[SL::Q], b[SL::Q];
     gather_slab<SL>(cur_a, g, n, x, y, z, halo_lo + a_off, halo_hi + a_off, a);
     gather_slab<SL>(cur_b, g, n, x, y, z, halo_lo + b_off, halo_hi + b_off, b);
@@ -415,6 +363,48 @@ cudaError_t fluid_reaction_with_velocity(int collision, const Real* cur_f, Real*
   }
   return cudaGetLastError();
 }
+
+// The slab form of fluid_reaction_with_velocity (all planes of the slab, no
+// statistics; u_out may be null): for the decomposed reactive adjoint. Buffers
+// are checked by the caller.
+template <class FL, class Real>
+cudaError_t fluid_reaction_slab_with_velocity(int collision, const Real* cur_f, Real* nxt_f,
+                                              const Real* cur_a, Real* nxt_a, const Real* cur_b,
+                                              Real* nxt_b, Real* u_out, const Grid& g, Real omega,
+                                              Real omega_c, Real k, const Real* halo_lo,
+                                              const Real* halo_hi, Real* send_lo, Real* send_hi,
+                                              cudaStream_t s) {
+#define LBCUBE_FRSV(CT, OM)                                                                        \
+  if (u_out != nullptr)                                                                            \
+    fluid_reaction_slab_kernel<FL, Real, CT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(   \
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, OM, omega_c, k, halo_lo, halo_hi,      \
+        send_lo, send_hi, nullptr, u_out);                                                         \
+  else                                                                                             \
+    fluid_reaction_slab_kernel<FL, Real, CT, false><<<grid_dims(g), block_dims(g), 0, s>>>(         \
+        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, OM, omega_c, k, halo_lo, halo_hi,      \
+        send_lo, send_hi, nullptr)
+  if (collision == kBGK) {
+    LBCUBE_FRSV(kBGK, Real(0));
+  } else if (collision == kTRT) {
+    LBCUBE_FRSV(kTRT, trt_omega_minus<Real>(omega));
+  } else if (collision == kMRT) {
+    LBCUBE_FRSV(kMRT, Real(0));
+  } else {
+    return cudaErrorInvalidValue;
+  }
+#undef LBCUBE_FRSV
+  return cudaGetLastError();
+}
+
+#define LBCUBE_FRSV_INST(FL, R)                                                                     \
+  template cudaError_t fluid_reaction_slab_with_velocity<FL, R>(                                   \
+      int, const R*, R*, const R*, R*, const R*, R*, R*, const Grid&, R, R, R, const R*, const R*, \
+      R*, R*, cudaStream_t);
+LBCUBE_FRSV_INST(D3Q19, float)
+LBCUBE_FRSV_INST(D3Q19, double)
+LBCUBE_FRSV_INST(D3Q27, float)
+LBCUBE_FRSV_INST(D3Q27, double)
+#undef LBCUBE_FRSV_INST
 
 #define LBCUBE_FRV(FL, R)                                                                     \
   template cudaError_t fluid_reaction_with_velocity<FL, R>(                                   \

@@ -113,6 +113,19 @@ def _declare(lib):
                                           _sz, d, d, d, _vp, _vp, _vp, _vp, _sz, _sz, _vp, _sz, _vp],
         "lbm_fluid_reaction_slab_pack_async": [C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
         "lbm_reactive_stats_sums_async": [C.c_int, _sz, _sz, _sz, _vp, _sz, _vp, _vp],
+        "lbm_reactive_slab_forward_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz,
+                                            _sz, _sz, d, d, d, _vp, _vp, _vp, _vp, _vp],
+        "lbm_reactive_slab_adjoint_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                                 _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz, d, d, d,
+                                                 _vp, _sz, _vp],
+        "lbm_reactive_slab_adjoint_unpack_async": [C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz,
+                                                   _vp],
+        "lbm_reactive_slab_seed_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz,
+                                         _sz, d, _vp, _sz, _vp],
+        "lbm_reactive_slab_init_gradients_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                                   _sz, _sz, _sz, d, _vp, _vp, _vp, _vp],
+        "lbm_reactive_slab_sums_async": [C.c_int, _sz, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _vp],
+        "lbm_reactive_slab_result_async": [C.c_int, C.c_int, _vp, _vp, d, d, _vp, _vp],
         "lbm_reactive_stats_append_async": [C.c_int, C.c_int, _sz, _sz, _sz, d, _vp, _sz, _vp, _sz, _vp, _vp],
         "lbm_reactive_stats_from_sums_async": [C.c_int, _vp, d, d, _vp, _vp],
         "lbm_macro_fields_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp, _vp],
@@ -140,6 +153,9 @@ def _declare(lib):
     lib.lbm_diagnostics_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
     lib.lbm_ke_gradient_workspace_bytes.restype = C.c_size_t
     lib.lbm_ke_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, _sz, _sz, _sz, C.c_int, C.c_int]
+    for name in ("lbm_reactive_slab_slots_bytes", "lbm_reactive_slab_objective_bytes"):
+        getattr(lib, name).restype = C.c_size_t
+        getattr(lib, name).argtypes = [C.c_int, _sz, _sz, _sz]
     lib.lbm_stage_timeouts.restype = C.c_uint
     lib.lbm_stage_timeouts.argtypes = [C.c_int]
 

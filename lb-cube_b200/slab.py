@@ -24,6 +24,11 @@ lbm_fluid_reaction_ab_async (one face buffer per side carries the fluid's
 crossing populations and one D3Q7 plane per species), and reduces the
 reactive statistics over ranks: each rank sums its cells into five FP64
 values, an all-reduce adds them, and every rank forms the same diagnostics.
+
+ReactiveSlabGradient runs the checkpointed reactive gradient
+(lbm_reactive_gradient_async) the same way: forward and adjoint steps on each
+slab, face exchanges between them, and an all-reduce of the FP64 statistics and
+gradient sums.
 """
 from __future__ import annotations
 
@@ -186,6 +191,228 @@ class ReactiveSlabDomain(SlabDomain):
                 dist.all_reduce(sums, op=dist.ReduceOp.SUM, group=group)
         return diagnostics_from_sums(self.torch, self.real, sums, self.nx * self.ny * self.nz * self.world,
                                      self.k, stream)
+
+
+class ReactiveSlabGradient(ReactiveSlabDomain):
+    """The checkpointed gradient of lbm_reactive_gradient_async on one rank's
+    slab: J and dJ/dk, dJ/dtau, dJ/dtau_c of the whole box, and dJ/dA0,
+    dJ/dB0, dJ/du0 on the rank's planes (native FP32 / FP64 states).
+
+    The whole-box host sequence (adjoint_reactive.cu: reactive_gradient) runs
+    on every rank with the slab entries of the C ABI; sequence() yields where
+    the ranks meet: ("exchange",) for a face exchange (send -> halo buffers,
+    as the forward step's), ("allreduce", t) for an in-place sum of the FP64
+    device tensor t over ranks. run() serves those yields for one rank of a
+    process group; run_local() steps the slabs of one process in lockstep.
+    Per forward step one exchange; per adjoint step two (the stored state's
+    faces for the pulls, then the adjoint scatter's sends) and an unpack of the
+    received scatter faces. Given the same seed the adjoint fields and the
+    initial-state gradients are bit-identical to the whole box's."""
+
+    def __init__(self, torch, lattice, real, collision, objective, nx, ny, nz_global, tau, tau_c, k, steps, interval,
+                 rank, world, device):
+        super().__init__(torch, lattice, real, collision, nx, ny, nz_global, 1.0 / tau, 1.0 / tau_c, k, rank, world,
+                         device)
+        if steps < 1 or interval < 2:
+            raise ValueError("need steps >= 1 and a checkpoint interval >= 2")
+        self.objective = objective
+        self.tau, self.tau_c = float(tau), float(tau_c)
+        self.steps, self.interval = int(steps), int(interval)
+        self.total_cells = float(nx * ny * nz_global)
+        dtype = torch.float32 if real == "float" else torch.float64
+        q = Q_OF[lattice]
+        shape = (self.nz, ny, nx)
+        self._dtype, self._device = dtype, device
+
+        def field(qq):
+            return torch.empty((qq,) + shape, dtype=dtype, device=device)
+
+        def state():
+            return (field(q), field(7), field(7), field(3))
+
+        nseg = (self.steps + self.interval - 1) // self.interval
+        self.nseg = nseg
+        self.ckpt = [state() for _ in range(nseg + 1)]
+        self.seg = [state() for _ in range(self.interval)]
+        self.lam = [(field(q), field(7), field(7)) for _ in range(2)]
+        self.ubar = field(3)
+        lib = E.load()
+        L = E.LATTICES[lattice]
+        self.slots_bytes = lib.lbm_reactive_slab_slots_bytes(L, nx, ny, self.nz)
+        self.obj_bytes = lib.lbm_reactive_slab_objective_bytes(L, nx, ny, self.nz)
+        if self.slots_bytes == 0 or self.obj_bytes == 0:
+            raise ValueError("slab extents rejected by the engine")
+        self.slots = torch.empty(self.slots_bytes // 8, dtype=torch.float64, device=device)
+        self.obj_partials = torch.empty(self.obj_bytes // 8, dtype=torch.float64, device=device)
+        self.diag = torch.zeros(8, dtype=torch.float64, device=device)
+        self.sums = torch.empty(4, dtype=torch.float64, device=device)
+        self.result = torch.empty(4, dtype=torch.float64, device=device)
+
+    # ---- the per-step entries
+    def _forward(self, cur, nxt, keep_u, stream=None):
+        E.check(E.load().lbm_reactive_slab_forward_async(
+            E.LATTICES[self.lattice], E.REALS[self.real], E.COLLISIONS[self.collision], cur[0].data_ptr(),
+            nxt[0].data_ptr(), cur[1].data_ptr(), nxt[1].data_ptr(), cur[2].data_ptr(), nxt[2].data_ptr(),
+            nxt[3].data_ptr() if keep_u else None, self.nx, self.ny, self.nz, self.tau, self.tau_c, self.k,
+            self.halo_lo.data_ptr(), self.halo_hi.data_ptr(), self.send_lo.data_ptr(), self.send_hi.data_ptr(),
+            E._stream(stream)), "reactive slab forward step")
+
+    def _adjoint(self, sn, u_next, ln, l, stream=None):
+        E.check(E.load().lbm_reactive_slab_adjoint_step_async(
+            E.LATTICES[self.lattice], E.REALS[self.real], E.COLLISIONS[self.collision], sn[0].data_ptr(),
+            sn[1].data_ptr(), sn[2].data_ptr(), self.halo_lo.data_ptr(), self.halo_hi.data_ptr(),
+            u_next.data_ptr(), ln[0].data_ptr(), ln[1].data_ptr(), ln[2].data_ptr(), l[0].data_ptr(),
+            l[1].data_ptr(), l[2].data_ptr(), self.ubar.data_ptr(), self.send_lo.data_ptr(),
+            self.send_hi.data_ptr(), self.nx, self.ny, self.nz, self.tau, self.tau_c, self.k, self.slots.data_ptr(),
+            self.slots_bytes, E._stream(stream)), "reactive slab adjoint step")
+
+    def _unpack(self, l, stream=None):
+        E.check(E.load().lbm_reactive_slab_adjoint_unpack_async(
+            E.LATTICES[self.lattice], E.REALS[self.real], self.halo_lo.data_ptr(), self.halo_hi.data_ptr(),
+            l[0].data_ptr(), l[1].data_ptr(), l[2].data_ptr(), self.nx, self.ny, self.nz, E._stream(stream)),
+            "reactive slab adjoint unpack")
+
+    def sequence(self, rho0, u0, a0, b0, grad_b0=True, grad_u0=True):
+        """Generator of one rank's gradient (inputs: this rank's planes of
+        rho0 [Z,Y,X], u0 [3,Z,Y,X], a0, b0 [Z,Y,X] on the device). Afterwards
+        self.result holds J, dJ/dk, dJ/dtau, dJ/dtau_c and self.grad_a0 (and
+        grad_b0, grad_u0 when asked) this rank's initial-state gradients."""
+        torch, lib = self.torch, E.load()
+        L, P = E.LATTICES[self.lattice], E.REALS[self.real]
+        SL = E.LATTICES["D3Q7"]
+        nx, ny, nz = self.nx, self.ny, self.nz
+        steps, interval, nseg = self.steps, self.interval, self.nseg
+        ckpt, seg = self.ckpt, self.seg
+        for t in (rho0, a0, b0):
+            assert tuple(t.shape) == (nz, ny, nx) and t.dtype == self._dtype and t.is_contiguous()
+        assert tuple(u0.shape) == (3, nz, ny, nx) and u0.dtype == self._dtype and u0.is_contiguous()
+
+        # forward: the equilibrium initial state, checkpoints every `interval`
+        # steps, the last segment's states kept
+        s0 = ckpt[0]
+        E.check(lib.lbm_init_equilibrium_async(L, P, rho0.data_ptr(), u0.data_ptr(), s0[0].data_ptr(), nx, ny, nz,
+                                               None), "init")
+        E.check(lib.lbm_init_equilibrium_async(SL, P, a0.data_ptr(), u0.data_ptr(), s0[1].data_ptr(), nx, ny, nz,
+                                               None), "init")
+        E.check(lib.lbm_init_equilibrium_async(SL, P, b0.data_ptr(), u0.data_ptr(), s0[2].data_ptr(), nx, ny, nz,
+                                               None), "init")
+        self.pack(s0[:3])
+        yield ("exchange",)
+        last0 = (nseg - 1) * interval
+        cur = s0
+        for n in range(steps):
+            kept = True
+            if n + 1 == steps or (n + 1) % interval == 0:
+                nxt = ckpt[(n + interval) // interval]
+            elif n + 1 > last0:
+                nxt = seg[n + 1 - last0]
+            else:
+                nxt, kept = seg[n % 2], False
+            self._forward(cur, nxt, kept)
+            if n + 1 < steps:
+                yield ("exchange",)
+            cur = nxt
+
+        # seed lambda^N (and the objective partials)
+        lN = self.lam[steps % 2]
+        if self.objective == "segregation":
+            scratch = torch.empty(8, dtype=torch.float64, device=self._device)
+            E.check(lib.lbm_reactive_stats_async(SL, P, cur[1].data_ptr(), cur[2].data_ptr(), nx, ny, nz, self.k,
+                                                 self.partials.data_ptr(), self.partials_bytes, scratch.data_ptr(),
+                                                 None), "statistics")
+            sums5 = self.rank_sums()
+            yield ("allreduce", sums5)
+            E.check(lib.lbm_reactive_stats_from_sums_async(P, sums5.data_ptr(), self.total_cells, self.k,
+                                                           self.diag.data_ptr(), None), "statistics")
+        obj = E.OBJECTIVES[self.objective]
+        E.check(lib.lbm_reactive_slab_seed_async(
+            L, P, obj, cur[1].data_ptr(), cur[2].data_ptr(), a0.data_ptr(), self.diag.data_ptr(), lN[0].data_ptr(),
+            lN[1].data_ptr(), lN[2].data_ptr(), nx, ny, nz, self.total_cells, self.obj_partials.data_ptr(),
+            self.obj_bytes, None), "reactive slab seed")
+        self.slots.zero_()
+
+        # backward sweep, segment by segment from the last
+        for kk in range(nseg - 1, -1, -1):
+            n0, n1 = kk * interval, min(steps, (kk + 1) * interval)
+            if kk < nseg - 1 and n1 - n0 > 1:  # recompute the segment's states from its checkpoint
+                src = ckpt[kk]
+                self.pack(src[:3])
+                yield ("exchange",)
+                for n in range(n0 + 1, n1):
+                    self._forward(src, seg[n - n0], True)
+                    if n + 1 < n1:
+                        yield ("exchange",)
+                    src = seg[n - n0]
+            for n in range(n1 - 1, n0 - 1, -1):
+                sn = ckpt[kk] if n == n0 else seg[n - n0]
+                sn1 = ckpt[kk + 1] if n + 1 == n1 else seg[n + 1 - n0]  # holds u^{n+1}
+                ln, l = self.lam[(n + 1) % 2], self.lam[n % 2]
+                self.pack(sn[:3])
+                yield ("exchange",)
+                self._adjoint(sn, sn1[3], ln, l)
+                yield ("exchange",)
+                self._unpack(l)
+
+        # initial-state gradients and the four scalars
+        l0 = self.lam[0]
+        self.grad_a0 = torch.empty((nz, ny, nx), dtype=self._dtype, device=self._device)
+        self.grad_b0 = torch.empty_like(self.grad_a0) if grad_b0 else None
+        self.grad_u0 = torch.empty((3, nz, ny, nx), dtype=self._dtype, device=self._device) if grad_u0 else None
+        E.check(lib.lbm_reactive_slab_init_gradients_async(
+            L, P, obj, rho0.data_ptr(), u0.data_ptr(), a0.data_ptr(), b0.data_ptr(), l0[0].data_ptr(),
+            l0[1].data_ptr(), l0[2].data_ptr(), nx, ny, nz, self.total_cells, self.grad_a0.data_ptr(),
+            None if self.grad_b0 is None else self.grad_b0.data_ptr(),
+            None if self.grad_u0 is None else self.grad_u0.data_ptr(), None), "reactive slab gradients")
+        E.check(lib.lbm_reactive_slab_sums_async(L, nx, ny, nz, self.slots.data_ptr(), self.slots_bytes,
+                                                 self.obj_partials.data_ptr(), self.obj_bytes, self.sums.data_ptr(),
+                                                 None), "reactive slab sums")
+        yield ("allreduce", self.sums)
+        E.check(lib.lbm_reactive_slab_result_async(P, obj, self.sums.data_ptr(), self.diag.data_ptr(),
+                                                   self.total_cells, self.tau_c, self.result.data_ptr(), None),
+                "reactive slab result")
+
+    def run(self, rho0, u0, a0, b0, exchange, dist=None, group=None, grad_b0=True, grad_u0=True):
+        """One rank of a process group (exchange: HostExchange or
+        DistributedExchange). Returns (result, grad_a0, grad_b0, grad_u0)."""
+        for op in self.sequence(rho0, u0, a0, b0, grad_b0, grad_u0):
+            if op[0] == "exchange":
+                exchange.exchange(self)
+            else:
+                _all_reduce(dist, group, op[1], self.world)
+        return self.result, self.grad_a0, self.grad_b0, self.grad_u0
+
+
+def _all_reduce(dist, group, t, world):
+    if world == 1:
+        return
+    if dist.get_backend(group) == "gloo" and t.is_cuda:
+        host = t.cpu()
+        dist.all_reduce(host, op=dist.ReduceOp.SUM, group=group)
+        t.copy_(host)
+    else:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+
+
+def run_local(gradients, inputs, grad_b0=True, grad_u0=True):
+    """The slabs of one process (every rank of the box), stepped in lockstep:
+    LocalExchange for the exchanges, sums in rank order for the all-reduces.
+    inputs[r] = (rho0, u0, a0, b0) of rank r's planes."""
+    gens = [g.sequence(*inp, grad_b0=grad_b0, grad_u0=grad_u0) for g, inp in zip(gradients, inputs)]
+    ex = LocalExchange(gradients)
+    while True:
+        ops = [next(gen, None) for gen in gens]
+        if all(op is None for op in ops):
+            break
+        if any(op is None for op in ops) or len({op[0] for op in ops}) != 1:
+            raise RuntimeError("slab ranks left the lockstep")
+        if ops[0][0] == "exchange":
+            ex.exchange_all()
+        else:
+            total = ops[0][1].clone()
+            for op in ops[1:]:
+                total += op[1]
+            for op in ops:
+                op[1].copy_(total)
 
 
 def diagnostics_from_sums(torch, real, sums, cells, k, stream=None):

@@ -6,7 +6,10 @@ lbm_fluid_reaction_slab_async for the coupled fluid + A + B -> C step);
 HostExchange moves the face buffers between them through host memory, so no
 kernel ever waits on the other rank. The assembled slabs must be bit-identical
 to the whole box stepped in this process, and the reactive statistics
-all-reduced over the two ranks must equal the whole box's to 1e-12. (This
+all-reduced over the two ranks must equal the whole box's to 1e-12; the
+reactive gradient run as two slabs (slab.ReactiveSlabGradient.run) must give
+the whole box's initial-state gradients bit for bit and its four scalars to
+1e-10. (This
 runs on one GPU; across GPUs the same host code moves the faces with NCCL,
 slab.DistributedExchange.)
 """
@@ -65,7 +68,20 @@ def _worker(rank, port, case, q):
         f, a, b = _states(lat, dt)
         q_f = E.Q_OF[lat]
         ex = slab.HostExchange(dist)
-        if op.startswith("coupled-"):
+        if op.startswith("adjoint-"):  # the reactive gradient: (result, dJ/dA0, dJ/dB0, dJ/du0)
+            from test_gpu_adjoint_reactive import fields
+
+            _, cop, obj = op.split("-", 2)
+            rho, u, a0, b0 = fields(lat, (nz, ny, nx), dev, torch.float32 if dn == "float" else torch.float64, 91)
+            g = slab.ReactiveSlabGradient(torch, lat, dn, cop, obj, nx, ny, nz, 0.8, 0.7, 0.6, 7, 3, rank, WORLD,
+                                          dev)
+            sl = slice(g.z0, g.z0 + g.nz)
+            res = g.run(rho[sl].contiguous(), u[:, sl].contiguous(), a0[sl].contiguous(), b0[sl].contiguous(),
+                        ex, dist)
+            torch.cuda.synchronize()
+            stats = res[0].cpu().numpy()
+            out = [t.cpu().numpy() for t in res[1:]]
+        elif op.startswith("coupled-"):
             d = slab.ReactiveSlabDomain(torch, lat, dn, op[8:], nx, ny, nz, OMEGA, OMEGA_C, K, rank, WORLD, dev)
 
             def mine(x, qq):
@@ -167,3 +183,19 @@ def test_coupled_slabs_in_two_processes(engine, dev, lat, dn, op):
     w = want_stats.cpu().numpy()
     for rank, _, stats, _ in res:
         assert np.all(np.abs(stats - w) <= 1e-12 * np.maximum(np.abs(w), 1e-300)), (rank, stats, w)
+
+
+@pytest.mark.parametrize("lat,dn,op", [("D3Q19", "double", "TRT"), ("D3Q27", "float", "BGK")])
+def test_reactive_gradient_slabs_in_two_processes(engine, dev, lat, dn, op):
+    from test_gpu_slab_adjoint import whole_box
+    from test_gpu_adjoint_reactive import fields
+
+    nx, ny, nz = DIMS
+    rho, u, a0, b0 = fields(lat, (nz, ny, nx), dev, torch.float32 if dn == "float" else torch.float64, 91)
+    want = whole_box(lat, dn, op, "mean_product", rho, u, a0, b0, DIMS, 7, 3)
+    res = _run((lat, dn, f"adjoint-{op}-mean_product", False))
+    for rank, _, result, _ in res:
+        assert np.all(np.abs(result - want[0]) <= 1e-10 * np.abs(want[0])), (rank, result, want[0])
+    for idx, axis in ((0, 0), (1, 0), (2, 1)):
+        got = np.concatenate([r[1][idx] for r in res], axis=axis)
+        assert U.same_bits(got, want[1 + idx]), ("dJ/dA0", "dJ/dB0", "dJ/du0")[idx]
