@@ -546,15 +546,21 @@ int lbm_fluid_reaction_slab_pack_async(int fluid_lattice, int precision, const v
     void* send_lo, void* send_hi, void* stream);
 
 /* The gradient of lbm_reactive_gradient_async on a z-slab (no reference
- * counterpart): native FP32 / FP64 states, D3Q19 (BGK, TRT, MRT) or D3Q27
- * (BGK, TRT) fluid with two D3Q7 species. Every rank runs the whole-box
- * sequence on its slab (z_extent = its own planes, total_cells = cells of the
- * whole box); the face buffers have the layout above, and each exchange moves
- * send_hi(r) into halo_lo(r + 1) and send_lo(r) into halo_hi(r - 1):
- *   forward step  lbm_reactive_slab_forward_async (velocity, [3, Z, Y, X],
- *                 may be null for states the backward sweep recomputes), then
- *                 an exchange;
- *   adjoint step  n (state n and u^{n+1} stored): lbm_fluid_reaction_slab_pack_async
+ * counterpart): D3Q19 (BGK, TRT, MRT) or D3Q27 (BGK, TRT) fluid with two D3Q7
+ * species, states stored as lbm_reactive_gradient_async stores them (storage
+ * LBM_NATIVE: in the precision; a 16-bit format: codes, scalars shifted by c0,
+ * precision LBM_FLOAT). Every rank runs the whole-box sequence on its slab
+ * (z_extent = its own planes, total_cells = cells of the whole box); the face
+ * buffers have the layout above with elements of the stored states (state
+ * faces: forward steps and packs) or of the precision (the adjoint's scatter
+ * sends), and each exchange moves send_hi(r) into halo_lo(r + 1) and send_lo(r)
+ * into halo_hi(r - 1):
+ *   initial state  lbm_init_equilibrium_async (16-bit: in FP32, then
+ *                 lbm_encode_shifted_async, fluid shifted by 1, scalars by c0);
+ *   forward step  lbm_reactive_slab_forward_async (velocity, [3, Z, Y, X] in the
+ *                 precision, may be null for states the backward sweep
+ *                 recomputes), then an exchange;
+ *   adjoint step  n (state n and u^{n+1} stored): lbm_reactive_slab_pack_async
  *                 of state n + exchange (its halos), then
  *                 lbm_reactive_slab_adjoint_step_async (lambda^{n+1} ->
  *                 lambda^n; velocity_adjoint is [3, Z, Y, X] scratch; adds to
@@ -580,13 +586,17 @@ size_t lbm_reactive_slab_slots_bytes(int fluid_lattice, size_t x_extent, size_t 
     size_t z_extent);
 size_t lbm_reactive_slab_objective_bytes(int fluid_lattice, size_t x_extent, size_t y_extent,
     size_t z_extent);
-int lbm_reactive_slab_forward_async(int fluid_lattice, int precision, int collision,
-    const void* current_fluid, void* next_fluid, const void* current_a, void* next_a,
-    const void* current_b, void* next_b, void* velocity, size_t x_extent, size_t y_extent,
-    size_t z_extent, double tau, double tau_c, double k_react, const void* halo_lo,
-    const void* halo_hi, void* send_lo, void* send_hi, void* stream);
-int lbm_reactive_slab_adjoint_step_async(int fluid_lattice, int precision, int collision,
-    const void* fluid_n, const void* a_n, const void* b_n, const void* halo_lo,
+int lbm_reactive_slab_pack_async(int fluid_lattice, int precision, int storage,
+    const void* fluid, const void* a, const void* b, size_t x_extent, size_t y_extent,
+    size_t z_extent, void* send_lo, void* send_hi, void* stream);
+int lbm_reactive_slab_forward_async(int fluid_lattice, int precision, int storage, float c0,
+    int collision, const void* current_fluid, void* next_fluid, const void* current_a,
+    void* next_a, const void* current_b, void* next_b, void* velocity, size_t x_extent,
+    size_t y_extent, size_t z_extent, double tau, double tau_c, double k_react,
+    const void* halo_lo, const void* halo_hi, void* send_lo, void* send_hi, void* stream);
+int lbm_reactive_slab_adjoint_step_async(int fluid_lattice, int precision, int storage,
+    float c0, int collision, const void* fluid_n, const void* a_n, const void* b_n,
+    const void* halo_lo,
     const void* halo_hi, const void* velocity_next, const void* lambda_fluid_next,
     const void* lambda_a_next, const void* lambda_b_next, void* lambda_fluid, void* lambda_a,
     void* lambda_b, void* velocity_adjoint, void* send_lo, void* send_hi, size_t x_extent,
@@ -595,8 +605,8 @@ int lbm_reactive_slab_adjoint_step_async(int fluid_lattice, int precision, int c
 int lbm_reactive_slab_adjoint_unpack_async(int fluid_lattice, int precision,
     const void* recv_lo, const void* recv_hi, void* lambda_fluid, void* lambda_a,
     void* lambda_b, size_t x_extent, size_t y_extent, size_t z_extent, void* stream);
-int lbm_reactive_slab_seed_async(int fluid_lattice, int precision, int objective,
-    const void* a_final, const void* b_final, const void* a0, const double* diagnostics,
+int lbm_reactive_slab_seed_async(int fluid_lattice, int precision, int storage, float c0,
+    int objective, const void* a_final, const void* b_final, const void* a0, const double* diagnostics,
     void* lambda_fluid, void* lambda_a, void* lambda_b, size_t x_extent, size_t y_extent,
     size_t z_extent, double total_cells, double* objective_partials, size_t partials_bytes,
     void* stream);

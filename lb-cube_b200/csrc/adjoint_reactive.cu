@@ -105,6 +105,15 @@ struct NativeState {
                                                float, Real (&out)[L::Q]) {
     load_cell<L>(p, g, cell, out);
   }
+  // the pull on a z-slab, across its faces from halo buffers
+  template <class L>
+  __device__ __forceinline__ static void pulled_slab(const elem* __restrict__ p, const Grid& g,
+                                                     const Neighbours& n, int x, int y, int z, float,
+                                                     const elem* __restrict__ halo_lo,
+                                                     const elem* __restrict__ halo_hi,
+                                                     Real (&out)[L::Q]) {
+    gather_slab<L>(p, g, n, x, y, z, halo_lo, halo_hi, out);
+  }
 };
 template <int FMT>
 struct ShiftedState {
@@ -128,6 +137,18 @@ struct ShiftedState {
       out[LB_I(I)] = ShiftedStorage<FMT>::template decode<L, LB_I(I)>(h[LB_I(I)], {ref});
     });
   }
+  template <class L>
+  __device__ __forceinline__ static void pulled_slab(const elem* __restrict__ p, const Grid& g,
+                                                     const Neighbours& n, int x, int y, int z,
+                                                     float ref, const elem* __restrict__ halo_lo,
+                                                     const elem* __restrict__ halo_hi,
+                                                     float (&out)[L::Q]) {
+    unsigned short h[L::Q];
+    gather_slab<L>(p, g, n, x, y, z, halo_lo, halo_hi, h);
+    static_for<L::Q>([&](auto I) {
+      out[LB_I(I)] = ShiftedStorage<FMT>::template decode<L, LB_I(I)>(h[LB_I(I)], {ref});
+    });
+  }
 };
 
 // FP64 slots of the reactive adjoint, one set per warp (kThreads / 32 per
@@ -138,11 +159,12 @@ constexpr int kReactiveSlots = 3;
 constexpr int kWarpsPerBlock = kThreads / 32;
 
 // The face buffers of a z-slab (slab_faces.cuh): halos of the stored state the
-// step pulls from, and sends of the adjoint scatter. Unused on the whole box.
-template <class Real>
+// step pulls from (its elements: Real or 16-bit codes), and sends of the
+// adjoint scatter (Real). Unused on the whole box.
+template <class E, class Real>
 struct SlabFaces {
-  const Real* halo_lo;
-  const Real* halo_hi;
+  const E* halo_lo;
+  const E* halo_hi;
   Real* send_lo;
   Real* send_hi;
 };
@@ -162,9 +184,8 @@ __global__ void __launch_bounds__(kThreads)
                             const Real* __restrict__ lb_next, Real* __restrict__ la,
                             Real* __restrict__ lb, Real* __restrict__ ubar_out, Grid g,
                             ReactiveParams rp, double* __restrict__ slots,
-                            SlabFaces<Real> faces = {}) {
+                            SlabFaces<typename SP::elem, Real> faces = {}) {
   using SL = typename ScalarOf<FL>::type;
-  static_assert(!SLAB || std::is_same_v<SP, NativeState<Real>>);
   const size_t a_off = (size_t)face_planes<FL>() * g.ny * g.nx;
   const size_t b_off = a_off + (size_t)face_planes<SL>() * g.ny * g.nx;
   int x, y, z;
@@ -178,8 +199,10 @@ __global__ void __launch_bounds__(kThreads)
     static_for<FL::D>([&](auto D) { u[LB_I(D)] = __ldg(u_next + plane * LB_I(D) + cell); });
     Real ga[SL::Q], gb[SL::Q], lA[SL::Q], lB[SL::Q];
     if constexpr (SLAB) {
-      gather_slab<SL>(an, g, n, x, y, z, faces.halo_lo + a_off, faces.halo_hi + a_off, ga);
-      gather_slab<SL>(bn, g, n, x, y, z, faces.halo_lo + b_off, faces.halo_hi + b_off, gb);
+      SP::template pulled_slab<SL>(an, g, n, x, y, z, rp.c0, faces.halo_lo + a_off,
+                                   faces.halo_hi + a_off, ga);
+      SP::template pulled_slab<SL>(bn, g, n, x, y, z, rp.c0, faces.halo_lo + b_off,
+                                   faces.halo_hi + b_off, gb);
     } else {
       SP::template pulled<SL>(an, g, n, x, y, z, rp.c0, ga);
       SP::template pulled<SL>(bn, g, n, x, y, z, rp.c0, gb);
@@ -243,8 +266,8 @@ __global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
     coupled_fluid_adjoint_kernel(const typename SP::elem* __restrict__ fn,
                                  const Real* __restrict__ lf_next, const Real* __restrict__ ubar_in,
                                  Real* __restrict__ lf, Grid g, AdjointParams ap, float rho0,
-                                 double* __restrict__ slots, SlabFaces<Real> faces = {}) {
-  static_assert(!SLAB || std::is_same_v<SP, NativeState<Real>>);
+                                 double* __restrict__ slots,
+                                 SlabFaces<typename SP::elem, Real> faces = {}) {
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double dtau = 0.0;
@@ -253,7 +276,7 @@ __global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
     const int cell = (z * g.ny + y) * g.nx + x;
     const size_t plane = (size_t)g.plane;
     Real gv[FL::Q], lv[FL::Q], mu[FL::Q], rho, u[FL::D], ub[FL::D];
-    if constexpr (SLAB) gather_slab<FL>(fn, g, n, x, y, z, faces.halo_lo, faces.halo_hi, gv);
+    if constexpr (SLAB) SP::template pulled_slab<FL>(fn, g, n, x, y, z, rho0, faces.halo_lo, faces.halo_hi, gv);
     else SP::template pulled<FL>(fn, g, n, x, y, z, rho0, gv);
     load_cell<FL>(lf_next, g, cell, lv);
     static_for<FL::D>([&](auto D) { ub[LB_I(D)] = __ldg(ubar_in + plane * LB_I(D) + cell); });
@@ -777,22 +800,29 @@ inline size_t slab_slots_bytes(const Grid& g) {
   return (size_t)g.blocks() * kWarpsPerBlock * kReactiveSlots * sizeof(double);
 }
 
-template <class FL, class Real>
-cudaError_t slab_adjoint_step(int collision, const Real* fn, const Real* an, const Real* bn,
-                              const Real* halo_lo, const Real* halo_hi, const Real* u_next,
-                              const Real* lf_next, const Real* la_next, const Real* lb_next,
-                              Real* lf, Real* la, Real* lb, Real* ubar, Real* send_lo,
-                              Real* send_hi, const Grid& g, double tau, double tau_c, double k,
-                              double* slots, cudaStream_t s) {
+// One adjoint step on a slab; SP: the stored states' policy (NativeState<Real>
+// or ShiftedState<FMT> with Real float).
+template <class FL, class Real, class SP>
+cudaError_t slab_adjoint_step(int collision, const typename SP::elem* fn,
+                              const typename SP::elem* an, const typename SP::elem* bn,
+                              const typename SP::elem* halo_lo, const typename SP::elem* halo_hi,
+                              const Real* u_next, const Real* lf_next, const Real* la_next,
+                              const Real* lb_next, Real* lf, Real* la, Real* lb, Real* ubar,
+                              Real* send_lo, Real* send_hi, const Grid& g, double tau, double tau_c,
+                              double k, float c0, double* slots, cudaStream_t s) {
   using SL = typename ScalarOf<FL>::type;
-  using SP = NativeState<Real>;
-  const size_t fb = (size_t)FL::Q * g.plane * sizeof(Real);
-  const size_t sb = (size_t)SL::Q * g.plane * sizeof(Real);
+  using E = typename SP::elem;
+  const size_t fe = (size_t)FL::Q * g.plane, se = (size_t)SL::Q * g.plane;
   const size_t ub = (size_t)FL::D * g.plane * sizeof(Real);
-  const size_t hb = (size_t)coupled_face_planes<FL>() * g.ny * g.nx * sizeof(Real);
-  const Span reads[9] = {{fn, fb},      {an, sb},     {bn, sb},      {halo_lo, hb}, {halo_hi, hb},
-                         {u_next, ub},  {lf_next, fb}, {la_next, sb}, {lb_next, sb}};
-  const Span writes[7] = {{lf, fb}, {la, sb}, {lb, sb}, {ubar, ub}, {send_lo, hb}, {send_hi, hb},
+  const size_t he = (size_t)coupled_face_planes<FL>() * g.ny * g.nx;
+  const Span reads[9] = {{fn, fe * sizeof(E)},      {an, se * sizeof(E)},
+                         {bn, se * sizeof(E)},      {halo_lo, he * sizeof(E)},
+                         {halo_hi, he * sizeof(E)}, {u_next, ub},
+                         {lf_next, fe * sizeof(Real)}, {la_next, se * sizeof(Real)},
+                         {lb_next, se * sizeof(Real)}};
+  const Span writes[7] = {{lf, fe * sizeof(Real)},      {la, se * sizeof(Real)},
+                          {lb, se * sizeof(Real)},      {ubar, ub},
+                          {send_lo, he * sizeof(Real)}, {send_hi, he * sizeof(Real)},
                           {slots, slab_slots_bytes(g)}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
   ReactiveParams rp{};
@@ -800,8 +830,8 @@ cudaError_t slab_adjoint_step(int collision, const Real* fn, const Real* an, con
   rp.omega_c = (double)(Real(1) / Real(tau_c));
   rp.k = (double)Real(k);
   rp.rho0 = 1.0f;
-  rp.c0 = 0.0f;
-  const SlabFaces<Real> faces{halo_lo, halo_hi, send_lo, send_hi};
+  rp.c0 = c0;
+  const SlabFaces<E, Real> faces{halo_lo, halo_hi, send_lo, send_hi};
   reaction_adjoint_kernel<FL, Real, SP, true><<<grid_dims(g), block_dims(g), 0, s>>>(
       an, bn, u_next, la_next, lb_next, la, lb, ubar, g, rp, slots, faces);
   if (collision == kBGK)
@@ -817,6 +847,33 @@ cudaError_t slab_adjoint_step(int collision, const Real* fn, const Real* an, con
     return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
+
+// Calls fn(FL{}, Real{}, std::integral_constant<int, FMT>{}) for a slab's
+// fluid lattice, precision and storage (FMT -1: states in Real; a 16-bit
+// format needs Real float).
+template <class F>
+int slab_dispatch(int fluid_lattice, int precision, int storage, F&& fn) {
+  const int fmt = storage_fmt(storage);
+  if (storage != LBM_NATIVE && (fmt < 0 || precision != LBM_FLOAT)) return (int)cudaErrorInvalidValue;
+  auto by_format = [&](auto fl, auto r) -> int {
+    if (fmt < 0) return fn(fl, r, std::integral_constant<int, -1>{});
+    if constexpr (std::is_same_v<decltype(r), float>) {
+      if (fmt == kF16S) return fn(fl, r, std::integral_constant<int, kF16S>{});
+      if (fmt == kBF16S) return fn(fl, r, std::integral_constant<int, kBF16S>{});
+      if (fmt == kE3M12S) return fn(fl, r, std::integral_constant<int, kE3M12S>{});
+      if (fmt == kQ15S) return fn(fl, r, std::integral_constant<int, kQ15S>{});
+    }
+    return (int)cudaErrorInvalidValue;
+  };
+  if (fluid_lattice == kD3Q19 && precision == LBM_FLOAT) return by_format(D3Q19{}, 0.0f);
+  if (fluid_lattice == kD3Q19 && precision == LBM_DOUBLE) return by_format(D3Q19{}, 0.0);
+  if (fluid_lattice == kD3Q27 && precision == LBM_FLOAT) return by_format(D3Q27{}, 0.0f);
+  if (fluid_lattice == kD3Q27 && precision == LBM_DOUBLE) return by_format(D3Q27{}, 0.0);
+  return (int)cudaErrorInvalidValue;
+}
+
+template <class Real, int FMT>
+using SlabState = std::conditional_t<(FMT < 0), NativeState<Real>, ShiftedState<(FMT < 0 ? 0 : FMT)>>;
 
 }  // namespace lbcube
 
@@ -883,18 +940,12 @@ extern "C" size_t lbm_reactive_slab_objective_bytes(int fluid_lattice, size_t x_
   return (size_t)g.blocks() * sizeof(double);
 }
 
-#define LBCUBE_SLAB_DISPATCH(...)                                                                 \
-  if (fluid_lattice == kD3Q19 && precision == LBM_FLOAT) { using FL = D3Q19; using R = float; __VA_ARGS__; } \
-  if (fluid_lattice == kD3Q19 && precision == LBM_DOUBLE) { using FL = D3Q19; using R = double; __VA_ARGS__; } \
-  if (fluid_lattice == kD3Q27 && precision == LBM_FLOAT) { using FL = D3Q27; using R = float; __VA_ARGS__; } \
-  if (fluid_lattice == kD3Q27 && precision == LBM_DOUBLE) { using FL = D3Q27; using R = double; __VA_ARGS__; } \
-  return (int)cudaErrorInvalidValue;
-
 extern "C" int lbm_reactive_slab_forward_async(
-    int fluid_lattice, int precision, int collision, const void* current_fluid, void* next_fluid,
-    const void* current_a, void* next_a, const void* current_b, void* next_b, void* velocity,
-    size_t x_extent, size_t y_extent, size_t z_extent, double tau, double tau_c, double k_react,
-    const void* halo_lo, const void* halo_hi, void* send_lo, void* send_hi, void* stream) {
+    int fluid_lattice, int precision, int storage, float c0, int collision,
+    const void* current_fluid, void* next_fluid, const void* current_a, void* next_a,
+    const void* current_b, void* next_b, void* velocity, size_t x_extent, size_t y_extent,
+    size_t z_extent, double tau, double tau_c, double k_react, const void* halo_lo,
+    const void* halo_hi, void* send_lo, void* send_hi, void* stream) {
   Grid g;
   cudaError_t err = slab_domain(fluid_lattice, precision,
                                 current_fluid == nullptr || next_fluid == nullptr ||
@@ -906,30 +957,46 @@ extern "C" int lbm_reactive_slab_forward_async(
   if (err != cudaSuccess) return (int)err;
   if (!slab_collision_ok(fluid_lattice, collision) || !(tau > 0.5) || !(tau_c > 0.5))
     return (int)cudaErrorInvalidValue;
-  const size_t real = precision == LBM_DOUBLE ? 8 : 4;
-  const size_t fq = fluid_lattice == kD3Q19 ? 19 : 27;
-  const size_t fb = fq * g.plane * real, sb = 7 * g.plane * real, ub = 3 * g.plane * real;
-  const size_t hb = lbm_fluid_reaction_slab_face_elems(fluid_lattice, x_extent, y_extent) * real;
-  const Span reads[5] = {{current_fluid, fb}, {current_a, sb}, {current_b, sb}, {halo_lo, hb},
-                         {halo_hi, hb}};
-  const Span writes[6] = {{next_fluid, fb}, {next_a, sb},   {next_b, sb},
-                          {send_lo, hb},    {send_hi, hb},  {velocity, velocity ? ub : 0}};
-  if (any_overlap(reads, writes)) return (int)cudaErrorInvalidValue;
   const cudaStream_t s = as_stream(stream);
-  // the relaxation rates as the whole-box gradient forms them
-  LBCUBE_SLAB_DISPATCH(return (int)fluid_reaction_slab_with_velocity<FL, R>(
-      collision, (const R*)current_fluid, (R*)next_fluid, (const R*)current_a, (R*)next_a,
-      (const R*)current_b, (R*)next_b, (R*)velocity, g, R(1) / R(tau), R(1) / R(tau_c), R(k_react),
-      (const R*)halo_lo, (const R*)halo_hi, (R*)send_lo, (R*)send_hi, s))
+  return slab_dispatch(fluid_lattice, precision, storage, [&](auto fl, auto r, auto f) -> int {
+    using FL = decltype(fl);
+    using R = decltype(r);
+    constexpr int FMT = decltype(f)::value;
+    using E = typename SlabState<R, FMT>::elem;
+    const size_t fe = FL::Q * (size_t)g.plane, se = 7 * (size_t)g.plane;
+    const size_t ub = 3 * (size_t)g.plane * sizeof(R);
+    const size_t hb = lbm_fluid_reaction_slab_face_elems(fluid_lattice, x_extent, y_extent) * sizeof(E);
+    const Span reads[5] = {{current_fluid, fe * sizeof(E)}, {current_a, se * sizeof(E)},
+                           {current_b, se * sizeof(E)},     {halo_lo, hb},
+                           {halo_hi, hb}};
+    const Span writes[6] = {{next_fluid, fe * sizeof(E)}, {next_a, se * sizeof(E)},
+                            {next_b, se * sizeof(E)},     {send_lo, hb},
+                            {send_hi, hb},                {velocity, velocity ? ub : 0}};
+    if (any_overlap(reads, writes)) return (int)cudaErrorInvalidValue;
+    // the relaxation rates as the whole-box gradient forms them
+    if constexpr (FMT < 0) {
+      return (int)fluid_reaction_slab_with_velocity<FL, R>(
+          collision, (const R*)current_fluid, (R*)next_fluid, (const R*)current_a, (R*)next_a,
+          (const R*)current_b, (R*)next_b, (R*)velocity, g, R(1) / R(tau), R(1) / R(tau_c),
+          R(k_react), (const R*)halo_lo, (const R*)halo_hi, (R*)send_lo, (R*)send_hi, s);
+    } else {
+      return (int)fluid_reaction_shifted_slab<FL, FMT>(
+          collision, (const E*)current_fluid, (E*)next_fluid, (const E*)current_a, (E*)next_a,
+          (const E*)current_b, (E*)next_b, (float*)velocity, g, 1.0f / (float)tau,
+          1.0f / (float)tau_c, (float)k_react, 1.0f, c0, (const E*)halo_lo, (const E*)halo_hi,
+          (E*)send_lo, (E*)send_hi, s);
+    }
+  });
 }
 
 extern "C" int lbm_reactive_slab_adjoint_step_async(
-    int fluid_lattice, int precision, int collision, const void* fluid_n, const void* a_n,
-    const void* b_n, const void* halo_lo, const void* halo_hi, const void* velocity_next,
-    const void* lambda_fluid_next, const void* lambda_a_next, const void* lambda_b_next,
-    void* lambda_fluid, void* lambda_a, void* lambda_b, void* velocity_adjoint, void* send_lo,
-    void* send_hi, size_t x_extent, size_t y_extent, size_t z_extent, double tau, double tau_c,
-    double k_react, double* slots, size_t slots_bytes, void* stream) {
+    int fluid_lattice, int precision, int storage, float c0, int collision, const void* fluid_n,
+    const void* a_n, const void* b_n, const void* halo_lo, const void* halo_hi,
+    const void* velocity_next, const void* lambda_fluid_next, const void* lambda_a_next,
+    const void* lambda_b_next, void* lambda_fluid, void* lambda_a, void* lambda_b,
+    void* velocity_adjoint, void* send_lo, void* send_hi, size_t x_extent, size_t y_extent,
+    size_t z_extent, double tau, double tau_c, double k_react, double* slots, size_t slots_bytes,
+    void* stream) {
   Grid g;
   cudaError_t err = slab_domain(
       fluid_lattice, precision,
@@ -944,12 +1011,18 @@ extern "C" int lbm_reactive_slab_adjoint_step_async(
       slots_bytes < slab_slots_bytes(g))
     return (int)cudaErrorInvalidValue;
   const cudaStream_t s = as_stream(stream);
-  LBCUBE_SLAB_DISPATCH(return (int)slab_adjoint_step<FL, R>(
-      collision, (const R*)fluid_n, (const R*)a_n, (const R*)b_n, (const R*)halo_lo,
-      (const R*)halo_hi, (const R*)velocity_next, (const R*)lambda_fluid_next,
-      (const R*)lambda_a_next, (const R*)lambda_b_next, (R*)lambda_fluid, (R*)lambda_a,
-      (R*)lambda_b, (R*)velocity_adjoint, (R*)send_lo, (R*)send_hi, g, tau, tau_c, k_react, slots,
-      s))
+  return slab_dispatch(fluid_lattice, precision, storage, [&](auto fl, auto r, auto f) -> int {
+    using FL = decltype(fl);
+    using R = decltype(r);
+    using SP = SlabState<R, decltype(f)::value>;
+    using E = typename SP::elem;
+    return (int)slab_adjoint_step<FL, R, SP>(
+        collision, (const E*)fluid_n, (const E*)a_n, (const E*)b_n, (const E*)halo_lo,
+        (const E*)halo_hi, (const R*)velocity_next, (const R*)lambda_fluid_next,
+        (const R*)lambda_a_next, (const R*)lambda_b_next, (R*)lambda_fluid, (R*)lambda_a,
+        (R*)lambda_b, (R*)velocity_adjoint, (R*)send_lo, (R*)send_hi, g, tau, tau_c, k_react, c0,
+        slots, s);
+  });
 }
 
 extern "C" int lbm_reactive_slab_adjoint_unpack_async(int fluid_lattice, int precision,
@@ -976,19 +1049,23 @@ extern "C" int lbm_reactive_slab_adjoint_unpack_async(int fluid_lattice, int pre
   const cudaStream_t s = as_stream(stream);
   const long long total = 2LL * g.ny * g.nx;
   const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-  LBCUBE_SLAB_DISPATCH(reactive_slab_unpack_kernel<FL, R><<<blocks, 256, 0, s>>>(
-                           (const R*)recv_lo, (const R*)recv_hi, (R*)lambda_fluid, (R*)lambda_a,
-                           (R*)lambda_b, g);
-                       return (int)cudaGetLastError())
+  return slab_dispatch(fluid_lattice, precision, LBM_NATIVE, [&](auto fl, auto r, auto) -> int {
+    using FL = decltype(fl);
+    using R = decltype(r);
+    reactive_slab_unpack_kernel<FL, R><<<blocks, 256, 0, s>>>(
+        (const R*)recv_lo, (const R*)recv_hi, (R*)lambda_fluid, (R*)lambda_a, (R*)lambda_b, g);
+    return (int)cudaGetLastError();
+  });
 }
 
-extern "C" int lbm_reactive_slab_seed_async(int fluid_lattice, int precision, int objective,
-                                            const void* a_final, const void* b_final,
-                                            const void* a0, const double* diagnostics,
-                                            void* lambda_fluid, void* lambda_a, void* lambda_b,
-                                            size_t x_extent, size_t y_extent, size_t z_extent,
-                                            double total_cells, double* objective_partials,
-                                            size_t partials_bytes, void* stream) {
+extern "C" int lbm_reactive_slab_seed_async(int fluid_lattice, int precision, int storage,
+                                            float c0, int objective, const void* a_final,
+                                            const void* b_final, const void* a0,
+                                            const double* diagnostics, void* lambda_fluid,
+                                            void* lambda_a, void* lambda_b, size_t x_extent,
+                                            size_t y_extent, size_t z_extent, double total_cells,
+                                            double* objective_partials, size_t partials_bytes,
+                                            void* stream) {
   Grid g;
   cudaError_t err = slab_domain(
       fluid_lattice, precision,
@@ -1002,14 +1079,21 @@ extern "C" int lbm_reactive_slab_seed_async(int fluid_lattice, int precision, in
     return (int)cudaErrorInvalidValue;
   const cudaStream_t s = as_stream(stream);
   const double inv_n = 1.0 / total_cells;
-#define LBCUBE_SEED(OBJ)                                                                           \
-  reactive_seed_kernel<FL, R, OBJ, NativeState<R>><<<grid_dims(g), block_dims(g), 0, s>>>(         \
-      (const R*)a_final, (const R*)b_final, (const R*)a0, diagnostics, (R*)lambda_fluid,           \
-      (R*)lambda_a, (R*)lambda_b, g, 0.0f, inv_n, objective_partials)
-  LBCUBE_SLAB_DISPATCH(if (objective == LBM_OBJECTIVE_SEGREGATION) LBCUBE_SEED(LBM_OBJECTIVE_SEGREGATION);
-                       else LBCUBE_SEED(LBM_OBJECTIVE_MEAN_PRODUCT);
-                       return (int)cudaGetLastError())
-#undef LBCUBE_SEED
+  return slab_dispatch(fluid_lattice, precision, storage, [&](auto fl, auto r, auto f) -> int {
+    using FL = decltype(fl);
+    using R = decltype(r);
+    using SP = SlabState<R, decltype(f)::value>;
+    using E = typename SP::elem;
+    if (objective == LBM_OBJECTIVE_SEGREGATION)
+      reactive_seed_kernel<FL, R, LBM_OBJECTIVE_SEGREGATION, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
+          (const E*)a_final, (const E*)b_final, (const R*)a0, diagnostics, (R*)lambda_fluid,
+          (R*)lambda_a, (R*)lambda_b, g, c0, inv_n, objective_partials);
+    else
+      reactive_seed_kernel<FL, R, LBM_OBJECTIVE_MEAN_PRODUCT, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
+          (const E*)a_final, (const E*)b_final, (const R*)a0, diagnostics, (R*)lambda_fluid,
+          (R*)lambda_a, (R*)lambda_b, g, c0, inv_n, objective_partials);
+    return (int)cudaGetLastError();
+  });
 }
 
 extern "C" int lbm_reactive_slab_init_gradients_async(
@@ -1030,16 +1114,21 @@ extern "C" int lbm_reactive_slab_init_gradients_async(
       !(total_cells >= (double)g.plane))
     return (int)cudaErrorInvalidValue;
   const cudaStream_t s = as_stream(stream);
-  LBCUBE_SLAB_DISPATCH(
-      const R direct = objective == LBM_OBJECTIVE_MEAN_PRODUCT ? R(1.0 / total_cells) : R(0);
+  return slab_dispatch(fluid_lattice, precision, LBM_NATIVE, [&](auto fl, auto r, auto) -> int {
+    using FL = decltype(fl);
+    using R = decltype(r);
+    const R direct = objective == LBM_OBJECTIVE_MEAN_PRODUCT ? R(1.0 / total_cells) : R(0);
+    scalar_init_gradient_kernel<FL, R><<<grid_dims(g), block_dims(g), 0, s>>>(
+        (const R*)u0, (const R*)lambda_a, direct, (R*)grad_a0, g);
+    if (grad_b0 != nullptr)
       scalar_init_gradient_kernel<FL, R><<<grid_dims(g), block_dims(g), 0, s>>>(
-          (const R*)u0, (const R*)lambda_a, direct, (R*)grad_a0, g);
-      if (grad_b0 != nullptr) scalar_init_gradient_kernel<FL, R><<<grid_dims(g), block_dims(g), 0, s>>>(
           (const R*)u0, (const R*)lambda_b, R(0), (R*)grad_b0, g);
-      if (grad_u0 != nullptr) reactive_velocity_gradient_kernel<FL, R><<<grid_dims(g), block_dims(g), 0, s>>>(
+    if (grad_u0 != nullptr)
+      reactive_velocity_gradient_kernel<FL, R><<<grid_dims(g), block_dims(g), 0, s>>>(
           (const R*)rho0, (const R*)u0, (const R*)a0, (const R*)b0, (const R*)lambda_fluid,
           (const R*)lambda_a, (const R*)lambda_b, (R*)grad_u0, g);
-      return (int)cudaGetLastError())
+    return (int)cudaGetLastError();
+  });
 }
 
 extern "C" int lbm_reactive_slab_sums_async(int fluid_lattice, size_t x_extent, size_t y_extent,
@@ -1077,4 +1166,3 @@ extern "C" int lbm_reactive_slab_result_async(int precision, int objective, cons
   return (int)cudaGetLastError();
 }
 
-#undef LBCUBE_SLAB_DISPATCH

@@ -596,6 +596,31 @@ extern "C" int lbm_fluid_reaction_slab_async(
   return (int)cudaErrorInvalidValue;
 }
 
+// The pack for any stored form of the reactive gradient's states: elements of
+// the precision (LBM_NATIVE) or 16-bit codes (a shifted format, LBM_FLOAT).
+extern "C" int lbm_reactive_slab_pack_async(int fluid_lattice, int precision, int storage,
+                                            const void* fluid, const void* a, const void* b,
+                                            size_t x_extent, size_t y_extent, size_t z_extent,
+                                            void* send_lo, void* send_hi, void* stream) {
+  if (storage != LBM_NATIVE)
+    return precision != LBM_FLOAT || (storage != LBM_F16S && storage != LBM_BF16S &&
+                                      storage != LBM_E3M12S && storage != LBM_Q15S)
+               ? (int)cudaErrorInvalidValue
+           : fluid_lattice == LBM_D3Q19
+               ? (int)launch_fluid_reaction_slab_pack<D3Q19, unsigned short>(
+                     (const unsigned short*)fluid, (const unsigned short*)a,
+                     (const unsigned short*)b, x_extent, y_extent, z_extent,
+                     (unsigned short*)send_lo, (unsigned short*)send_hi, as_stream(stream))
+           : fluid_lattice == LBM_D3Q27
+               ? (int)launch_fluid_reaction_slab_pack<D3Q27, unsigned short>(
+                     (const unsigned short*)fluid, (const unsigned short*)a,
+                     (const unsigned short*)b, x_extent, y_extent, z_extent,
+                     (unsigned short*)send_lo, (unsigned short*)send_hi, as_stream(stream))
+               : (int)cudaErrorInvalidValue;
+  return lbm_fluid_reaction_slab_pack_async(fluid_lattice, precision, fluid, a, b, x_extent,
+                                            y_extent, z_extent, send_lo, send_hi, stream);
+}
+
 extern "C" int lbm_fluid_reaction_slab_pack_async(int fluid_lattice, int precision,
                                                   const void* fluid, const void* a, const void* b,
                                                   size_t x_extent, size_t y_extent, size_t z_extent,

@@ -16,6 +16,7 @@
 #include "collide_dev.cuh"
 #include "common.cuh"
 #include "reduce.cuh"
+#include "slab_faces.cuh"
 #include "stream_vec.cuh"
 #include "../../include/lbcube_b200.h"
 
@@ -40,7 +41,34 @@ __device__ __forceinline__ void gather_codes(const unsigned short* __restrict__ 
   });
 }
 
-template <class FL, int FMT, int CT, bool STATS, bool UOUT>
+// Pull-gather of 16-bit codes on a z-slab (halo planes of codes at the faces,
+// slab_faces.cuh), decoded as gather_codes does.
+template <class L, int FMT, bool DEVIATION>
+__device__ __forceinline__ void gather_codes_slab(const unsigned short* __restrict__ cur, const Grid& g,
+                                                  const Neighbours& n, int x, int y, int z, float c0,
+                                                  const unsigned short* __restrict__ halo_lo,
+                                                  const unsigned short* __restrict__ halo_hi,
+                                                  float (&out)[L::Q]) {
+  unsigned short h[L::Q];
+  gather_slab<L>(cur, g, n, x, y, z, halo_lo, halo_hi, h);
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    if constexpr (DEVIATION) out[i] = Codec<FMT>::decode(h[i]);
+    else out[i] = ShiftedStorage<FMT>::template decode<L, i>(h[i], {c0});
+  });
+}
+
+// The face buffers of a slab of 16-bit states (codes; layout of slab_faces.cuh).
+struct CodeFaces {
+  const unsigned short* halo_lo;
+  const unsigned short* halo_hi;
+  unsigned short* send_lo;
+  unsigned short* send_hi;
+};
+
+// SLAB: a z-slab of a box, the pulls across its faces from `faces` and the
+// leaving codes stored into its send buffers (every plane of the slab).
+template <class FL, int FMT, int CT, bool STATS, bool UOUT, bool SLAB = false>
 __global__ void __launch_bounds__(kThreads)
     fluid_reaction_shifted_kernel(const unsigned short* __restrict__ cur_f,
                                   unsigned short* __restrict__ nxt_f,
@@ -49,8 +77,11 @@ __global__ void __launch_bounds__(kThreads)
                                   const unsigned short* __restrict__ cur_b,
                                   unsigned short* __restrict__ nxt_b, Grid g, float omega,
                                   float omega_minus, float omega_c, float k, float rho0, float c0,
-                                  double* __restrict__ partials, float* __restrict__ u_out) {
+                                  double* __restrict__ partials, float* __restrict__ u_out,
+                                  CodeFaces faces = {}) {
   using SL = typename ScalarOf<FL>::type;
+  const size_t a_off = (size_t)face_planes<FL>() * g.ny * g.nx;
+  const size_t b_off = a_off + (size_t)face_planes<SL>() * g.ny * g.nx;
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double sums[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -59,22 +90,40 @@ __global__ void __launch_bounds__(kThreads)
     const size_t plane = (size_t)g.plane;
     const Neighbours n = neighbours(g, x, y, z);
     float v[FL::Q], u[FL::D];
-    gather_codes<FL, FMT, true>(cur_f, g, n, x, y, z, 0.0f, v);
+    if constexpr (SLAB) gather_codes_slab<FL, FMT, true>(cur_f, g, n, x, y, z, 0.0f, faces.halo_lo, faces.halo_hi, v);
+    else gather_codes<FL, FMT, true>(cur_f, g, n, x, y, z, 0.0f, v);
     if constexpr (CT == kMRT) collide_dev_mrt<FL, FMT>(v, omega, rho0);
     else collide_dev<FL, CT, FMT>(v, omega, omega_minus, rho0);
-    static_for<FL::Q>([&](auto I) { nxt_f[plane * LB_I(I) + cell] = Codec<FMT>::encode(v[LB_I(I)]); });
+    unsigned short hf[FL::Q];
+    static_for<FL::Q>([&](auto I) {
+      hf[LB_I(I)] = Codec<FMT>::encode(v[LB_I(I)]);
+      nxt_f[plane * LB_I(I) + cell] = hf[LB_I(I)];
+    });
+    if constexpr (SLAB) send_slab<FL>(g, x, y, z, hf, faces.send_lo, faces.send_hi);
     dev_velocity<FL, FMT>(v, rho0, u);
     if constexpr (UOUT) static_for<FL::D>([&](auto D) { u_out[plane * LB_I(D) + cell] = u[LB_I(D)]; });
     float a[SL::Q], b[SL::Q];
-    gather_codes<SL, FMT, false>(cur_a, g, n, x, y, z, c0, a);
-    gather_codes<SL, FMT, false>(cur_b, g, n, x, y, z, c0, b);
+    if constexpr (SLAB) {
+      gather_codes_slab<SL, FMT, false>(cur_a, g, n, x, y, z, c0, faces.halo_lo + a_off, faces.halo_hi + a_off, a);
+      gather_codes_slab<SL, FMT, false>(cur_b, g, n, x, y, z, c0, faces.halo_lo + b_off, faces.halo_hi + b_off, b);
+    } else {
+      gather_codes<SL, FMT, false>(cur_a, g, n, x, y, z, c0, a);
+      gather_codes<SL, FMT, false>(cur_b, g, n, x, y, z, c0, b);
+    }
     react_pair<SL>(a, b, u, omega_c, k);
     const typename ShiftedStorage<FMT>::Params sp{c0};
+    unsigned short ha[SL::Q], hb[SL::Q];
     static_for<SL::Q>([&](auto I) {
       constexpr int i = LB_I(I);
-      nxt_a[plane * i + cell] = ShiftedStorage<FMT>::template encode<SL, i>(a[i], sp);
-      nxt_b[plane * i + cell] = ShiftedStorage<FMT>::template encode<SL, i>(b[i], sp);
+      ha[i] = ShiftedStorage<FMT>::template encode<SL, i>(a[i], sp);
+      hb[i] = ShiftedStorage<FMT>::template encode<SL, i>(b[i], sp);
+      nxt_a[plane * i + cell] = ha[i];
+      nxt_b[plane * i + cell] = hb[i];
     });
+    if constexpr (SLAB) {
+      send_slab<SL>(g, x, y, z, ha, faces.send_lo + a_off, faces.send_hi + a_off);
+      send_slab<SL>(g, x, y, z, hb, faces.send_lo + b_off, faces.send_hi + b_off);
+    }
     if constexpr (STATS) {
       const double sa = (double)concentration<SL>(a), sb = (double)concentration<SL>(b);
       sums[0] = sa;
@@ -128,6 +177,57 @@ cudaError_t fluid_reaction_shifted(int collision, const unsigned short* cur_f,
     default: return cudaErrorInvalidValue;
   }
 }
+
+// The slab form of fluid_reaction_shifted (all planes, no statistics; u_out
+// may be null). Buffers are checked by the caller.
+template <class FL, int FMT>
+cudaError_t fluid_reaction_shifted_slab(int collision, const unsigned short* cur_f,
+                                        unsigned short* nxt_f, const unsigned short* cur_a,
+                                        unsigned short* nxt_a, const unsigned short* cur_b,
+                                        unsigned short* nxt_b, float* u_out, const Grid& g,
+                                        float omega, float omega_c, float k, float rho0, float c0,
+                                        const unsigned short* halo_lo, const unsigned short* halo_hi,
+                                        unsigned short* send_lo, unsigned short* send_hi,
+                                        cudaStream_t s) {
+  const CodeFaces faces{halo_lo, halo_hi, send_lo, send_hi};
+  auto launch = [&](auto ct) -> cudaError_t {
+    constexpr int CT = decltype(ct)::value;
+    const float om = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
+    if (u_out != nullptr)
+      fluid_reaction_shifted_kernel<FL, FMT, CT, false, true, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, om, omega_c, k, rho0, c0, nullptr, u_out,
+          faces);
+    else
+      fluid_reaction_shifted_kernel<FL, FMT, CT, false, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
+          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, om, omega_c, k, rho0, c0, nullptr, nullptr,
+          faces);
+    return cudaGetLastError();
+  };
+  switch (collision) {
+    case kBGK: return launch(std::integral_constant<int, kBGK>{});
+    case kTRT: return launch(std::integral_constant<int, kTRT>{});
+    case kMRT:
+      if constexpr (FL::Q != 27) return launch(std::integral_constant<int, kMRT>{});
+      return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+#define LBCUBE_FRSS(FL, F)                                                                        \
+  template cudaError_t fluid_reaction_shifted_slab<FL, F>(                                        \
+      int, const unsigned short*, unsigned short*, const unsigned short*, unsigned short*,        \
+      const unsigned short*, unsigned short*, float*, const Grid&, float, float, float, float,    \
+      float, const unsigned short*, const unsigned short*, unsigned short*, unsigned short*,      \
+      cudaStream_t);
+LBCUBE_FRSS(D3Q19, kF16S)
+LBCUBE_FRSS(D3Q19, kBF16S)
+LBCUBE_FRSS(D3Q19, kE3M12S)
+LBCUBE_FRSS(D3Q19, kQ15S)
+LBCUBE_FRSS(D3Q27, kF16S)
+LBCUBE_FRSS(D3Q27, kBF16S)
+LBCUBE_FRSS(D3Q27, kE3M12S)
+LBCUBE_FRSS(D3Q27, kQ15S)
+#undef LBCUBE_FRSS
 
 #define LBCUBE_FRS(FL, F)                                                                         \
   template cudaError_t fluid_reaction_shifted<FL, F>(                                             \

@@ -113,15 +113,16 @@ def _declare(lib):
                                           _sz, d, d, d, _vp, _vp, _vp, _vp, _sz, _sz, _vp, _sz, _vp],
         "lbm_fluid_reaction_slab_pack_async": [C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
         "lbm_reactive_stats_sums_async": [C.c_int, _sz, _sz, _sz, _vp, _sz, _vp, _vp],
-        "lbm_reactive_slab_forward_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz,
-                                            _sz, _sz, d, d, d, _vp, _vp, _vp, _vp, _vp],
-        "lbm_reactive_slab_adjoint_step_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                                 _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz, d, d, d,
-                                                 _vp, _sz, _vp],
+        "lbm_reactive_slab_pack_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
+        "lbm_reactive_slab_forward_async": [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp, _vp, _vp, _vp,
+                                            _vp, _vp, _vp, _sz, _sz, _sz, d, d, d, _vp, _vp, _vp, _vp, _vp],
+        "lbm_reactive_slab_adjoint_step_async": [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp, _vp, _vp,
+                                                 _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz,
+                                                 _sz, _sz, d, d, d, _vp, _sz, _vp],
         "lbm_reactive_slab_adjoint_unpack_async": [C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz,
                                                    _vp],
-        "lbm_reactive_slab_seed_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz,
-                                         _sz, d, _vp, _sz, _vp],
+        "lbm_reactive_slab_seed_async": [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _vp, _vp, _vp, _vp, _vp,
+                                         _vp, _vp, _sz, _sz, _sz, d, _vp, _sz, _vp],
         "lbm_reactive_slab_init_gradients_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                                    _sz, _sz, _sz, d, _vp, _vp, _vp, _vp],
         "lbm_reactive_slab_sums_async": [C.c_int, _sz, _sz, _sz, _vp, _sz, _vp, _sz, _vp, _vp],

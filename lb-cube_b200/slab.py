@@ -210,25 +210,38 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
     initial-state gradients are bit-identical to the whole box's."""
 
     def __init__(self, torch, lattice, real, collision, objective, nx, ny, nz_global, tau, tau_c, k, steps, interval,
-                 rank, world, device):
+                 rank, world, device, storage=None, c0=0.5):
         super().__init__(torch, lattice, real, collision, nx, ny, nz_global, 1.0 / tau, 1.0 / tau_c, k, rank, world,
                          device)
         if steps < 1 or interval < 2:
             raise ValueError("need steps >= 1 and a checkpoint interval >= 2")
+        if storage not in (None, "native") and real != "float":
+            raise ValueError("16-bit states need real = 'float'")
         self.objective = objective
+        self.storage = E._storage(storage)  # 0: states in `real`; else a 16-bit format code
+        self.c0 = float(c0)
         self.tau, self.tau_c = float(tau), float(tau_c)
         self.steps, self.interval = int(steps), int(interval)
         self.total_cells = float(nx * ny * nz_global)
         dtype = torch.float32 if real == "float" else torch.float64
+        sdtype = dtype if self.storage == 0 else torch.int16  # element of a stored state
         q = Q_OF[lattice]
         shape = (self.nz, ny, nx)
         self._dtype, self._device = dtype, device
 
-        def field(qq):
-            return torch.empty((qq,) + shape, dtype=dtype, device=device)
+        def field(qq, dt=dtype):
+            return torch.empty((qq,) + shape, dtype=dt, device=device)
 
         def state():
-            return (field(q), field(7), field(7), field(3))
+            return (field(q, sdtype), field(7, sdtype), field(7, sdtype), field(3))
+
+        # face buffers: the stored states' (forward steps, packs) and the
+        # adjoint's (scatter sends, in `real`); exchanges move whichever set is
+        # current in halo_lo / halo_hi / send_lo / send_hi
+        n = E.load().lbm_fluid_reaction_slab_face_elems(E.LATTICES[lattice], nx, ny)
+        self._lam_faces = (self.halo_lo, self.halo_hi, self.send_lo, self.send_hi)
+        self._state_faces = self._lam_faces if self.storage == 0 else tuple(
+            torch.empty(n, dtype=sdtype, device=device) for _ in range(4))
 
         nseg = (self.steps + self.interval - 1) // self.interval
         self.nseg = nseg
@@ -249,24 +262,43 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
         self.result = torch.empty(4, dtype=torch.float64, device=device)
 
     # ---- the per-step entries
+    def _faces(self, which):
+        self.halo_lo, self.halo_hi, self.send_lo, self.send_hi = (
+            self._state_faces if which == "state" else self._lam_faces)
+
+    def pack(self, state, stream=None):
+        """Faces of a stored state (fluid, a, b) into the state send buffers."""
+        self._faces("state")
+        f, a, b = state[:3]
+        E.check(E.load().lbm_reactive_slab_pack_async(
+            E.LATTICES[self.lattice], E.REALS[self.real], self.storage, f.data_ptr(), a.data_ptr(), b.data_ptr(),
+            self.nx, self.ny, self.nz, self.send_lo.data_ptr(), self.send_hi.data_ptr(), E._stream(stream)),
+            "reactive slab pack")
+
     def _forward(self, cur, nxt, keep_u, stream=None):
+        self._faces("state")
         E.check(E.load().lbm_reactive_slab_forward_async(
-            E.LATTICES[self.lattice], E.REALS[self.real], E.COLLISIONS[self.collision], cur[0].data_ptr(),
+            E.LATTICES[self.lattice], E.REALS[self.real], self.storage, self.c0, E.COLLISIONS[self.collision],
+            cur[0].data_ptr(),
             nxt[0].data_ptr(), cur[1].data_ptr(), nxt[1].data_ptr(), cur[2].data_ptr(), nxt[2].data_ptr(),
             nxt[3].data_ptr() if keep_u else None, self.nx, self.ny, self.nz, self.tau, self.tau_c, self.k,
             self.halo_lo.data_ptr(), self.halo_hi.data_ptr(), self.send_lo.data_ptr(), self.send_hi.data_ptr(),
             E._stream(stream)), "reactive slab forward step")
 
     def _adjoint(self, sn, u_next, ln, l, stream=None):
+        # reads the state halos (exchanged after pack), writes the adjoint's sends
+        halo_lo, halo_hi = self._state_faces[0], self._state_faces[1]
+        self._faces("lambda")
         E.check(E.load().lbm_reactive_slab_adjoint_step_async(
-            E.LATTICES[self.lattice], E.REALS[self.real], E.COLLISIONS[self.collision], sn[0].data_ptr(),
-            sn[1].data_ptr(), sn[2].data_ptr(), self.halo_lo.data_ptr(), self.halo_hi.data_ptr(),
+            E.LATTICES[self.lattice], E.REALS[self.real], self.storage, self.c0, E.COLLISIONS[self.collision],
+            sn[0].data_ptr(), sn[1].data_ptr(), sn[2].data_ptr(), halo_lo.data_ptr(), halo_hi.data_ptr(),
             u_next.data_ptr(), ln[0].data_ptr(), ln[1].data_ptr(), ln[2].data_ptr(), l[0].data_ptr(),
             l[1].data_ptr(), l[2].data_ptr(), self.ubar.data_ptr(), self.send_lo.data_ptr(),
             self.send_hi.data_ptr(), self.nx, self.ny, self.nz, self.tau, self.tau_c, self.k, self.slots.data_ptr(),
             self.slots_bytes, E._stream(stream)), "reactive slab adjoint step")
 
     def _unpack(self, l, stream=None):
+        self._faces("lambda")
         E.check(E.load().lbm_reactive_slab_adjoint_unpack_async(
             E.LATTICES[self.lattice], E.REALS[self.real], self.halo_lo.data_ptr(), self.halo_hi.data_ptr(),
             l[0].data_ptr(), l[1].data_ptr(), l[2].data_ptr(), self.nx, self.ny, self.nz, E._stream(stream)),
@@ -290,12 +322,18 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
         # forward: the equilibrium initial state, checkpoints every `interval`
         # steps, the last segment's states kept
         s0 = ckpt[0]
-        E.check(lib.lbm_init_equilibrium_async(L, P, rho0.data_ptr(), u0.data_ptr(), s0[0].data_ptr(), nx, ny, nz,
+        # 16-bit states: the FP32 equilibrium in an adjoint buffer, then encoded
+        fi, ai, bi = (s0[:3] if self.storage == 0 else self.lam[0])
+        E.check(lib.lbm_init_equilibrium_async(L, P, rho0.data_ptr(), u0.data_ptr(), fi.data_ptr(), nx, ny, nz,
                                                None), "init")
-        E.check(lib.lbm_init_equilibrium_async(SL, P, a0.data_ptr(), u0.data_ptr(), s0[1].data_ptr(), nx, ny, nz,
+        E.check(lib.lbm_init_equilibrium_async(SL, P, a0.data_ptr(), u0.data_ptr(), ai.data_ptr(), nx, ny, nz,
                                                None), "init")
-        E.check(lib.lbm_init_equilibrium_async(SL, P, b0.data_ptr(), u0.data_ptr(), s0[2].data_ptr(), nx, ny, nz,
+        E.check(lib.lbm_init_equilibrium_async(SL, P, b0.data_ptr(), u0.data_ptr(), bi.data_ptr(), nx, ny, nz,
                                                None), "init")
+        if self.storage != 0:
+            for lat, src, dst, ref in ((L, fi, s0[0], 1.0), (SL, ai, s0[1], self.c0), (SL, bi, s0[2], self.c0)):
+                E.check(lib.lbm_encode_shifted_async(lat, self.storage, P, src.data_ptr(), dst.data_ptr(), nx, ny,
+                                                     nz, ref, None), "encode")
         self.pack(s0[:3])
         yield ("exchange",)
         last0 = (nseg - 1) * interval
@@ -317,7 +355,14 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
         lN = self.lam[steps % 2]
         if self.objective == "segregation":
             scratch = torch.empty(8, dtype=torch.float64, device=self._device)
-            E.check(lib.lbm_reactive_stats_async(SL, P, cur[1].data_ptr(), cur[2].data_ptr(), nx, ny, nz, self.k,
+            fa, fb = cur[1], cur[2]
+            if self.storage != 0:  # statistics of the decoded final fields (the other adjoint buffer)
+                tmp = self.lam[(steps + 1) % 2]
+                for src, dst in ((cur[1], tmp[1]), (cur[2], tmp[2])):
+                    E.check(lib.lbm_decode_shifted_async(SL, self.storage, P, src.data_ptr(), dst.data_ptr(), nx, ny,
+                                                         nz, self.c0, None), "decode")
+                fa, fb = tmp[1], tmp[2]
+            E.check(lib.lbm_reactive_stats_async(SL, P, fa.data_ptr(), fb.data_ptr(), nx, ny, nz, self.k,
                                                  self.partials.data_ptr(), self.partials_bytes, scratch.data_ptr(),
                                                  None), "statistics")
             sums5 = self.rank_sums()
@@ -326,7 +371,7 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
                                                            self.diag.data_ptr(), None), "statistics")
         obj = E.OBJECTIVES[self.objective]
         E.check(lib.lbm_reactive_slab_seed_async(
-            L, P, obj, cur[1].data_ptr(), cur[2].data_ptr(), a0.data_ptr(), self.diag.data_ptr(), lN[0].data_ptr(),
+            L, P, self.storage, self.c0, obj, cur[1].data_ptr(), cur[2].data_ptr(), a0.data_ptr(), self.diag.data_ptr(), lN[0].data_ptr(),
             lN[1].data_ptr(), lN[2].data_ptr(), nx, ny, nz, self.total_cells, self.obj_partials.data_ptr(),
             self.obj_bytes, None), "reactive slab seed")
         self.slots.zero_()
@@ -436,13 +481,14 @@ class HostExchange:
     def __init__(self, dist, group=None):
         self.dist = dist
         self.group = group
-        self._host = None
+        self._host = {}  # host staging buffers per (dtype, size) of face buffer
 
     def exchange(self, d: SlabDomain):
         torch = d.torch
-        if self._host is None:
-            self._host = [torch.empty(d.send_lo.shape, dtype=d.send_lo.dtype) for _ in range(4)]
-        s_hi, s_lo, h_lo, h_hi = self._host
+        key = (d.send_lo.dtype, d.send_lo.numel())
+        if key not in self._host:
+            self._host[key] = [torch.empty(d.send_lo.shape, dtype=d.send_lo.dtype) for _ in range(4)]
+        s_hi, s_lo, h_lo, h_hi = self._host[key]
         s_hi.copy_(d.send_hi)
         s_lo.copy_(d.send_lo)
         if d.world == 1:

@@ -14,7 +14,9 @@ arithmetic on the same inputs, so:
 * J, dJ/dk, dJ/dtau, dJ/dtau_c: the per-warp FP64 slot sums are the same
   numbers, added in another order: relative 1e-10.
 The step count is not a multiple of the checkpoint interval (a partial last
-segment, and recomputed segments before it).
+segment, and recomputed segments before it). With 16-bit stored states (each
+format once; the slabs exchange faces of codes and the adjoint's FP32 scatter
+faces) the same bars hold against the whole-box 16-bit gradient.
 """
 import numpy as np
 import pytest
@@ -28,24 +30,25 @@ from test_gpu_adjoint_reactive import fields
 pytestmark = pytest.mark.gpu
 
 TAU, TAU_C, K = 0.8, 0.7, 0.6
+C0 = 0.5  # shift of 16-bit scalar states
 
 
-def whole_box(fl, real, op, obj, rho, u, a, b, dims, steps, interval):
+def whole_box(fl, real, op, obj, rho, u, a, b, dims, steps, interval, storage=None):
     nx, ny, nz = dims
-    nb = E.reactive_gradient_workspace_bytes(fl, real, nx, ny, nz, steps, interval)
+    nb = E.reactive_gradient_workspace_bytes(fl, real, nx, ny, nz, steps, interval, storage=storage)
     ws = torch.empty(nb, dtype=torch.uint8, device=a.device)
     res = torch.zeros(4, dtype=torch.float64, device=a.device)
     ga, gb, gu = torch.empty_like(a), torch.empty_like(b), torch.empty_like(u)
     E.check(E.reactive_gradient_async(fl, real, op, obj, rho, u, a, b, nx, ny, nz, TAU, TAU_C, K, steps, interval,
-                                      ws, nb, res, ga, gb, gu))
+                                      ws, nb, res, ga, gb, gu, storage=storage, c0=C0))
     torch.cuda.synchronize()
     return res.cpu().numpy(), ga.cpu().numpy(), gb.cpu().numpy(), gu.cpu().numpy()
 
 
-def slabs(fl, real, op, obj, rho, u, a, b, dims, steps, interval, world):
+def slabs(fl, real, op, obj, rho, u, a, b, dims, steps, interval, world, storage=None):
     nx, ny, nz = dims
     grads = [slab.ReactiveSlabGradient(torch, fl, real, op, obj, nx, ny, nz, TAU, TAU_C, K, steps, interval, r, world,
-                                       a.device) for r in range(world)]
+                                       a.device, storage=storage, c0=C0) for r in range(world)]
     inputs = []
     for g in grads:
         sl = slice(g.z0, g.z0 + g.nz)
@@ -60,23 +63,28 @@ def slabs(fl, real, op, obj, rho, u, a, b, dims, steps, interval, world):
 
 
 CASES = [
-    ("D3Q19", "double", "BGK", "mean_product", (12, 6, 8), 7, 3, 2),
-    ("D3Q19", "double", "TRT", "segregation", (12, 6, 8), 7, 3, 4),
-    ("D3Q19", "double", "MRT", "mean_product", (12, 6, 8), 5, 2, 2),
-    ("D3Q19", "double", "BGK", "mean_product", (10, 4, 8), 5, 3, 8),
-    ("D3Q19", "float", "TRT", "mean_product", (16, 6, 6), 7, 3, 1),
-    ("D3Q27", "float", "TRT", "mean_product", (12, 6, 8), 7, 3, 2),
-    ("D3Q27", "double", "BGK", "segregation", (12, 6, 8), 6, 4, 2),
+    ("D3Q19", "double", "BGK", "mean_product", (12, 6, 8), 7, 3, 2, None),
+    ("D3Q19", "double", "TRT", "segregation", (12, 6, 8), 7, 3, 4, None),
+    ("D3Q19", "double", "MRT", "mean_product", (12, 6, 8), 5, 2, 2, None),
+    ("D3Q19", "double", "BGK", "mean_product", (10, 4, 8), 5, 3, 8, None),
+    ("D3Q19", "float", "TRT", "mean_product", (16, 6, 6), 7, 3, 1, None),
+    ("D3Q27", "float", "TRT", "mean_product", (12, 6, 8), 7, 3, 2, None),
+    ("D3Q27", "double", "BGK", "segregation", (12, 6, 8), 6, 4, 2, None),
+    # 16-bit stored states (the forward of the C5 configuration)
+    ("D3Q19", "float", "TRT", "mean_product", (12, 6, 8), 7, 3, 2, "f16s"),
+    ("D3Q19", "float", "MRT", "segregation", (12, 6, 8), 6, 3, 4, "q15s"),
+    ("D3Q19", "float", "BGK", "mean_product", (16, 6, 6), 7, 3, 1, "bf16s"),
+    ("D3Q27", "float", "TRT", "mean_product", (10, 4, 8), 5, 2, 8, "e3m12s"),
 ]
 
 
-@pytest.mark.parametrize("fl,real,op,obj,dims,steps,interval,world", CASES)
-def test_slab_gradient_matches_whole_box(engine, dev, fl, real, op, obj, dims, steps, interval, world):
+@pytest.mark.parametrize("fl,real,op,obj,dims,steps,interval,world,storage", CASES)
+def test_slab_gradient_matches_whole_box(engine, dev, fl, real, op, obj, dims, steps, interval, world, storage):
     nx, ny, nz = dims
     dtype = torch.float32 if real == "float" else torch.float64
     rho, u, a, b = fields(fl, (nz, ny, nx), dev, dtype, seed=91)
-    want = whole_box(fl, real, op, obj, rho, u, a, b, dims, steps, interval)
-    results, ga, gb, gu = slabs(fl, real, op, obj, rho, u, a, b, dims, steps, interval, world)
+    want = whole_box(fl, real, op, obj, rho, u, a, b, dims, steps, interval, storage)
+    results, ga, gb, gu = slabs(fl, real, op, obj, rho, u, a, b, dims, steps, interval, world, storage)
     for r in results[1:]:
         assert np.array_equal(r, results[0]), "ranks disagree on the all-reduced scalars"
     w = want[0]
@@ -96,21 +104,26 @@ def test_slab_gradient_rejects_bad_arguments(engine, dev):
     # D2Q9 has no slab form; D3Q27 MRT has no adjoint
     assert lib.lbm_reactive_slab_slots_bytes(E.LATTICES["D2Q9"], nx, ny, nz) == 0
     p = t.data_ptr()
-    rc = lib.lbm_reactive_slab_forward_async(E.LATTICES["D3Q27"], E.REALS["double"], E.COLLISIONS["MRT"], p, p, p, p,
-                                             p, p, None, args["nx"], args["ny"], args["nz"], TAU, TAU_C, K, p, p, p,
-                                             p, None)
+    rc = lib.lbm_reactive_slab_forward_async(E.LATTICES["D3Q27"], E.REALS["double"], 0, C0, E.COLLISIONS["MRT"], p,
+                                             p, p, p, p, p, None, args["nx"], args["ny"], args["nz"], TAU, TAU_C, K,
+                                             p, p, p, p, None)
+    assert rc != 0
+    # 16-bit states need FP32
+    rc = lib.lbm_reactive_slab_forward_async(E.LATTICES["D3Q19"], E.REALS["double"], E.FORMATS["f16s"], C0,
+                                             E.COLLISIONS["BGK"], p, p, p, p, p, p, None, args["nx"], args["ny"],
+                                             args["nz"], TAU, TAU_C, K, p, p, p, p, None)
     assert rc != 0
     # tau at the stability limit
     f = [torch.zeros((q, nz, ny, nx), dtype=torch.float64, device=dev) for q in (19, 19, 7, 7, 7, 7)]
     n = lib.lbm_fluid_reaction_slab_face_elems(E.LATTICES["D3Q19"], nx, ny)
     h = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(4)]
-    rc = lib.lbm_reactive_slab_forward_async(E.LATTICES["D3Q19"], E.REALS["double"], E.COLLISIONS["BGK"],
+    rc = lib.lbm_reactive_slab_forward_async(E.LATTICES["D3Q19"], E.REALS["double"], 0, C0, E.COLLISIONS["BGK"],
                                              f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), f[3].data_ptr(),
                                              f[4].data_ptr(), f[5].data_ptr(), None, nx, ny, nz, 0.5, TAU_C, K,
                                              h[0].data_ptr(), h[1].data_ptr(), h[2].data_ptr(), h[3].data_ptr(), None)
     assert rc != 0
     # a send buffer aliasing a halo buffer
-    rc = lib.lbm_reactive_slab_forward_async(E.LATTICES["D3Q19"], E.REALS["double"], E.COLLISIONS["BGK"],
+    rc = lib.lbm_reactive_slab_forward_async(E.LATTICES["D3Q19"], E.REALS["double"], 0, C0, E.COLLISIONS["BGK"],
                                              f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr(), f[3].data_ptr(),
                                              f[4].data_ptr(), f[5].data_ptr(), None, nx, ny, nz, TAU, TAU_C, K,
                                              h[0].data_ptr(), h[1].data_ptr(), h[0].data_ptr(), h[3].data_ptr(), None)
@@ -120,7 +133,7 @@ def test_slab_gradient_rejects_bad_arguments(engine, dev):
     slots = torch.zeros(sb // 8, dtype=torch.float64, device=dev)
     lam = [torch.zeros((q, nz, ny, nx), dtype=torch.float64, device=dev) for q in (19, 7, 7, 19, 7, 7)]
     rc = lib.lbm_reactive_slab_adjoint_step_async(
-        E.LATTICES["D3Q19"], E.REALS["double"], E.COLLISIONS["BGK"], f[0].data_ptr(), f[2].data_ptr(),
+        E.LATTICES["D3Q19"], E.REALS["double"], 0, C0, E.COLLISIONS["BGK"], f[0].data_ptr(), f[2].data_ptr(),
         f[3].data_ptr(), h[0].data_ptr(), h[1].data_ptr(), t.data_ptr(), lam[0].data_ptr(), lam[1].data_ptr(),
         lam[2].data_ptr(), lam[3].data_ptr(), lam[4].data_ptr(), lam[5].data_ptr(), f[1].data_ptr(), h[2].data_ptr(),
         h[3].data_ptr(), nx, ny, nz, TAU, TAU_C, K, slots.data_ptr(), sb - 8, None)
