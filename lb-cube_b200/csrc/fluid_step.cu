@@ -36,8 +36,12 @@ cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, 
       return cudaGetLastError();
     }
   }
-  fluid_step_kernel<L, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(cur, nxt, g, omega,
-                                                                         omega_minus);
+  if constexpr (kUsePlanes<L, Real, CT>)
+    fluid_step_planes_kernel<L, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(
+        planes_of<const Real, L::Q>(cur, g), planes_of<Real, L::Q>(nxt, g), g, omega, omega_minus);
+  else
+    fluid_step_kernel<L, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(cur, nxt, g, omega,
+                                                                           omega_minus);
   return cudaGetLastError();
 }
 

@@ -68,6 +68,56 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// The Q population planes of a buffer as separate base pointers, passed as
+// kernel parameters (read from the constant bank): every gather and store is
+// then one wide multiply-add of a 32-bit in-plane offset, where base + plane * i
+// otherwise costs 64-bit arithmetic per population. Used for MRT on D3Q19 and
+// D3Q27, where it measured faster (A/B, same box, bit-identical outputs:
+// D3Q19 FP64 MRT 0.94 -> 0.98 of the copy bandwidth at 256^3, D3Q27 FP32 MRT
+// 0.56 -> 0.585 at 224^3; D3Q19 FP32 MRT and D3Q27 BGK level; RLBM 1.5-7 % and
+// D2Q9 MRT 2.5 % slower, so those keep fluid_step_kernel). LBCUBE_PLANE_PTRS = 0
+// turns it off.
+#ifndef LBCUBE_PLANE_PTRS
+#define LBCUBE_PLANE_PTRS 1
+#endif
+template <class L, class Real, int CT>
+constexpr bool kUsePlanes = LBCUBE_PLANE_PTRS != 0 && CT == kMRT && L::Q >= 19;
+template <class Real, int Q>
+struct Planes {
+  Real* p[Q];
+};
+template <class Real, int Q>
+inline Planes<Real, Q> planes_of(Real* base, const Grid& g) {
+  Planes<Real, Q> r;
+  for (int i = 0; i < Q; ++i) r.p[i] = base + (size_t)g.plane * i;
+  return r;
+}
+
+// fluid_step_kernel (no diagnostics) on plane pointers: the same gather,
+// collision and stores, so the same bits.
+template <class L, class Real, int CT>
+__global__ void __launch_bounds__(kThreads)
+    fluid_step_planes_kernel(const Planes<const Real, L::Q> cur, const Planes<Real, L::Q> nxt,
+                             Grid g, Real omega, Real omega_minus) {
+  int x, y, z;
+  if (!cell_of(g, x, y, z)) return;
+  const int xm = x == 0 ? g.nx - 1 : x - 1, xp = x == g.nx - 1 ? 0 : x + 1;
+  const int ym = y == 0 ? g.ny - 1 : y - 1, yp = y == g.ny - 1 ? 0 : y + 1;
+  const int zm = z == 0 ? g.nz - 1 : z - 1, zp = z == g.nz - 1 ? 0 : z + 1;
+  Real f[L::Q];
+  static_for<L::Q>([&](auto I) {
+    constexpr int i = LB_I(I);
+    constexpr int cx = L::c[i][0], cy = L::c[i][1], cz = L::c[i][2];
+    const int sx = cx == 0 ? x : (cx > 0 ? xm : xp);
+    const int sy = cy == 0 ? y : (cy > 0 ? ym : yp);
+    const int sz = cz == 0 ? z : (cz > 0 ? zm : zp);
+    f[i] = __ldg(cur.p[i] + ((sz * g.ny + sy) * g.nx + sx));
+  });
+  collide<L, Real, CT>(f, omega, omega_minus);
+  const int cell = (z * g.ny + y) * g.nx + x;
+  static_for<L::Q>([&](auto I) { nxt.p[LB_I(I)][cell] = f[LB_I(I)]; });
+}
+
 // Cells per thread of the vectorised kernel, measured fastest on B200 at 256^3:
 // 2 FP32 D2Q9 / D3Q19 cells (8-byte words; D3Q19 TRT 0.99 of the copy
 // bandwidth against 0.80 at V = 4 and 0.76 at V = 1), 1 D3Q27 FP32 cell (BGK
