@@ -1,6 +1,7 @@
 """CPU: the z-slab decomposition's host side with gloo ranks (world size 2 and
 3). The face exchange delivers each neighbour's send buffers into the right
-halo buffers, and a streaming step assembled from slabs (a numpy restatement
+halo buffers (also through host staging, alternating face buffers of two
+element types), and a streaming step assembled from slabs (a numpy restatement
 of the slab kernel's pull: halo_lo for c_z = +1 at plane 0, halo_hi for c_z = -1
 at the top plane) equals the periodic streaming of the whole box."""
 import os
@@ -98,6 +99,56 @@ def test_slab_exchange_and_streaming_gloo(world):
         assert not err, err
         assert ok1, f"rank {rank}: halos do not hold the neighbours' send buffers"
         assert ok2, f"rank {rank}: slab streaming differs from the periodic box"
+
+
+def _host_worker(rank, world, port, q):
+    """HostExchange alternating two kinds of face buffer (16-bit codes and FP64,
+    as the slab reactive gradient does): each exchange must deliver the
+    neighbours' buffers of the kind in use."""
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "lb-cube_b200"))
+    import slab
+
+    try:
+        dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+        d = slab.SlabDomain(torch, "D3Q19", "double", "BGK", NX, NY, NZ, 1.0, rank, world, "cpu")
+        n = d.send_lo.numel()
+        kinds = {"codes": tuple(torch.zeros(n, dtype=torch.int16) for _ in range(4)),
+                 "real": (d.halo_lo, d.halo_hi, d.send_lo, d.send_hi)}
+        ex = slab.HostExchange(dist)
+        lower, upper = (rank - 1) % world, (rank + 1) % world
+        ok = True
+        for step, kind in enumerate(["codes", "real", "codes", "real"]):
+            d.halo_lo, d.halo_hi, d.send_lo, d.send_hi = kinds[kind]
+            dt = d.send_lo.dtype
+            tag = lambda r, side: (torch.arange(n) % 97 + 100 * r + 10 * side + step).to(dt)
+            d.send_lo.copy_(tag(rank, 0))
+            d.send_hi.copy_(tag(rank, 1))
+            ex.exchange(d)
+            ok = ok and torch.equal(d.halo_lo, tag(lower, 1)) and torch.equal(d.halo_hi, tag(upper, 0))
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put((rank, bool(ok), ""))
+    except Exception as e:  # reported to the parent
+        q.put((rank, False, repr(e)))
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_host_exchange_two_face_kinds_gloo(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_host_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+    for rank, ok, err in sorted(res):
+        assert not err, err
+        assert ok, f"rank {rank}: a halo does not hold its neighbour's send buffer of the same kind"
 
 
 def test_slab_domain_rejects_bad_splits():
