@@ -144,6 +144,40 @@ def _stochastic(fmt, lat, op):
     return fmt in ("f16s", "bf16s") and (op in ("BGK", "TRT") or (op == "MRT" and lat != "D3Q27"))
 
 
+@pytest.mark.parametrize("nx", [512, 1024])
+@pytest.mark.parametrize("fmt,op", [("f16s", "TRT"), ("q15s", "MRT")])
+def test_shifted_step_wide_rows(engine, dev, nx, fmt, op):
+    """Rows of 512 and 1024 cells: the row-staged D3Q19 kernel then holds 58 KB and
+    117 KB of shared memory (more than the 48 KB default). One step is the
+    rounded FP32 step to the bound above, and a second run gives the same bits."""
+    lat, ny, nz = "D3Q19", 4, 3
+    f = torch.from_numpy(U.random_state(lat, nx, ny, nz, np.float32, seed=12)).to(dev)
+    h0 = torch.empty(f.shape, dtype=torch.int16, device=dev)
+    engine.check(engine.encode_shifted_async(lat, fmt, "float", f, h0, nx, ny, nz, 1.0))
+    f0 = torch.empty_like(f)
+    engine.check(engine.decode_shifted_async(lat, fmt, "float", h0, f0, nx, ny, nz, 1.0))
+    f1 = torch.empty_like(f)
+    engine.check(engine.launch_step_gpu(lat, "float", op, f0, f1, nx, ny, nz, 1 / 0.6))
+    want_f = torch.empty_like(f)
+    want = torch.empty_like(h0)
+    engine.check(engine.encode_shifted_async(lat, fmt, "float", f1, want, nx, ny, nz, 1.0))
+    engine.check(engine.decode_shifted_async(lat, fmt, "float", want, want_f, nx, ny, nz, 1.0))
+    runs = []
+    for _ in range(2):
+        h1 = torch.full_like(h0, -1)
+        engine.check(engine.step_shifted_async(lat, fmt, op, h0, h1, nx, ny, nz, 1 / 0.6, 1.0))
+        runs.append(h1)
+    assert engine.stage_timeouts(reset=True) == 0
+    got_f = torch.empty_like(f)
+    engine.check(engine.decode_shifted_async(lat, fmt, "float", runs[0], got_f, nx, ny, nz, 1.0))
+    torch.cuda.synchronize()
+    assert torch.equal(runs[0], runs[1])
+    w = _w(lat).to(dev).view(-1, 1)
+    dv = (got_f.double() - want_f.double()).abs().view(19, -1) / w
+    step = ULP[fmt] * (want_f.double().view(19, -1) / w - 1.0).abs() * 2 + 2 * ABS_FLOOR[fmt] + 2e-6
+    assert bool((dv <= step).all()), float((dv - step).max())
+
+
 def test_shifted_rejects_unaligned_extent(engine, dev):
     h = torch.zeros((19, 4, 4, 30), dtype=torch.int16, device=dev)
     g = torch.empty_like(h)
