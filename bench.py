@@ -426,6 +426,65 @@ def blob_fields(torch, dev, n, block, seed):
     return a.contiguous(), (1.0 - a).contiguous()
 
 
+def run_slab_gradient(torch, E, dev, n=160, steps=600, interval=100, world=2, tau=0.56, tau_c=0.55,
+                      k=0.03 / 16, storage="f16s", c0=0.5):
+    """The reactive gradient of run_reactive_adjoint_cost decomposed into `world`
+    z-slabs (slab.ReactiveSlabGradient), all ranks in this process on this GPU
+    (slab.run_local: faces exchanged by device copies, all-reduces as sums),
+    against the same gradient of the whole box (lbm_reactive_gradient_async).
+    Both timed by CUDA events around the whole call, host sequencing included;
+    the slab path issues every rank's launches from this one process and runs
+    them one after the other on this GPU, so the ratio is the cost of the
+    decomposition (exchanges, unpacks, twice the launches from one host
+    thread), not a multi-GPU speed-up. The slab's initial-state gradients
+    must equal the whole box's bit for bit."""
+    import slab
+
+    u0 = solenoidal_field(torch, dev, n, 0.03, 4.0, SEED).float()
+    rho0 = torch.ones((n, n, n), dtype=torch.float32, device=dev)
+    a0, b0 = blob_fields(torch, dev, n, 16, SEED)
+    nbytes = E.reactive_gradient_workspace_bytes("D3Q19", "float", n, n, n, steps, interval, storage=storage)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    res = torch.zeros(4, dtype=torch.float64, device=dev)
+    ga, gb, gu = torch.empty_like(a0), torch.empty_like(b0), torch.empty_like(u0)
+    grads = [slab.ReactiveSlabGradient(torch, "D3Q19", "float", "TRT", "mean_product", n, n, n, tau, tau_c, k,
+                                       steps, interval, r, world, dev, storage=storage, c0=c0)
+             for r in range(world)]
+    inputs = [(rho0[g.z0:g.z0 + g.nz].contiguous(), u0[:, g.z0:g.z0 + g.nz].contiguous(),
+               a0[g.z0:g.z0 + g.nz].contiguous(), b0[g.z0:g.z0 + g.nz].contiguous()) for g in grads]
+
+    def whole():
+        E.check(E.reactive_gradient_async("D3Q19", "float", "TRT", "mean_product", rho0, u0, a0, b0, n, n, n,
+                                          tau, tau_c, k, steps, interval, ws, nbytes, res, ga, gb, gu,
+                                          storage=storage, c0=c0))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        fn()
+        t1.record()
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1)
+
+    whole()  # warm-up
+    slab.run_local(grads, inputs)
+    whole_ms = timed(whole)
+    slab_ms = timed(lambda: slab.run_local(grads, inputs))
+    same = all(bool(torch.equal(torch.cat([getattr(g, name) for g in grads], dim=axis).view(torch.int32),
+                                want.view(torch.int32)))
+               for name, axis, want in (("grad_a0", 0, ga), ("grad_b0", 0, gb), ("grad_u0", 1, gu)))
+    rel = max(abs(float(x) - float(y)) / max(abs(float(y)), 1e-300)
+              for x, y in zip(grads[0].result.tolist(), res.tolist()))
+    store = "FP32" if storage is None else f"{FORMAT_NOTE[storage]} populations (scalars shifted by {c0})"
+    return {"config": f"the reactive gradient of adjoint_reactive at {n}^3, {steps} steps, checkpoint every "
+                      f"{interval}, {store}, as {world} z-slabs of {n // world} planes stepped in one process",
+            "whole_box_ms": round(whole_ms, 2), "slabs_ms": round(slab_ms, 2),
+            "slabs_over_whole_box": round(slab_ms / whole_ms, 3),
+            "gradient_fields_bit_identical": same, "scalars_max_rel_diff": rel}
+
+
 def run_reactive_adjoint_cost(torch, E, dev, n=192, steps=3000, interval=100, tau=0.56, tau_c=0.55,
                               k=0.03 / 16, storage=None, c0=0.5):
     """Reactive adjoint cost: D3Q19 TRT + two D3Q7 scalars (A + B -> C), FP32
@@ -854,6 +913,7 @@ def run_engine(args, rank, world, local_rank):
     peak, peak_kind = measured_hbm_peak()
     traffic = committed_traffic(f"d3q19_float_trt_{NX}") if storage == "fp32" and OP == "TRT" else None
     variants = accuracy = fp16_store = adjoint = adjoint_reactive = adjoint_reactive_16 = mixing = None
+    slab_gradient = None
     if world == 1 and not args.no_variants and storage == "fp32" and OP == "TRT":
         variants = run_variants(torch, E, dev, f, peak, ms_per_step)
         del f, g
@@ -870,6 +930,7 @@ def run_engine(args, rank, world, local_rank):
         # the same gradient against the FP32 forward run of the configuration
         adjoint_reactive_16["cost_ratio_vs_fp32_forward"] = round(adjoint_reactive_16["gradient_ms"] /
                                                                   adjoint_reactive["forward_ms"], 3)
+        slab_gradient = run_slab_gradient(torch, E, dev)
         mixing = run_reactive_mixing(torch, E, dev)
         # per operator: the fastest 16-bit format meeting the 1e-3 velocity error
         # bar, with its speed-up over FP32 storage of the same operator
@@ -897,7 +958,7 @@ def run_engine(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": bytes_per_lu * cells},
         "e2e": e2e, "clocks": clocks, "gpu_launches": args.steps * launches_per_step,
         "fp16_store": fp16_store, "adjoint": adjoint, "adjoint_reactive": adjoint_reactive,
-        "adjoint_reactive_f16s": adjoint_reactive_16,
+        "adjoint_reactive_f16s": adjoint_reactive_16, "slab_gradient": slab_gradient,
         "reactive_mixing": mixing,
         "variants": variants, "accuracy": accuracy,
     }

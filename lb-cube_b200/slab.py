@@ -204,10 +204,10 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
     as the forward step's), ("allreduce", t) for an in-place sum of the FP64
     device tensor t over ranks. run() serves those yields for one rank of a
     process group; run_local() steps the slabs of one process in lockstep.
-    Per forward step one exchange; per adjoint step two (the stored state's
-    faces for the pulls, then the adjoint scatter's sends) and an unpack of the
-    received scatter faces. Given the same seed the adjoint fields and the
-    initial-state gradients are bit-identical to the whole box's."""
+    Per forward step one exchange, whose halos are kept with the state it
+    produced; per adjoint step one (the adjoint scatter's sends) and an unpack
+    of the received scatter faces. Given the same seed the adjoint fields and
+    the initial-state gradients are bit-identical to the whole box's."""
 
     def __init__(self, torch, lattice, real, collision, objective, nx, ny, nz_global, tau, tau_c, k, steps, interval,
                  rank, world, device, storage=None, c0=0.5):
@@ -232,16 +232,23 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
         def field(qq, dt=dtype):
             return torch.empty((qq,) + shape, dtype=dt, device=device)
 
-        def state():
-            return (field(q, sdtype), field(7, sdtype), field(7, sdtype), field(3))
-
-        # face buffers: the stored states' (forward steps, packs) and the
-        # adjoint's (scatter sends, in `real`); exchanges move whichever set is
-        # current in halo_lo / halo_hi / send_lo / send_hi
         n = E.load().lbm_fluid_reaction_slab_face_elems(E.LATTICES[lattice], nx, ny)
+
+        def state():
+            # fluid, A, B, the advecting velocity that produced it, and the two
+            # halos the forward step that produced it received: every step that
+            # pulls from the state (forward or adjoint) reads them, so the
+            # backward sweep exchanges no state faces
+            return (field(q, sdtype), field(7, sdtype), field(7, sdtype), field(3),
+                    torch.empty(n, dtype=sdtype, device=device), torch.empty(n, dtype=sdtype, device=device))
+
+        # face buffers: the states' sends (forward steps, packs; the received
+        # halos land in the produced state's own halo buffers) and the
+        # adjoint's scatter faces (in `real`); an exchange moves whichever set
+        # is current in halo_lo / halo_hi / send_lo / send_hi
         self._lam_faces = (self.halo_lo, self.halo_hi, self.send_lo, self.send_hi)
-        self._state_faces = self._lam_faces if self.storage == 0 else tuple(
-            torch.empty(n, dtype=sdtype, device=device) for _ in range(4))
+        self._state_sends = (self.send_lo, self.send_hi) if self.storage == 0 else tuple(
+            torch.empty(n, dtype=sdtype, device=device) for _ in range(2))
 
         nseg = (self.steps + self.interval - 1) // self.interval
         self.nseg = nseg
@@ -262,13 +269,19 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
         self.result = torch.empty(4, dtype=torch.float64, device=device)
 
     # ---- the per-step entries
-    def _faces(self, which):
-        self.halo_lo, self.halo_hi, self.send_lo, self.send_hi = (
-            self._state_faces if which == "state" else self._lam_faces)
+    def _faces(self, target=None):
+        """The face buffers of the next exchange: a state's (the states' sends
+        in, `target`'s halos out) or, with no target, the adjoint's."""
+        if target is None:
+            self.halo_lo, self.halo_hi, self.send_lo, self.send_hi = self._lam_faces
+        else:
+            self.send_lo, self.send_hi = self._state_sends
+            self.halo_lo, self.halo_hi = target[4], target[5]
 
     def pack(self, state, stream=None):
-        """Faces of a stored state (fluid, a, b) into the state send buffers."""
-        self._faces("state")
+        """Faces of a stored state into the state send buffers (its halos come
+        back into its own halo buffers at the next exchange)."""
+        self._faces(state)
         f, a, b = state[:3]
         E.check(E.load().lbm_reactive_slab_pack_async(
             E.LATTICES[self.lattice], E.REALS[self.real], self.storage, f.data_ptr(), a.data_ptr(), b.data_ptr(),
@@ -276,29 +289,30 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
             "reactive slab pack")
 
     def _forward(self, cur, nxt, keep_u, stream=None):
-        self._faces("state")
+        """One step cur -> nxt (pulling across the faces from cur's halos); the
+        next exchange delivers nxt's halos."""
+        self._faces(nxt)
         E.check(E.load().lbm_reactive_slab_forward_async(
             E.LATTICES[self.lattice], E.REALS[self.real], self.storage, self.c0, E.COLLISIONS[self.collision],
             cur[0].data_ptr(),
             nxt[0].data_ptr(), cur[1].data_ptr(), nxt[1].data_ptr(), cur[2].data_ptr(), nxt[2].data_ptr(),
             nxt[3].data_ptr() if keep_u else None, self.nx, self.ny, self.nz, self.tau, self.tau_c, self.k,
-            self.halo_lo.data_ptr(), self.halo_hi.data_ptr(), self.send_lo.data_ptr(), self.send_hi.data_ptr(),
+            cur[4].data_ptr(), cur[5].data_ptr(), self.send_lo.data_ptr(), self.send_hi.data_ptr(),
             E._stream(stream)), "reactive slab forward step")
 
     def _adjoint(self, sn, u_next, ln, l, stream=None):
-        # reads the state halos (exchanged after pack), writes the adjoint's sends
-        halo_lo, halo_hi = self._state_faces[0], self._state_faces[1]
-        self._faces("lambda")
+        # pulls from state n across the faces through its stored halos; writes the adjoint's sends
+        self._faces()
         E.check(E.load().lbm_reactive_slab_adjoint_step_async(
             E.LATTICES[self.lattice], E.REALS[self.real], self.storage, self.c0, E.COLLISIONS[self.collision],
-            sn[0].data_ptr(), sn[1].data_ptr(), sn[2].data_ptr(), halo_lo.data_ptr(), halo_hi.data_ptr(),
+            sn[0].data_ptr(), sn[1].data_ptr(), sn[2].data_ptr(), sn[4].data_ptr(), sn[5].data_ptr(),
             u_next.data_ptr(), ln[0].data_ptr(), ln[1].data_ptr(), ln[2].data_ptr(), l[0].data_ptr(),
             l[1].data_ptr(), l[2].data_ptr(), self.ubar.data_ptr(), self.send_lo.data_ptr(),
             self.send_hi.data_ptr(), self.nx, self.ny, self.nz, self.tau, self.tau_c, self.k, self.slots.data_ptr(),
             self.slots_bytes, E._stream(stream)), "reactive slab adjoint step")
 
     def _unpack(self, l, stream=None):
-        self._faces("lambda")
+        self._faces()
         E.check(E.load().lbm_reactive_slab_adjoint_unpack_async(
             E.LATTICES[self.lattice], E.REALS[self.real], self.halo_lo.data_ptr(), self.halo_hi.data_ptr(),
             l[0].data_ptr(), l[1].data_ptr(), l[2].data_ptr(), self.nx, self.ny, self.nz, E._stream(stream)),
@@ -334,7 +348,7 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
             for lat, src, dst, ref in ((L, fi, s0[0], 1.0), (SL, ai, s0[1], self.c0), (SL, bi, s0[2], self.c0)):
                 E.check(lib.lbm_encode_shifted_async(lat, self.storage, P, src.data_ptr(), dst.data_ptr(), nx, ny,
                                                      nz, ref, None), "encode")
-        self.pack(s0[:3])
+        self.pack(s0)
         yield ("exchange",)
         last0 = (nseg - 1) * interval
         cur = s0
@@ -379,21 +393,16 @@ class ReactiveSlabGradient(ReactiveSlabDomain):
         # backward sweep, segment by segment from the last
         for kk in range(nseg - 1, -1, -1):
             n0, n1 = kk * interval, min(steps, (kk + 1) * interval)
-            if kk < nseg - 1 and n1 - n0 > 1:  # recompute the segment's states from its checkpoint
+            if kk < nseg - 1:  # recompute the segment's states (and their halos) from its checkpoint
                 src = ckpt[kk]
-                self.pack(src[:3])
-                yield ("exchange",)
                 for n in range(n0 + 1, n1):
                     self._forward(src, seg[n - n0], True)
-                    if n + 1 < n1:
-                        yield ("exchange",)
+                    yield ("exchange",)
                     src = seg[n - n0]
             for n in range(n1 - 1, n0 - 1, -1):
                 sn = ckpt[kk] if n == n0 else seg[n - n0]
                 sn1 = ckpt[kk + 1] if n + 1 == n1 else seg[n + 1 - n0]  # holds u^{n+1}
                 ln, l = self.lam[(n + 1) % 2], self.lam[n % 2]
-                self.pack(sn[:3])
-                yield ("exchange",)
                 self._adjoint(sn, sn1[3], ln, l)
                 yield ("exchange",)
                 self._unpack(l)
