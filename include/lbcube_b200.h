@@ -560,8 +560,10 @@ int lbm_fluid_reaction_slab_pack_async(int fluid_lattice, int precision, const v
  *   forward step  lbm_reactive_slab_forward_async (velocity, [3, Z, Y, X] in the
  *                 precision, may be null for states the backward sweep
  *                 recomputes), then an exchange;
- *   adjoint step  n (state n and u^{n+1} stored): lbm_reactive_slab_pack_async
- *                 of state n + exchange (its halos), then
+ *   adjoint step  n (state n and u^{n+1} stored): state n's halos (those the
+ *                 exchange after the step that produced it delivered, kept with
+ *                 the state; or lbm_reactive_slab_pack_async of state n and an
+ *                 exchange), then
  *                 lbm_reactive_slab_adjoint_step_async (lambda^{n+1} ->
  *                 lambda^n; velocity_adjoint is [3, Z, Y, X] scratch; adds to
  *                 the per-warp slots of lbm_reactive_slab_slots_bytes, zeroed
