@@ -4,10 +4,12 @@
 // and compute_max_velocity (src/turbulent_tgv_3d.cpp:150-173), which need the
 // whole population field copied to the host (src/main.cpp:595-606). Pass 1
 // reads the Q populations of every cell once (one cell per thread, coalesced
-// rows) and writes per-block partials; pass 2 (one block) adds them in a fixed
-// order. The host reads five doubles instead of Q values per cell. The fused
+// rows) and writes per-block partials; pass 2 (one cluster of blocks) adds them
+// in a fixed order. The host reads five doubles instead of Q values per cell. The fused
 // form, one collide-stream step that also reduces the diagnostics of the state
 // it writes, is lbm_step_diagnostics_async (fluid_step.cu).
+#include <cooperative_groups.h>
+
 #include "collide.cuh"
 #include "common.cuh"
 #include "diag.cuh"
@@ -31,13 +33,21 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 constexpr int kDiagFinalThreads = 1024;
+// Blocks of the second pass: one thread-block cluster, each block taking every
+// kDiagFinalBlocks-th run of kDiagFinalThreads partials; the blocks' totals
+// meet in rank order through distributed shared memory (a fixed order).
+#ifndef LBCUBE_FINAL_BLOCKS
+#define LBCUBE_FINAL_BLOCKS 8
+#endif
+constexpr int kDiagFinalBlocks = LBCUBE_FINAL_BLOCKS;
 
-__global__ void __launch_bounds__(kDiagFinalThreads)
+__global__ void __cluster_dims__(kDiagFinalBlocks, 1, 1) __launch_bounds__(kDiagFinalThreads)
     diag_finalize_kernel(const double* __restrict__ partials, long long count,
                          double speed_limit, double* __restrict__ out) {
   __shared__ double sh[kDiagFinalThreads][kDiagPartials];
   double m = 0.0, k = 0.0, n = 0.0, v = 0.0;
-  for (long long b = threadIdx.x; b < count; b += kDiagFinalThreads) {
+  for (long long b = (long long)blockIdx.x * kDiagFinalThreads + threadIdx.x; b < count;
+       b += (long long)kDiagFinalBlocks * kDiagFinalThreads) {
     m += partials[b * kDiagPartials + 0];
     k += partials[b * kDiagPartials + 1];
     n += partials[b * kDiagPartials + 2];
@@ -57,10 +67,28 @@ __global__ void __launch_bounds__(kDiagFinalThreads)
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    const double vmax = sh[0][3], nonfinite = sh[0][2];
-    out[0] = sh[0][0];
-    out[1] = sh[0][1];
+  bool holder = threadIdx.x == 0;
+  double tot[kDiagPartials] = {sh[0][0], sh[0][1], sh[0][2], sh[0][3]};
+  if constexpr (kDiagFinalBlocks > 1) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    holder = holder && cluster.block_rank() == 0;
+    if (holder) {
+      for (unsigned int r = 1; r < (unsigned int)kDiagFinalBlocks; ++r) {
+        const double* remote = cluster.map_shared_rank(&sh[0][0], r);
+        tot[0] += remote[0];
+        tot[1] += remote[1];
+        tot[2] += remote[2];
+        tot[3] = fmax(tot[3], remote[3]);
+      }
+    }
+    cluster.sync();
+  }
+  if (holder) {
+    const double vmax = tot[3], nonfinite = tot[2];
+    out[0] = tot[0];
+    out[1] = tot[1];
     out[2] = vmax;
     out[3] = nonfinite;
     out[4] = (nonfinite > 0.0 || vmax > speed_limit) ? 1.0 : 0.0;
@@ -69,7 +97,7 @@ __global__ void __launch_bounds__(kDiagFinalThreads)
 
 cudaError_t launch_diag_finalize(const double* partials, long long count, double speed_limit,
                                  double* out, cudaStream_t s) {
-  diag_finalize_kernel<<<1, kDiagFinalThreads, 0, s>>>(partials, count, speed_limit, out);
+  diag_finalize_kernel<<<kDiagFinalBlocks, kDiagFinalThreads, 0, s>>>(partials, count, speed_limit, out);
   return cudaGetLastError();
 }
 

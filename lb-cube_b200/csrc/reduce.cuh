@@ -1,8 +1,8 @@
 // Deterministic FP64 block reductions for the statistics epilogues.
 //
-// Every block writes one partial per quantity; a single-block second pass sums
-// the partials in a fixed order. No atomics, so the result is identical from
-// run to run for a given domain.
+// Every block writes one partial per quantity; a second pass (one cluster of
+// blocks, stats.cu / diag.cu) sums the partials in a fixed order. No atomics,
+// so the result is identical from run to run for a given domain.
 #pragma once
 
 #include "common.cuh"

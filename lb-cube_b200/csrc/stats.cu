@@ -3,9 +3,11 @@
 //
 // Pass 1 (stats_partials_kernel, or the epilogue of fluid_reaction_kernel)
 // writes per-block FP64 sums of C_A, C_B, C_A^2, C_B^2, C_A C_B. Pass 2
-// (stats_finalize_kernel, one block) adds the partials in a fixed order and
+// (stats_finalize_kernel, one cluster of blocks) adds the partials in a fixed order and
 // forms the eight ReactiveDiagnostics fields (lattice_io.hpp:148-166) with the
 // reference's formulas (:318-337), in FP64.
+#include <cooperative_groups.h>
+
 #include "collide.cuh"
 #include "common.cuh"
 #include "reduce.cuh"
@@ -40,14 +42,27 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 constexpr int kFinalThreads = 1024;
+// Blocks of the second pass: one thread-block cluster (distributed shared
+// memory), each block taking every kFinalBlocks-th run of kFinalThreads
+// partials, so a pass over the 8 192 partials of a 1024^2 launch is one load
+// per thread instead of eight dependent ones. LBCUBE_FINAL_BLOCKS = 1: one block.
+#ifndef LBCUBE_FINAL_BLOCKS
+#define LBCUBE_FINAL_BLOCKS 8
+#endif
+constexpr int kFinalBlocks = LBCUBE_FINAL_BLOCKS;
 
-// Adds the partials in a fixed order; thread 0 returns the five sums in s.
-__device__ __forceinline__ void sum_partials(const double* __restrict__ partials, long long blocks,
+// Adds the partials in a fixed order (per thread the partials
+// blockIdx.x * kFinalThreads + threadIdx.x + j * kFinalBlocks * kFinalThreads
+// in ascending j, then a fixed tree within each block, then the blocks' totals
+// in rank order); returns true in the one thread that holds the five sums in s.
+// Every thread of the cluster must call it.
+__device__ __forceinline__ bool sum_partials(const double* __restrict__ partials, long long blocks,
                                              double (&s)[kStatSums]) {
   __shared__ double sh[kFinalThreads][kStatSums];
 #pragma unroll
   for (int q = 0; q < kStatSums; ++q) s[q] = 0.0;
-  for (long long blk = threadIdx.x; blk < blocks; blk += kFinalThreads) {
+  for (long long blk = (long long)blockIdx.x * kFinalThreads + threadIdx.x; blk < blocks;
+       blk += (long long)kFinalBlocks * kFinalThreads) {
 #pragma unroll
     for (int q = 0; q < kStatSums; ++q) s[q] += partials[blk * kStatSums + q];
   }
@@ -61,8 +76,27 @@ __device__ __forceinline__ void sum_partials(const double* __restrict__ partials
     }
     __syncthreads();
   }
+  if constexpr (kFinalBlocks == 1) {
 #pragma unroll
-  for (int q = 0; q < kStatSums; ++q) s[q] = sh[0][q];
+    for (int q = 0; q < kStatSums; ++q) s[q] = sh[0][q];
+    return threadIdx.x == 0;
+  } else {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();  // every block's total is in its shared memory
+    const bool holder = cluster.block_rank() == 0 && threadIdx.x == 0;
+    if (holder) {
+#pragma unroll
+      for (int q = 0; q < kStatSums; ++q) s[q] = sh[0][q];
+      for (unsigned int r = 1; r < (unsigned int)kFinalBlocks; ++r) {
+        const double* remote = cluster.map_shared_rank(&sh[0][0], r);
+#pragma unroll
+        for (int q = 0; q < kStatSums; ++q) s[q] += remote[q];
+      }
+    }
+    cluster.sync();  // the other blocks keep their shared memory until it has been read
+    return holder;
+  }
 }
 
 // The eight ReactiveDiagnostics fields from the five sums over `cells` cells
@@ -85,25 +119,23 @@ __device__ __forceinline__ void diagnostics_from_sums(const double (&s)[kStatSum
   out[7] = k * ma * mb;
 }
 
-__global__ void __launch_bounds__(kFinalThreads)
+__global__ void __cluster_dims__(kFinalBlocks, 1, 1) __launch_bounds__(kFinalThreads)
     stats_finalize_kernel(const double* __restrict__ partials, long long blocks, long long cells,
                           double k, double* __restrict__ out) {
   double s[kStatSums];
-  sum_partials(partials, blocks, s);
-  if (threadIdx.x == 0) diagnostics_from_sums(s, (double)cells, k, out);
+  if (sum_partials(partials, blocks, s)) diagnostics_from_sums(s, (double)cells, k, out);
 }
 
 // Finalize into the next row of a device table: row *row_counter (if below
 // rows), then the counter advances. The destination is read on the device, so
 // a captured sequence of steps plus this launch can be replayed to fill
 // successive rows.
-__global__ void __launch_bounds__(kFinalThreads)
+__global__ void __cluster_dims__(kFinalBlocks, 1, 1) __launch_bounds__(kFinalThreads)
     stats_append_kernel(const double* __restrict__ partials, long long blocks, long long cells,
                         double k, double* __restrict__ table, unsigned long long rows,
                         unsigned long long* __restrict__ row_counter) {
   double s[kStatSums];
-  sum_partials(partials, blocks, s);
-  if (threadIdx.x == 0) {
+  if (sum_partials(partials, blocks, s)) {
     const unsigned long long row = *row_counter;
     if (row < rows) diagnostics_from_sums(s, (double)cells, k, table + row * 8);
     *row_counter = row + 1;
@@ -111,11 +143,10 @@ __global__ void __launch_bounds__(kFinalThreads)
 }
 
 // The five sums alone: a rank's share of the statistics of a decomposed domain.
-__global__ void __launch_bounds__(kFinalThreads)
+__global__ void __cluster_dims__(kFinalBlocks, 1, 1) __launch_bounds__(kFinalThreads)
     stats_sums_kernel(const double* __restrict__ partials, long long blocks, double* __restrict__ out) {
   double s[kStatSums];
-  sum_partials(partials, blocks, s);
-  if (threadIdx.x == 0) {
+  if (sum_partials(partials, blocks, s)) {
 #pragma unroll
     for (int q = 0; q < kStatSums; ++q) out[q] = s[q];
   }
@@ -131,7 +162,7 @@ __global__ void stats_from_sums_kernel(const double* __restrict__ sums, double c
 
 cudaError_t launch_finalize(const Grid& g, double k, const double* partials, double* out,
                             cudaStream_t s) {
-  stats_finalize_kernel<<<1, kFinalThreads, 0, s>>>(partials, g.blocks(), g.plane, k, out);
+  stats_finalize_kernel<<<kFinalBlocks, kFinalThreads, 0, s>>>(partials, g.blocks(), g.plane, k, out);
   return cudaGetLastError();
 }
 
@@ -230,7 +261,7 @@ extern "C" int lbm_reactive_stats_append_async(int fluid_lattice, int precision,
   const Span writes[2] = {{table, table_rows * 8 * sizeof(double)}, {row_counter, sizeof(unsigned long long)}};
   if (any_overlap(reads, writes)) return (int)cudaErrorInvalidValue;
   const double k = precision == LBM_FLOAT ? (double)(float)k_react : k_react;
-  stats_append_kernel<<<1, kFinalThreads, 0, as_stream(stream)>>>(partials, g.blocks(), g.plane, k, table,
+  stats_append_kernel<<<kFinalBlocks, kFinalThreads, 0, as_stream(stream)>>>(partials, g.blocks(), g.plane, k, table,
                                                                   table_rows, row_counter);
   return (int)cudaGetLastError();
 }
@@ -249,7 +280,7 @@ extern "C" int lbm_reactive_stats_sums_async(int fluid_lattice, size_t x_extent,
                                     x_extent, y_extent, z_extent, g);
   if (err != cudaSuccess) return (int)err;
   if (partials_bytes < (size_t)g.blocks() * kStatSums * sizeof(double)) return (int)cudaErrorInvalidValue;
-  stats_sums_kernel<<<1, kFinalThreads, 0, as_stream(stream)>>>(partials, g.blocks(), sums);
+  stats_sums_kernel<<<kFinalBlocks, kFinalThreads, 0, as_stream(stream)>>>(partials, g.blocks(), sums);
   return (int)cudaGetLastError();
 }
 
