@@ -520,6 +520,12 @@ int lbm_step_slab_async(int lattice, int precision, int collision,
     void* send_hi, size_t z_begin, size_t z_end, void* stream);
 int lbm_slab_pack_async(int lattice, int precision, const void* populations, size_t x_extent,
     size_t y_extent, size_t z_extent, void* send_lo, void* send_hi, void* stream);
+/* The face exchange of slabs that share one device (every rank of a box in one
+ * process): copies src[i] to dst[i], `bytes` each, for i < count <= 64, in one
+ * launch. src and dst are host arrays of device pointers; no destination may
+ * overlap a source or another destination. */
+int lbm_copy_buffers_async(int count, const void* const* src, void* const* dst, size_t bytes,
+    void* stream);
 
 /* The coupled fluid + A + B -> C step of lbm_fluid_reaction_ab_async on a
  * z-slab (D3Q19 or D3Q27 fluid with two D3Q7 species). One face buffer per

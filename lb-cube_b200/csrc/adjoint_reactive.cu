@@ -252,8 +252,8 @@ __global__ void __launch_bounds__(kThreads)
   }
   warp_sum<2>(acc);
   if ((threadIdx.x & 31) == 0) {
-    slots[warp_slot() * kReactiveSlots + 0] += acc[0];
-    slots[warp_slot() * kReactiveSlots + 2] += acc[1];
+    slots[warp_slot(g) * kReactiveSlots + 0] += acc[0];
+    slots[warp_slot(g) * kReactiveSlots + 2] += acc[1];
   }
 }
 
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
   }
   double v[1] = {dtau};
   warp_sum<1>(v);
-  if ((threadIdx.x & 31) == 0) slots[warp_slot() * kReactiveSlots + 1] += v[0];
+  if ((threadIdx.x & 31) == 0) slots[warp_slot(g) * kReactiveSlots + 1] += v[0];
 }
 
 // Seeds lambda^N = dJ/d(f^N, A^N, B^N) and writes the block's FP64 share of J.
@@ -831,20 +831,43 @@ cudaError_t slab_adjoint_step(int collision, const typename SP::elem* fn,
   rp.k = (double)Real(k);
   rp.rho0 = 1.0f;
   rp.c0 = c0;
-  const SlabFaces<E, Real> faces{halo_lo, halo_hi, send_lo, send_hi};
-  reaction_adjoint_kernel<FL, Real, SP, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-      an, bn, u_next, la_next, lb_next, la, lb, ubar, g, rp, slots, faces);
-  if (collision == kBGK)
-    coupled_fluid_adjoint_kernel<FL, Real, kBGK, SP, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots, faces);
-  else if (collision == kTRT)
-    coupled_fluid_adjoint_kernel<FL, Real, kTRT, SP, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots, faces);
-  else if constexpr (FL::Q != 27)
-    coupled_fluid_adjoint_kernel<FL, Real, kMRT, SP, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots, faces);
-  else
+  if (collision != kBGK && collision != kTRT && (collision != kMRT || FL::Q == 27))
     return cudaErrorInvalidValue;
+  const SlabFaces<E, Real> faces{halo_lo, halo_hi, send_lo, send_hi};
+  // Planes 1 .. nz-2 pull and scatter only inside the slab: the whole-box
+  // kernels (fewer registers than the SLAB forms); planes 0 and nz-1 the SLAB
+  // forms. Every reaction launch precedes the fluid launches (they read its
+  // ubar); slots are indexed by absolute plane.
+  auto ranges = [&](auto each) {
+    if (g.nz >= 3) each(1, g.nz - 2, std::false_type{});
+    each(0, 1, std::true_type{});
+    if (g.nz >= 2) each(g.nz - 1, 1, std::true_type{});
+  };
+  ranges([&](int z0, int planes, auto slab) {
+    constexpr bool SLAB = decltype(slab)::value;
+    Grid gr = g;
+    gr.z0 = z0;
+    dim3 grid = grid_dims(gr);
+    grid.y = (unsigned)planes;
+    reaction_adjoint_kernel<FL, Real, SP, SLAB><<<grid, block_dims(gr), 0, s>>>(
+        an, bn, u_next, la_next, lb_next, la, lb, ubar, gr, rp, slots, faces);
+  });
+  ranges([&](int z0, int planes, auto slab) {
+    constexpr bool SLAB = decltype(slab)::value;
+    Grid gr = g;
+    gr.z0 = z0;
+    dim3 grid = grid_dims(gr);
+    grid.y = (unsigned)planes;
+    if (collision == kBGK)
+      coupled_fluid_adjoint_kernel<FL, Real, kBGK, SP, SLAB><<<grid, block_dims(gr), 0, s>>>(
+          fn, lf_next, ubar, lf, gr, rp.fluid, rp.rho0, slots, faces);
+    else if (collision == kTRT)
+      coupled_fluid_adjoint_kernel<FL, Real, kTRT, SP, SLAB><<<grid, block_dims(gr), 0, s>>>(
+          fn, lf_next, ubar, lf, gr, rp.fluid, rp.rho0, slots, faces);
+    else if constexpr (FL::Q != 27)
+      coupled_fluid_adjoint_kernel<FL, Real, kMRT, SP, SLAB><<<grid, block_dims(gr), 0, s>>>(
+          fn, lf_next, ubar, lf, gr, rp.fluid, rp.rho0, slots, faces);
+  });
   return cudaGetLastError();
 }
 

@@ -398,8 +398,10 @@ cudaError_t fluid_reaction_with_velocity(int collision, const Real* cur_f, Real*
 }
 
 // The slab form of fluid_reaction_with_velocity (all planes of the slab, no
-// statistics; u_out may be null): for the decomposed reactive adjoint. Buffers
-// are checked by the caller.
+// statistics; u_out may be null): for the decomposed reactive adjoint. Planes
+// 1 .. nz-2 pull and send nothing across a face, so they run the whole-box
+// kernel (fewer registers than the SLAB form); planes 0 and nz-1 run the SLAB
+// form. Buffers are checked by the caller.
 template <class FL, class Real>
 cudaError_t fluid_reaction_slab_with_velocity(int collision, const Real* cur_f, Real* nxt_f,
                                               const Real* cur_a, Real* nxt_a, const Real* cur_b,
@@ -407,26 +409,38 @@ cudaError_t fluid_reaction_slab_with_velocity(int collision, const Real* cur_f, 
                                               Real omega_c, Real k, const Real* halo_lo,
                                               const Real* halo_hi, Real* send_lo, Real* send_hi,
                                               cudaStream_t s) {
-#define LBCUBE_FRSV(CT, OM)                                                                        \
-  if (u_out != nullptr)                                                                            \
-    fluid_reaction_slab_kernel<FL, Real, CT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(   \
-        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, OM, omega_c, k, halo_lo, halo_hi,      \
-        send_lo, send_hi, nullptr, u_out);                                                         \
-  else                                                                                             \
-    fluid_reaction_slab_kernel<FL, Real, CT, false><<<grid_dims(g), block_dims(g), 0, s>>>(         \
-        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, OM, omega_c, k, halo_lo, halo_hi,      \
-        send_lo, send_hi, nullptr)
-  if (collision == kBGK) {
-    LBCUBE_FRSV(kBGK, Real(0));
-  } else if (collision == kTRT) {
-    LBCUBE_FRSV(kTRT, trt_omega_minus<Real>(omega));
-  } else if (collision == kMRT) {
-    LBCUBE_FRSV(kMRT, Real(0));
-  } else {
-    return cudaErrorInvalidValue;
-  }
-#undef LBCUBE_FRSV
-  return cudaGetLastError();
+  auto run = [&](auto ct) -> cudaError_t {
+    constexpr int CT = decltype(ct)::value;
+    const Real om = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
+    auto launch = [&](int z0, int planes, bool face) {
+      Grid gr = g;
+      gr.z0 = z0;
+      dim3 grid = grid_dims(gr);
+      grid.y = (unsigned)planes;
+      if (face && u_out != nullptr)
+        fluid_reaction_slab_kernel<FL, Real, CT, false, true><<<grid, block_dims(gr), 0, s>>>(
+            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, halo_lo, halo_hi,
+            send_lo, send_hi, nullptr, u_out);
+      else if (face)
+        fluid_reaction_slab_kernel<FL, Real, CT, false><<<grid, block_dims(gr), 0, s>>>(
+            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, halo_lo, halo_hi,
+            send_lo, send_hi, nullptr);
+      else if (u_out != nullptr)
+        fluid_reaction_kernel<FL, Real, CT, false, true><<<grid, block_dims(gr), 0, s>>>(
+            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, nullptr, u_out);
+      else
+        fluid_reaction_kernel<FL, Real, CT, false><<<grid, block_dims(gr), 0, s>>>(
+            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, nullptr);
+    };
+    if (g.nz >= 3) launch(1, g.nz - 2, false);
+    launch(0, 1, true);
+    if (g.nz >= 2) launch(g.nz - 1, 1, true);
+    return cudaGetLastError();
+  };
+  if (collision == kBGK) return run(std::integral_constant<int, kBGK>{});
+  if (collision == kTRT) return run(std::integral_constant<int, kTRT>{});
+  if (collision == kMRT) return run(std::integral_constant<int, kMRT>{});
+  return cudaErrorInvalidValue;
 }
 
 #define LBCUBE_FRSV_INST(FL, R)                                                                     \

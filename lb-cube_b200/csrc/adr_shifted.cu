@@ -189,18 +189,30 @@ cudaError_t fluid_reaction_shifted_slab(int collision, const unsigned short* cur
                                         const unsigned short* halo_lo, const unsigned short* halo_hi,
                                         unsigned short* send_lo, unsigned short* send_hi,
                                         cudaStream_t s) {
+  // planes 1 .. nz-2 neither pull nor send across a face: the whole-box
+  // kernel (fewer registers); planes 0 and nz-1: the SLAB form
   const CodeFaces faces{halo_lo, halo_hi, send_lo, send_hi};
   auto launch = [&](auto ct) -> cudaError_t {
     constexpr int CT = decltype(ct)::value;
     const float om = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
-    if (u_out != nullptr)
-      fluid_reaction_shifted_kernel<FL, FMT, CT, false, true, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, om, omega_c, k, rho0, c0, nullptr, u_out,
-          faces);
-    else
-      fluid_reaction_shifted_kernel<FL, FMT, CT, false, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, om, omega_c, k, rho0, c0, nullptr, nullptr,
-          faces);
+    auto range = [&](int z0, int planes, auto slab) {
+      constexpr bool SLAB = decltype(slab)::value;
+      Grid gr = g;
+      gr.z0 = z0;
+      dim3 grid = grid_dims(gr);
+      grid.y = (unsigned)planes;
+      if (u_out != nullptr)
+        fluid_reaction_shifted_kernel<FL, FMT, CT, false, true, SLAB><<<grid, block_dims(gr), 0, s>>>(
+            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, rho0, c0, nullptr, u_out,
+            faces);
+      else
+        fluid_reaction_shifted_kernel<FL, FMT, CT, false, false, SLAB><<<grid, block_dims(gr), 0, s>>>(
+            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, rho0, c0, nullptr, nullptr,
+            faces);
+    };
+    if (g.nz >= 3) range(1, g.nz - 2, std::false_type{});
+    range(0, 1, std::true_type{});
+    if (g.nz >= 2) range(g.nz - 1, 1, std::true_type{});
     return cudaGetLastError();
   };
   switch (collision) {

@@ -204,3 +204,63 @@ extern "C" int lbm_slab_pack_async(int lattice, int precision, const void* popul
 #undef LBCUBE_PACK
   return (int)cudaErrorInvalidValue;
 }
+
+// ---- face copies between slabs held by one process ----------------------------
+// The exchange of ranks that share one device (every rank of a box stepped in
+// one process): `count` buffers of `bytes` bytes each copied in one launch, one
+// block column per buffer, 16-byte words where both addresses allow it. The
+// pointer lists travel as a kernel parameter.
+namespace lbcube {
+
+constexpr int kMaxCopies = 64;
+
+struct CopyList {
+  const unsigned char* src[kMaxCopies];
+  unsigned char* dst[kMaxCopies];
+};
+
+static __global__ void __launch_bounds__(256)
+    copy_buffers_kernel(const CopyList list, size_t bytes) {
+  const unsigned char* __restrict__ src = list.src[blockIdx.y];
+  unsigned char* __restrict__ dst = list.dst[blockIdx.y];
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((((uintptr_t)src | (uintptr_t)dst) & 15u) == 0) {
+    const size_t words = bytes / 16;
+    for (size_t i = t; i < words; i += stride)
+      reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+    for (size_t i = words * 16 + t; i < bytes; i += stride) dst[i] = src[i];
+  } else {
+    for (size_t i = t; i < bytes; i += stride) dst[i] = src[i];
+  }
+}
+
+}  // namespace lbcube
+
+extern "C" int lbm_copy_buffers_async(int count, const void* const* src, void* const* dst,
+                                      size_t bytes, void* stream) {
+  if (src == nullptr || dst == nullptr) return (int)cudaErrorInvalidDevicePointer;
+  if (count < 0 || count > kMaxCopies) return (int)cudaErrorInvalidValue;
+  if (count == 0 || bytes == 0) return (int)cudaSuccess;
+  CopyList list{};
+  for (int i = 0; i < count; ++i) {
+    if (src[i] == nullptr || dst[i] == nullptr) return (int)cudaErrorInvalidDevicePointer;
+    list.src[i] = static_cast<const unsigned char*>(src[i]);
+    list.dst[i] = static_cast<unsigned char*>(dst[i]);
+  }
+  // no copy may write into a buffer that another copy of the list reads or writes
+  for (int i = 0; i < count; ++i)
+    for (int j = 0; j < count; ++j) {
+      const Span a[1] = {{src[j], bytes}};
+      const Span b[1] = {{dst[i], bytes}};
+      if (any_overlap(a, b)) return (int)cudaErrorInvalidValue;
+      if (j > i) {
+        const Span c[1] = {{dst[j], bytes}};
+        if (any_overlap(c, b)) return (int)cudaErrorInvalidValue;
+      }
+    }
+  const size_t words = (bytes + 15) / 16;
+  const unsigned blocks_x = (unsigned)std::min<size_t>((words + 255) / 256, 64);
+  copy_buffers_kernel<<<dim3(blocks_x, (unsigned)count), 256, 0, as_stream(stream)>>>(list, bytes);
+  return (int)cudaGetLastError();
+}

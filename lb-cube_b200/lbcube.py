@@ -154,11 +154,21 @@ def _declare(lib):
     lib.lbm_diagnostics_partials_bytes.argtypes = [C.c_int, _sz, _sz, _sz]
     lib.lbm_ke_gradient_workspace_bytes.restype = C.c_size_t
     lib.lbm_ke_gradient_workspace_bytes.argtypes = [C.c_int, C.c_int, _sz, _sz, _sz, C.c_int, C.c_int]
+    lib.lbm_copy_buffers_async.restype = C.c_int
+    lib.lbm_copy_buffers_async.argtypes = [C.c_int, C.POINTER(_vp), C.POINTER(_vp), _sz, _vp]
     for name in ("lbm_reactive_slab_slots_bytes", "lbm_reactive_slab_objective_bytes"):
         getattr(lib, name).restype = C.c_size_t
         getattr(lib, name).argtypes = [C.c_int, _sz, _sz, _sz]
     lib.lbm_stage_timeouts.restype = C.c_uint
     lib.lbm_stage_timeouts.argtypes = [C.c_int]
+
+
+def copy_buffers_async(src, dst, nbytes, stream=None) -> int:
+    """Copies device buffers src[i] -> dst[i] (nbytes each, at most 64 pairs) in one launch."""
+    n = len(src)
+    arr = (C.c_void_p * max(n, 1))
+    return load().lbm_copy_buffers_async(n, arr(*[_ptr(b) for b in src]), arr(*[_ptr(b) for b in dst]),
+                                         int(nbytes), _stream(stream))
 
 
 def _ptr(buf):
