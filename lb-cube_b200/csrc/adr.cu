@@ -99,7 +99,11 @@ __device__ __forceinline__ void fluid_reaction_body(const Real* __restrict__ cur
       sums[4] = ca * cb;
     }
   }
-  if constexpr (STATS) block_sum_to<kStatSums>(sums, partials + block_linear() * kStatSums);
+  // partials by absolute plane: a launch over planes [g.z0, g.z0 + gridDim.y)
+  // writes the partials of those planes' blocks
+  if constexpr (STATS)
+    block_sum_to<kStatSums>(sums, partials + (((long long)g.z0 + blockIdx.y) * gridDim.x + blockIdx.x) *
+                                                 kStatSums);
 }
 
 template <class FL, class Real, int CT, bool STATS, bool UOUT = false>
@@ -259,17 +263,33 @@ cudaError_t launch_fluid_reaction_slab(const Real* cur_f, Real* nxt_f, const Rea
                           {partials, partials != nullptr ? need : 0}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
-  g.z0 = (int)z_begin;
-  dim3 grid = grid_dims(g);
-  grid.y = (unsigned)(z_end - z_begin);
-  if (partials != nullptr)
-    fluid_reaction_slab_kernel<FL, Real, CT, true><<<grid, block_dims(g), 0, stream>>>(
-        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, halo_lo,
-        halo_hi, send_lo, send_hi, partials);
-  else
-    fluid_reaction_slab_kernel<FL, Real, CT, false><<<grid, block_dims(g), 0, stream>>>(
-        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, halo_lo,
-        halo_hi, send_lo, send_hi, nullptr);
+  // planes 0 and nz-1 of the range: the SLAB form; planes in between pull and
+  // send nothing across a face: the whole-box kernel (fewer registers)
+  auto launch = [&](int z0, int z1, bool face) {
+    if (z0 >= z1) return;
+    Grid gr = g;
+    gr.z0 = z0;
+    dim3 grid = grid_dims(gr);
+    grid.y = (unsigned)(z1 - z0);
+    if (face && partials != nullptr)
+      fluid_reaction_slab_kernel<FL, Real, CT, true><<<grid, block_dims(gr), 0, stream>>>(
+          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, halo_lo,
+          halo_hi, send_lo, send_hi, partials);
+    else if (face)
+      fluid_reaction_slab_kernel<FL, Real, CT, false><<<grid, block_dims(gr), 0, stream>>>(
+          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, halo_lo,
+          halo_hi, send_lo, send_hi, nullptr);
+    else if (partials != nullptr)
+      fluid_reaction_kernel<FL, Real, CT, true><<<grid, block_dims(gr), 0, stream>>>(
+          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, partials);
+    else
+      fluid_reaction_kernel<FL, Real, CT, false><<<grid, block_dims(gr), 0, stream>>>(
+          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, nullptr);
+  };
+  const int zb = (int)z_begin, ze = (int)z_end, last = g.nz - 1;
+  if (zb == 0) launch(0, 1, true);
+  launch(std::max(zb, 1), std::min(ze, last), false);
+  if (ze - 1 == last && last > 0 && zb <= last) launch(last, last + 1, true);
   return cudaGetLastError();
 }
 
