@@ -192,3 +192,23 @@ def test_reactive_gradient_validation(lib):
     assert E.load().lbm_reactive_gradient_async(1, 0, 9, 0.5, 1, 0, A0, A1, A2, A3, 16, 12, 10, 0.8, 0.7, 0.1,
                                                 20, 4, A4, nb, A4 + 8, A4 + 16, None, None, None) == \
         E.cudaErrorInvalidValue
+
+
+def test_copy_buffers_validation(lib):
+    """lbm_copy_buffers_async (face copies of slabs sharing a device) rejects
+    bad lists before it touches the device: more than 64 pairs, a null
+    pointer, a destination overlapping a source or another destination."""
+    arr = C.c_void_p * 65
+    src, dst = arr(*[A0 + i * 4096 for i in range(65)]), arr(*[A4 + i * 4096 for i in range(65)])
+    assert lib.lbm_copy_buffers_async(65, src, dst, 1024, None) == E.cudaErrorInvalidValue
+    assert lib.lbm_copy_buffers_async(-1, src, dst, 1024, None) == E.cudaErrorInvalidValue
+    assert lib.lbm_copy_buffers_async(2, None, dst, 1024, None) == E.cudaErrorInvalidDevicePointer
+    two = C.c_void_p * 2
+    assert lib.lbm_copy_buffers_async(2, two(A0, None), two(A4, A4 + 4096), 1024, None) == \
+        E.cudaErrorInvalidDevicePointer
+    # a destination inside a source, and two destinations that overlap
+    assert lib.lbm_copy_buffers_async(2, two(A0, A0 + 4096), two(A0 + 512, A4), 1024, None) == \
+        E.cudaErrorInvalidValue
+    assert lib.lbm_copy_buffers_async(2, two(A0, A0 + 4096), two(A4, A4 + 512), 1024, None) == \
+        E.cudaErrorInvalidValue
+    assert lib.lbm_copy_buffers_async(0, two(A0, A0), two(A4, A4), 1024, None) == 0  # nothing to copy
