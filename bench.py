@@ -801,12 +801,19 @@ def run_engine(args, rank, world, local_rank):
     bytes_per_lu = BYTES_PER_LU if storage == "fp32" else BYTES_PER_LU // 2
     slabs = None
     launches_per_step = 1
-    if storage == "fp32" and world > 1:
+    if storage != "fp32":  # 16-bit codes of the initial state
+        h = torch.empty(f.shape, dtype=torch.int16, device=dev)
+        E.check(E.encode_shifted_async("D3Q19", storage, "float", f, h, NX, NY, NZ, 1.0))
+        torch.cuda.synchronize()
+        f = h
+    if world > 1:
         # one periodic NX x NY x (NZ * world) box cut into z-slabs, one per rank;
-        # the face populations cross NVLink (NCCL point-to-point) every step
+        # the face populations (or their 16-bit codes) cross NVLink (NCCL
+        # point-to-point) every step
         import slab
 
-        slabs = slab.SlabDomain(torch, "D3Q19", "float", OP, NX, NY, NZ * world, omega, rank, world, dev)
+        slabs = slab.SlabDomain(torch, "D3Q19", "float", OP, NX, NY, NZ * world, omega, rank, world, dev,
+                                storage=None if storage == "fp32" else storage)
         exchange = slab.DistributedExchange(dist)
         slabs.prime(f, exchange)
         launches_per_step = len(sum(slabs.ranges(), []))
@@ -818,11 +825,6 @@ def run_engine(args, rank, world, local_rank):
         def step(cur, nxt):
             return E.launch_step_gpu("D3Q19", "float", OP, cur, nxt, NX, NY, NZ, omega)
     else:
-        h = torch.empty(f.shape, dtype=torch.int16, device=dev)
-        E.check(E.encode_shifted_async("D3Q19", storage, "float", f, h, NX, NY, NZ, 1.0))
-        torch.cuda.synchronize()
-        f = h
-
         def step(cur, nxt):
             return E.step_shifted_async("D3Q19", storage, OP, cur, nxt, NX, NY, NZ, omega, 1.0)
     g = torch.empty_like(f)
@@ -893,23 +895,23 @@ def run_engine(args, rank, world, local_rank):
                "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
                "note": "pinned host field copied in, K steps via lbm_launch_step_gpu_d3q19_float_trt, "
                        "field copied back; copies amortised over K"}
-        if storage != "fp32":
+        if slabs is not None:
+            e2e["note"] = e2e["note"].replace(
+                "lbm_launch_step_gpu_d3q19_float_trt",
+                ("lbm_step_slab_async" if storage == "fp32" else "lbm_step_slab_shifted_async") +
+                " + NCCL face exchange")
+        elif storage != "fp32":
             e2e["note"] = e2e["note"].replace("lbm_launch_step_gpu_d3q19_float_trt", "lbm_step_shifted_async")
-        elif slabs is not None:
-            e2e["note"] = e2e["note"].replace("lbm_launch_step_gpu_d3q19_float_trt",
-                                              "lbm_step_slab_async + NCCL face exchange")
         del host
 
     if rank != 0:
         return None
     if world == 1:
         parallelism = "single GPU"
-    elif slabs is not None:
+    else:
         parallelism = (f"z-slab decomposition of one {NX}x{NY}x{NZ * world} periodic box over {world} GPUs "
                        f"({NZ} planes each), NCCL point-to-point face exchange every step, overlapped with "
                        f"the interior planes")
-    else:
-        parallelism = f"{world} independent replicas (16-bit storage has no slab path)"
     peak, peak_kind = measured_hbm_peak()
     traffic = committed_traffic(f"d3q19_float_trt_{NX}") if storage == "fp32" and OP == "TRT" else None
     variants = accuracy = fp16_store = adjoint = adjoint_reactive = adjoint_reactive_16 = mixing = None

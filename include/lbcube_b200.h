@@ -520,6 +520,17 @@ int lbm_step_slab_async(int lattice, int precision, int collision,
     void* send_hi, size_t z_begin, size_t z_end, void* stream);
 int lbm_slab_pack_async(int lattice, int precision, const void* populations, size_t x_extent,
     size_t y_extent, size_t z_extent, void* send_lo, void* send_hi, void* stream);
+/* The z-slab step on shifted 16-bit storage (lbm_step_shifted_async's formats
+ * and operators, D3Q19 or D3Q27): face buffers of lbm_slab_face_elems 16-bit
+ * codes, otherwise as lbm_step_slab_async. A box stepped as slabs gives the
+ * codes of the box stepped whole. lbm_slab_pack_shifted_async fills the send
+ * buffers from a 16-bit state. */
+int lbm_step_slab_shifted_async(int lattice, int format, int collision,
+    const void* current_populations, void* next_populations, size_t x_extent, size_t y_extent,
+    size_t z_extent, float omega, float rho0, const void* halo_lo, const void* halo_hi,
+    void* send_lo, void* send_hi, size_t z_begin, size_t z_end, void* stream);
+int lbm_slab_pack_shifted_async(int lattice, const void* populations, size_t x_extent,
+    size_t y_extent, size_t z_extent, void* send_lo, void* send_hi, void* stream);
 /* The face exchange of slabs that share one device (every rank of a box in one
  * process): copies src[i] to dst[i], `bytes` each, for i < count <= 64, in one
  * launch. src and dst are host arrays of device pointers; no destination may

@@ -95,6 +95,103 @@ cudaError_t shifted_by_lattice(int lattice, int collision, const void* cur, void
   }
 }
 
+// ---- z-slab form -----------------------------------------------------------------
+// One step of planes [z_begin, z_end) of a z-slab of a box on 16-bit storage:
+// populations crossing a face are pulled from halo buffers of codes and the
+// leaving codes stored into send buffers (layout of lbm_slab_face_elems). Where
+// the row-staged kernel applies it steps every plane of the range, its bulk
+// copies reading the halo rows at the faces, so a box stepped as slabs gives
+// the bits of the box stepped whole; otherwise the vectorised kernel steps the
+// interior planes and its SLAB form the face planes.
+template <class L, int FMT, int CT>
+cudaError_t launch_shifted_slab_step(const void* cur_v, void* nxt_v, size_t nx, size_t ny,
+                                     size_t nz, float omega, float rho0, const void* hl_v,
+                                     const void* hh_v, void* sl_v, void* sh_v, size_t z_begin,
+                                     size_t z_end, cudaStream_t stream) {
+  using S = ShiftedPolicy<L, FMT, CT>;
+  using E = unsigned short;
+  const E* cur = static_cast<const E*>(cur_v);
+  E* nxt = static_cast<E*>(nxt_v);
+  const E *hl = static_cast<const E*>(hl_v), *hh = static_cast<const E*>(hh_v);
+  E *sl = static_cast<E*>(sl_v), *sh = static_cast<E*>(sh_v);
+  Grid g;
+  cudaError_t err = validate_domain(cur == nullptr || nxt == nullptr, 1, 1, 1, 3, nx, ny, nz, g);
+  if (err != cudaSuccess) return err;
+  if (L::D != 3 || z_begin >= z_end || z_end > nz) return cudaErrorInvalidValue;
+  const bool lo_face = z_begin == 0, hi_face = z_end == nz;
+  if ((lo_face && (hl == nullptr || sl == nullptr)) || (hi_face && (hh == nullptr || sh == nullptr)))
+    return cudaErrorInvalidDevicePointer;
+  if (nz == 1 && (hl == nullptr || hh == nullptr || sl == nullptr || sh == nullptr))
+    return cudaErrorInvalidDevicePointer;
+  const size_t bytes = (size_t)L::Q * g.plane * sizeof(E);
+  const size_t hbytes = (size_t)zcount<L>() * g.ny * g.nx * sizeof(E);
+  const Span reads[3] = {{cur, bytes}, {hl, hl ? hbytes : 0}, {hh, hh ? hbytes : 0}};
+  const Span writes[3] = {{nxt, bytes}, {sl, sl ? hbytes : 0}, {sh, sh ? hbytes : 0}};
+  if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
+  // the public contract of the 16-bit step (x_extent a multiple of 4, 8-byte
+  // aligned buffers), face buffers included
+  if (g.nx % 4 != 0 || !vec_eligible<S>(g, cur, nxt)) return cudaErrorInvalidValue;
+  for (const void* q : {hl_v, hh_v, (const void*)sl, (const void*)sh})
+    if ((uintptr_t)q % 8 != 0) return cudaErrorInvalidValue;
+  const float omega_minus = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
+  const typename S::Params p{rho0};
+  const SlabArgs<E> faces{hl, hh, sl, sh, 0};
+  if constexpr (kShiftedStaged && S::kBudgeted && S::V == 4 && L::Q <= 19) {
+    bool faces16 = true;
+    for (const void* q : {hl_v, hh_v, (const void*)sl, (const void*)sh})
+      faces16 = faces16 && (uintptr_t)q % 16 == 0;
+    if (faces16 && staged_eligible<L>(g, cur, nxt))
+      return launch_staged_step<L, S, CT, true>(g, stream, cur, nxt, omega, omega_minus, p,
+                                                (int)z_begin, (int)z_end, faces);
+  }
+  VecGrid vg = make_vec_grid(g, S::V);
+  const size_t ib = std::max<size_t>(z_begin, 1), ie = std::min<size_t>(z_end, nz - 1);
+  if (ib < ie) {
+    vg.z0 = (int)ib;
+    dim3 grid = vec_grid_dims(vg);
+    grid.y = (unsigned)(ie - ib);
+    launch_vec_step<L, S, CT>(vg, grid, vec_block_threads(vg), stream, cur, nxt, omega, omega_minus, p);
+    vg.z0 = 0;
+  }
+  auto face = [&](size_t z) {
+    dim3 grid = vec_grid_dims(vg);
+    grid.y = 1;
+    SlabArgs<E> f = faces;
+    f.z_begin = (int)z;
+    fluid_step_vec_kernel<L, S, CT, false, true><<<grid, vec_block_threads(vg), 0, stream>>>(
+        cur, nxt, vg, omega, omega_minus, p, nullptr, f);
+  };
+  if (lo_face) face(0);
+  if (hi_face && nz > 1) face(nz - 1);
+  return cudaGetLastError();
+}
+
+template <class L, int FMT>
+cudaError_t shifted_slab_by_collision(int collision, const void* cur, void* nxt, size_t nx,
+                                      size_t ny, size_t nz, float omega, float rho0, const void* hl,
+                                      const void* hh, void* sl, void* sh, size_t z0, size_t z1,
+                                      cudaStream_t s) {
+  switch (collision) {
+    case kBGK: return launch_shifted_slab_step<L, FMT, kBGK>(cur, nxt, nx, ny, nz, omega, rho0, hl, hh, sl, sh, z0, z1, s);
+    case kTRT: return launch_shifted_slab_step<L, FMT, kTRT>(cur, nxt, nx, ny, nz, omega, rho0, hl, hh, sl, sh, z0, z1, s);
+    case kMRT: return launch_shifted_slab_step<L, FMT, kMRT>(cur, nxt, nx, ny, nz, omega, rho0, hl, hh, sl, sh, z0, z1, s);
+    case kRLBM: return launch_shifted_slab_step<L, FMT, kRLBM>(cur, nxt, nx, ny, nz, omega, rho0, hl, hh, sl, sh, z0, z1, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int FMT>
+cudaError_t shifted_slab_by_lattice(int lattice, int collision, const void* cur, void* nxt,
+                                    size_t nx, size_t ny, size_t nz, float omega, float rho0,
+                                    const void* hl, const void* hh, void* sl, void* sh, size_t z0,
+                                    size_t z1, cudaStream_t s) {
+  switch (lattice) {
+    case kD3Q19: return shifted_slab_by_collision<D3Q19, FMT>(collision, cur, nxt, nx, ny, nz, omega, rho0, hl, hh, sl, sh, z0, z1, s);
+    case kD3Q27: return shifted_slab_by_collision<D3Q27, FMT>(collision, cur, nxt, nx, ny, nz, omega, rho0, hl, hh, sl, sh, z0, z1, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // ---- conversions --------------------------------------------------------------
 // grid.y = population i (its weight w_i is a compile-time constant of the
 // block's branch), grid-stride over the cells of that plane.
@@ -225,6 +322,25 @@ extern "C" int lbm_step_shifted_async(int lattice, int format, int collision,
     return (int)shifted_by_lattice<kQ15S>(lattice, collision, current_populations,
                                           next_populations, x_extent, y_extent, z_extent, omega,
                                           rho0, s);
+  return (int)cudaErrorInvalidValue;
+}
+
+extern "C" int lbm_step_slab_shifted_async(int lattice, int format, int collision,
+                                           const void* current_populations, void* next_populations,
+                                           size_t x_extent, size_t y_extent, size_t z_extent,
+                                           float omega, float rho0, const void* halo_lo,
+                                           const void* halo_hi, void* send_lo, void* send_hi,
+                                           size_t z_begin, size_t z_end, void* stream) {
+  const cudaStream_t s = as_stream(stream);
+#define LBCUBE_SLAB16(F)                                                                           \
+  return (int)shifted_slab_by_lattice<F>(lattice, collision, current_populations, next_populations, \
+                                         x_extent, y_extent, z_extent, omega, rho0, halo_lo,       \
+                                         halo_hi, send_lo, send_hi, z_begin, z_end, s)
+  if (format == LBM_F16S) LBCUBE_SLAB16(kF16S);
+  if (format == LBM_BF16S) LBCUBE_SLAB16(kBF16S);
+  if (format == LBM_E3M12S) LBCUBE_SLAB16(kE3M12S);
+  if (format == LBM_Q15S) LBCUBE_SLAB16(kQ15S);
+#undef LBCUBE_SLAB16
   return (int)cudaErrorInvalidValue;
 }
 

@@ -205,6 +205,21 @@ extern "C" int lbm_slab_pack_async(int lattice, int precision, const void* popul
   return (int)cudaErrorInvalidValue;
 }
 
+// The pack of a slab state on 16-bit storage (codes of any format).
+extern "C" int lbm_slab_pack_shifted_async(int lattice, const void* populations, size_t x_extent,
+                                           size_t y_extent, size_t z_extent, void* send_lo,
+                                           void* send_hi, void* stream) {
+  using E = unsigned short;
+  const E* f = static_cast<const E*>(populations);
+  if (lattice == LBM_D3Q19)
+    return (int)launch_slab_pack<D3Q19, E>(f, x_extent, y_extent, z_extent, static_cast<E*>(send_lo),
+                                           static_cast<E*>(send_hi), as_stream(stream));
+  if (lattice == LBM_D3Q27)
+    return (int)launch_slab_pack<D3Q27, E>(f, x_extent, y_extent, z_extent, static_cast<E*>(send_lo),
+                                           static_cast<E*>(send_hi), as_stream(stream));
+  return (int)cudaErrorInvalidValue;
+}
+
 // ---- face copies between slabs held by one process ----------------------------
 // The exchange of ranks that share one device (every rank of a box stepped in
 // one process): `count` buffers of `bytes` bytes each copied in one launch, one

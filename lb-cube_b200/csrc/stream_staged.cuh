@@ -94,14 +94,19 @@ __device__ __forceinline__ void bulk_copy_g2s(unsigned int dst, const void* src,
 struct StagedGrid {
   int nx, ny, nz;
   long long plane;
-  int rows;       // ny * nz
+  int rows;       // end of the launch's rows (exclusive); ny * nz for every row
   int row_bytes;  // nx * 2
+  int row0;       // first row of the launch
 };
 
-// Issues the Q source rows of output row `r` into stage buffer `buf`.
-template <class L>
+// Issues the Q source rows of output row `r` into stage buffer `buf`. SLAB: a
+// z-slab of a box (slab_faces.cuh layout of the halo buffers): at plane 0 the
+// c_z = +1 rows come from halo_lo, at plane nz - 1 the c_z = -1 rows from
+// halo_hi, instead of the periodic wrap.
+template <class L, bool SLAB = false>
 __device__ __forceinline__ void issue_row(const unsigned short* __restrict__ cur, const StagedGrid& g,
-                                          int r, unsigned int buf, unsigned int bar) {
+                                          int r, unsigned int buf, unsigned int bar,
+                                          const SlabArgs<unsigned short>& slab = {}) {
   const int z = r / g.ny, y = r - z * g.ny;
   const int ym = y == 0 ? g.ny - 1 : y - 1, yp = y == g.ny - 1 ? 0 : y + 1;
   const int zm = z == 0 ? g.nz - 1 : z - 1, zp = z == g.nz - 1 ? 0 : z + 1;
@@ -112,15 +117,21 @@ __device__ __forceinline__ void issue_row(const unsigned short* __restrict__ cur
     const int sy = cy == 0 ? y : (cy > 0 ? ym : yp);
     const int sz = cz == 0 ? z : (cz > 0 ? zm : zp);
     const unsigned short* src = cur + g.plane * i + ((long long)sz * g.ny + sy) * g.nx;
+    if constexpr (SLAB && cz > 0) {
+      if (z == 0) src = slab.halo_lo + ((long long)zslot<L>(i) * g.ny + sy) * g.nx;
+    } else if constexpr (SLAB && cz < 0) {
+      if (z == g.nz - 1) src = slab.halo_hi + ((long long)zslot<L>(i) * g.ny + sy) * g.nx;
+    }
     bulk_copy_g2s(buf + (unsigned int)(i * g.row_bytes), src, (unsigned int)g.row_bytes, bar);
   });
 }
 
-template <class L, class S, int CT>
+template <class L, class S, int CT, bool SLAB = false>
 __global__ void __launch_bounds__(kMaxRowThreads, LBCUBE_STAGED_MIN_BLOCKS)
     fluid_step_staged_kernel(const unsigned short* __restrict__ cur,
                              unsigned short* __restrict__ nxt, StagedGrid g, float omega,
-                             float omega_minus, typename S::Params p) {
+                             float omega_minus, typename S::Params p,
+                             SlabArgs<unsigned short> slab = {}) {
   static_assert(S::V == 4, "four cells per thread");
   // kStages row buffers, then the kStages mbarriers (8-byte aligned: a stage
   // is a multiple of 16 bytes)
@@ -133,7 +144,7 @@ __global__ void __launch_bounds__(kMaxRowThreads, LBCUBE_STAGED_MIN_BLOCKS)
     if (t == 0) atomicAdd(&g_stage_timeouts, 1u);
     return;
   }
-  const int r0 = blockIdx.x * kStagedRows;
+  const int r0 = g.row0 + blockIdx.x * kStagedRows;
   const int nrows = min(kStagedRows, g.rows - r0);
   const int x0 = 4 * t;
   const bool active = x0 < g.nx;
@@ -147,7 +158,7 @@ __global__ void __launch_bounds__(kMaxRowThreads, LBCUBE_STAGED_MIN_BLOCKS)
   int issued = 0;  // rows whose copies have been issued (thread 0's count)
   if (t == 0)
     for (; issued < kStages && issued < nrows; ++issued)
-      issue_row<L>(cur, g, r0 + issued, base + issued * stage_bytes, bars + 8 * issued);
+      issue_row<L, SLAB>(cur, g, r0 + issued, base + issued * stage_bytes, bars + 8 * issued, slab);
   bool failed = false;
   for (int k = 0; k < nrows; ++k) {
     const int s = k % kStages;
@@ -180,7 +191,7 @@ __global__ void __launch_bounds__(kMaxRowThreads, LBCUBE_STAGED_MIN_BLOCKS)
       break;
     }
     if (t == 0 && issued < nrows) {
-      issue_row<L>(cur, g, r0 + issued, base + s * stage_bytes, bars + 8 * s);
+      issue_row<L, SLAB>(cur, g, r0 + issued, base + s * stage_bytes, bars + 8 * s, slab);
       ++issued;
     }
     if (active) {
@@ -201,6 +212,19 @@ __global__ void __launch_bounds__(kMaxRowThreads, LBCUBE_STAGED_MIN_BLOCKS)
         constexpr int i = LB_I(I);
         *reinterpret_cast<uint2*>(nxt + g.plane * i + cell) = make_uint2(raw[i][0], raw[i][1]);
       });
+      if constexpr (SLAB) {  // the populations leaving through a face, at the cells' own (x, y)
+        const int z = (r0 + k) / g.ny, y = (r0 + k) - z * g.ny;
+        static_for<L::Q>([&](auto I) {
+          constexpr int i = LB_I(I);
+          constexpr int cz = L::c[i][2];
+          const long long at = ((long long)zslot<L>(i) * g.ny + y) * g.nx + x0;
+          if constexpr (cz > 0) {
+            if (z == g.nz - 1) *reinterpret_cast<uint2*>(slab.send_hi + at) = make_uint2(raw[i][0], raw[i][1]);
+          } else if constexpr (cz < 0) {
+            if (z == 0) *reinterpret_cast<uint2*>(slab.send_lo + at) = make_uint2(raw[i][0], raw[i][1]);
+          }
+        });
+      }
     }
   }
   if (failed && t == 0) {
@@ -224,26 +248,32 @@ inline bool staged_eligible(const Grid& g, const void* a, const void* b) {
          (uintptr_t)a % 16 == 0 && (uintptr_t)b % 16 == 0;
 }
 
-template <class L, class S, int CT>
+// Planes [z_begin, z_end) (every plane by default); SLAB: the planes of a
+// z-slab, with its halo and send buffers in `slab`.
+template <class L, class S, int CT, bool SLAB = false>
 inline cudaError_t launch_staged_step(const Grid& g, cudaStream_t stream, const unsigned short* cur,
                                       unsigned short* nxt, float omega, float omega_minus,
-                                      const typename S::Params& p) {
+                                      const typename S::Params& p, int z_begin = 0, int z_end = -1,
+                                      const SlabArgs<unsigned short>& slab = {}) {
   StagedGrid sg;
   sg.nx = g.nx;
   sg.ny = g.ny;
   sg.nz = g.nz;
   sg.plane = g.plane;
-  sg.rows = g.ny * g.nz;
+  sg.row0 = z_begin * g.ny;
+  sg.rows = (z_end < 0 ? g.nz : z_end) * g.ny;
   sg.row_bytes = g.nx * 2;
+  if (sg.rows <= sg.row0) return cudaSuccess;
   const size_t smem = (size_t)kStages * L::Q * sg.row_bytes + kStages * 8;
-  auto kernel = fluid_step_staged_kernel<L, S, CT>;
+  auto kernel = fluid_step_staged_kernel<L, S, CT, SLAB>;
   if (smem > 48 * 1024) {
     const cudaError_t err =
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
   }
-  const unsigned blocks = (unsigned)((sg.rows + kStagedRows - 1) / kStagedRows);
-  kernel<<<blocks, (unsigned)staged_threads(g.nx), smem, stream>>>(cur, nxt, sg, omega, omega_minus, p);
+  const unsigned blocks = (unsigned)((sg.rows - sg.row0 + kStagedRows - 1) / kStagedRows);
+  kernel<<<blocks, (unsigned)staged_threads(g.nx), smem, stream>>>(cur, nxt, sg, omega, omega_minus, p,
+                                                                    slab);
   return cudaGetLastError();
 }
 

@@ -109,6 +109,9 @@ def _declare(lib):
         "lbm_step_slab_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, d, _vp, _vp, _vp, _vp, _sz,
                                 _sz, _vp],
         "lbm_slab_pack_async": [C.c_int, C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
+        "lbm_step_slab_shifted_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _sz, _sz, _sz, C.c_float,
+                                        C.c_float, _vp, _vp, _vp, _vp, _sz, _sz, _vp],
+        "lbm_slab_pack_shifted_async": [C.c_int, _vp, _sz, _sz, _sz, _vp, _vp, _vp],
         "lbm_fluid_reaction_slab_async": [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz,
                                           _sz, d, d, d, _vp, _vp, _vp, _vp, _sz, _sz, _vp, _sz, _vp],
         "lbm_fluid_reaction_slab_pack_async": [C.c_int, C.c_int, _vp, _vp, _vp, _sz, _sz, _sz, _vp, _vp, _vp],

@@ -42,9 +42,12 @@ def face_elems(lattice: str, nx: int, ny: int) -> int:
 
 
 class SlabDomain:
-    """One rank's slab: extents, face buffers and the step launches."""
+    """One rank's slab: extents, face buffers and the step launches. storage:
+    None for populations in `real`, or a 16-bit format of lbcube.FORMATS
+    (codes shifted by rho0; face buffers of codes)."""
 
-    def __init__(self, torch, lattice, real, collision, nx, ny, nz_global, omega, rank, world, device):
+    def __init__(self, torch, lattice, real, collision, nx, ny, nz_global, omega, rank, world, device,
+                 storage=None, rho0=1.0):
         if lattice not in Q_OF:
             raise ValueError("slab decomposition needs a 3-D fluid lattice (D3Q19, D3Q27)")
         if nz_global % world != 0:
@@ -55,7 +58,8 @@ class SlabDomain:
         self.z0 = rank * self.nz
         self.rank, self.world = rank, world
         self.omega = float(omega)
-        dtype = torch.float32 if real == "float" else torch.float64
+        self.storage, self.rho0 = storage, float(rho0)
+        dtype = (torch.float32 if real == "float" else torch.float64) if storage is None else torch.int16
         n = face_elems(lattice, nx, ny)
         self.halo_lo, self.halo_hi, self.send_lo, self.send_hi = (
             torch.empty(n, dtype=dtype, device=device) for _ in range(4))
@@ -66,16 +70,31 @@ class SlabDomain:
 
     def pack(self, f, stream=None):
         """Face populations of state ``f`` into the send buffers."""
-        E.check(E.load().lbm_slab_pack_async(E.LATTICES[self.lattice], E.REALS[self.real], f.data_ptr(),
-                                             self.nx, self.ny, self.nz, self.send_lo.data_ptr(),
-                                             self.send_hi.data_ptr(), E._stream(stream)), "slab pack")
+        lib = E.load()
+        if self.storage is not None:
+            rc = lib.lbm_slab_pack_shifted_async(E.LATTICES[self.lattice], f.data_ptr(), self.nx, self.ny, self.nz,
+                                                 self.send_lo.data_ptr(), self.send_hi.data_ptr(), E._stream(stream))
+        else:
+            rc = lib.lbm_slab_pack_async(E.LATTICES[self.lattice], E.REALS[self.real], f.data_ptr(), self.nx,
+                                         self.ny, self.nz, self.send_lo.data_ptr(), self.send_hi.data_ptr(),
+                                         E._stream(stream))
+        E.check(rc, "slab pack")
 
     def launch(self, cur, nxt, z_begin, z_end, stream=None):
-        E.check(E.load().lbm_step_slab_async(
-            E.LATTICES[self.lattice], E.REALS[self.real], E.COLLISIONS[self.collision], cur.data_ptr(),
-            nxt.data_ptr(), self.nx, self.ny, self.nz, self.omega, self.halo_lo.data_ptr(),
-            self.halo_hi.data_ptr(), self.send_lo.data_ptr(), self.send_hi.data_ptr(), z_begin, z_end,
-            E._stream(stream)), "slab step")
+        lib = E.load()
+        if self.storage is not None:
+            rc = lib.lbm_step_slab_shifted_async(
+                E.LATTICES[self.lattice], E.FORMATS[self.storage], E.COLLISIONS[self.collision], cur.data_ptr(),
+                nxt.data_ptr(), self.nx, self.ny, self.nz, self.omega, self.rho0, self.halo_lo.data_ptr(),
+                self.halo_hi.data_ptr(), self.send_lo.data_ptr(), self.send_hi.data_ptr(), z_begin, z_end,
+                E._stream(stream))
+        else:
+            rc = lib.lbm_step_slab_async(
+                E.LATTICES[self.lattice], E.REALS[self.real], E.COLLISIONS[self.collision], cur.data_ptr(),
+                nxt.data_ptr(), self.nx, self.ny, self.nz, self.omega, self.halo_lo.data_ptr(),
+                self.halo_hi.data_ptr(), self.send_lo.data_ptr(), self.send_hi.data_ptr(), z_begin, z_end,
+                E._stream(stream))
+        E.check(rc, "slab step")
 
     def ranges(self):
         """(interior, faces): plane ranges that need no halo, and those that do."""
@@ -546,10 +565,13 @@ class DistributedExchange:
             return
         dist = self.dist
         up, down = (d.rank + 1) % d.world, (d.rank - 1) % d.world
-        ops = [dist.P2POp(dist.isend, d.send_hi, up, self.group),
-               dist.P2POp(dist.isend, d.send_lo, down, self.group),
-               dist.P2POp(dist.irecv, d.halo_lo, down, self.group),
-               dist.P2POp(dist.irecv, d.halo_hi, up, self.group)]
+        # 16-bit codes travel as float16 (the same bytes; NCCL has no int16 and
+        # point-to-point transfers do no arithmetic)
+        wire = (lambda t: t.view(d.torch.float16)) if d.send_lo.dtype == d.torch.int16 else (lambda t: t)
+        ops = [dist.P2POp(dist.isend, wire(d.send_hi), up, self.group),
+               dist.P2POp(dist.isend, wire(d.send_lo), down, self.group),
+               dist.P2POp(dist.irecv, wire(d.halo_lo), down, self.group),
+               dist.P2POp(dist.irecv, wire(d.halo_hi), up, self.group)]
         for req in dist.batch_isend_irecv(ops):
             req.wait()
 

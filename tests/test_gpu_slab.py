@@ -186,3 +186,49 @@ def test_coupled_slabs_match_whole_box(engine, dev, lat, dn, op, dims, world):
         assert U.same_bits(g, w)
     else:
         assert np.all(np.abs(g - w) <= 1e-12 * np.maximum(np.abs(w), 1e-300)), (g, w)
+
+
+CASES16 = [("D3Q19", "f16s", "TRT", (32, 6, 8)), ("D3Q19", "q15s", "MRT", (16, 4, 8)),
+           ("D3Q19", "bf16s", "BGK", (12, 4, 4)), ("D3Q27", "e3m12s", "TRT", (16, 4, 4)),
+           ("D3Q19", "f16s", "RLBM", (16, 4, 4))]
+
+
+@pytest.mark.parametrize("lat,fmt,op,dims", CASES16)
+@pytest.mark.parametrize("world", [1, 2, 4])
+def test_16bit_slabs_match_whole_box(engine, dev, lat, fmt, op, dims, world):
+    """16-bit storage (lbm_step_slab_shifted_async, face buffers of codes):
+    the slabs give the codes of the whole box stepped with
+    lbm_step_shifted_async, bit for bit. Rows of a multiple of 8 cells run the
+    row-staged kernel on every plane (its copies read the halo rows at the
+    faces); 12-cell rows and the operators that decode to populations run the
+    vectorised kernel and its SLAB form."""
+    nx, ny, nz = dims
+    steps = 6
+    f = torch.from_numpy(U.random_state(lat, nx, ny, nz, np.float32, seed=23)).to(dev)
+    Q = f.shape[0]
+    h = torch.empty(f.shape, dtype=torch.int16, device=dev)
+    E.check(E.encode_shifted_async(lat, fmt, "float", f, h, nx, ny, nz, 1.0))
+    a, b = h.clone(), torch.empty_like(h)
+    for _ in range(steps):
+        E.check(E.step_shifted_async(lat, fmt, op, a, b, nx, ny, nz, 1 / 0.6, 1.0))
+        a, b = b, a
+    torch.cuda.synchronize()
+    want = a.cpu().numpy().reshape(Q, -1)
+    h4 = h.view(Q, nz, ny, nx)
+    doms = [slab.SlabDomain(torch, lat, "float", op, nx, ny, nz, 1 / 0.6, r, world, dev, storage=fmt)
+            for r in range(world)]
+    cur = [h4[:, d.z0:d.z0 + d.nz].contiguous() for d in doms]
+    nxt = [torch.empty_like(c) for c in cur]
+    ex = slab.LocalExchange(doms)
+    for d, c in zip(doms, cur):
+        d.pack(c)
+    ex.exchange_all()
+    for _ in range(steps):
+        for d, c, n in zip(doms, cur, nxt):
+            d.compute(c, n)
+        ex.exchange_all()
+        cur, nxt = nxt, cur
+    assert E.stage_timeouts(reset=True) == 0
+    torch.cuda.synchronize()
+    got = np.concatenate([c.cpu().numpy() for c in cur], axis=1).reshape(Q, -1)
+    assert np.array_equal(got, want)

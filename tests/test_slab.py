@@ -67,6 +67,16 @@ def _worker(rank, world, port, q):
         lower, upper = (rank - 1) % world, (rank + 1) % world
         ok1 = (torch.equal(d.halo_lo, torch.arange(n, dtype=torch.float64) + 1000 * lower + 500) and
                torch.equal(d.halo_hi, torch.arange(n, dtype=torch.float64) + 1000 * upper + 1))
+        # 16-bit codes (face buffers of a slab on shifted storage), bit patterns
+        # that are NaN or subnormal as float16 included
+        saved = (d.halo_lo, d.halo_hi, d.send_lo, d.send_hi)
+        d.halo_lo, d.halo_hi, d.send_lo, d.send_hi = (torch.zeros(n, dtype=torch.int16) for _ in range(4))
+        code = lambda r, side: ((torch.arange(n) * 7919 + 977 * r + 31 * side) % 65536 - 32768).to(torch.int16)
+        d.send_lo.copy_(code(rank, 0))
+        d.send_hi.copy_(code(rank, 1))
+        ex.exchange(d)
+        ok1 = ok1 and torch.equal(d.halo_lo, code(lower, 1)) and torch.equal(d.halo_hi, code(upper, 0))
+        d.halo_lo, d.halo_hi, d.send_lo, d.send_hi = saved
         # 2. one streaming step assembled from slabs vs the whole box
         rng = np.random.default_rng(5)
         full = rng.random((19, NZ, NY, NX))
