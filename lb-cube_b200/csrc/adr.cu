@@ -68,6 +68,7 @@ __device__ __forceinline__ void fluid_reaction_body(const Real* __restrict__ cur
                                                     Real omega_c, Real k, double* __restrict__ partials,
                                                     Real* __restrict__ u_out) {
   using SL = typename ScalarOf<FL>::type;
+  pdl_enter();
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double sums[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -379,18 +380,20 @@ cudaError_t launch_fluid_reaction(const Real* cur_f, Real* nxt_f, const Real* cu
     if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
   }
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
+  // launched as programmatic dependents of the previous launch (pdl_enter)
   if (partials != nullptr) {
     if constexpr (FL::Q == 9 && sizeof(Real) == 4 && LBCUBE_STATS_MIN_BLOCKS > 0)
-      fluid_reaction_stats_kernel<FL, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, partials);
+      return launch_pdl(fluid_reaction_stats_kernel<FL, Real, CT>, grid_dims(g), dim3(block_dims(g)),
+                        stream, cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus,
+                        omega_c, k, partials);
     else
-      fluid_reaction_kernel<FL, Real, CT, true><<<grid_dims(g), block_dims(g), 0, stream>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, partials);
-  } else {
-    fluid_reaction_kernel<FL, Real, CT, false><<<grid_dims(g), block_dims(g), 0, stream>>>(
-        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c, k, nullptr);
+      return launch_pdl(fluid_reaction_kernel<FL, Real, CT, true, false>, grid_dims(g),
+                        dim3(block_dims(g)), stream, cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g,
+                        omega, omega_minus, omega_c, k, partials, (Real*)nullptr);
   }
-  return cudaGetLastError();
+  return launch_pdl(fluid_reaction_kernel<FL, Real, CT, false, false>, grid_dims(g), dim3(block_dims(g)),
+                    stream, cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c,
+                    k, (double*)nullptr, (Real*)nullptr);
 }
 
 // The fused step with the advecting velocity stored (no statistics), for the

@@ -6,6 +6,7 @@
 #include <climits>
 #include <cstddef>
 #include <cstdint>
+#include <utility>
 
 #include "lattices.cuh"
 
@@ -42,6 +43,40 @@ __device__ __forceinline__ bool cell_of(const Grid& g, int& x, int& y, int& z) {
 // Linear block index used to address per-block partial sums.
 __device__ __forceinline__ long long block_linear() {
   return (long long)blockIdx.y * gridDim.x + blockIdx.x;
+}
+
+// Programmatic dependent launch. pdl_enter() at the top of a kernel waits
+// until the grid it depends on has completed and its writes are visible (a
+// no-op unless the kernel was launched with the programmatic-serialization
+// attribute), then lets the next launch in the stream be scheduled, so that
+// launch's blocks take the SMs that this grid's last blocks free instead of
+// waiting for the whole grid to drain. launch_pdl launches with that attribute.
+#ifndef LBCUBE_PDL
+#define LBCUBE_PDL 1
+#endif
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                              Args&&... args) {
+  if (!LBCUBE_PDL) {
+    kernel<<<grid, block, 0, s>>>(std::forward<Args>(args)...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 inline dim3 grid_dims(const Grid& g) { return dim3((unsigned)(g.xblocks * g.ny), (unsigned)g.nz, 1); }

@@ -134,6 +134,7 @@ __global__ void __cluster_dims__(kFinalBlocks, 1, 1) __launch_bounds__(kFinalThr
     stats_append_kernel(const double* __restrict__ partials, long long blocks, long long cells,
                         double k, double* __restrict__ table, unsigned long long rows,
                         unsigned long long* __restrict__ row_counter) {
+  pdl_enter();
   double s[kStatSums];
   if (sum_partials(partials, blocks, s)) {
     const unsigned long long row = *row_counter;
@@ -261,9 +262,9 @@ extern "C" int lbm_reactive_stats_append_async(int fluid_lattice, int precision,
   const Span writes[2] = {{table, table_rows * 8 * sizeof(double)}, {row_counter, sizeof(unsigned long long)}};
   if (any_overlap(reads, writes)) return (int)cudaErrorInvalidValue;
   const double k = precision == LBM_FLOAT ? (double)(float)k_react : k_react;
-  stats_append_kernel<<<kFinalBlocks, kFinalThreads, 0, as_stream(stream)>>>(partials, g.blocks(), g.plane, k, table,
-                                                                  table_rows, row_counter);
-  return (int)cudaGetLastError();
+  return (int)launch_pdl(stats_append_kernel, dim3(kFinalBlocks), dim3(kFinalThreads), as_stream(stream),
+                         (const double*)partials, (long long)g.blocks(), (long long)g.plane, k, table,
+                         (unsigned long long)table_rows, row_counter);
 }
 
 // Statistics of a domain split across ranks: each rank reduces its partials
