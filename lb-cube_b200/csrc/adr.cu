@@ -383,16 +383,16 @@ cudaError_t launch_fluid_reaction(const Real* cur_f, Real* nxt_f, const Real* cu
   // launched as programmatic dependents of the previous launch (pdl_enter)
   if (partials != nullptr) {
     if constexpr (FL::Q == 9 && sizeof(Real) == 4 && LBCUBE_STATS_MIN_BLOCKS > 0)
-      return launch_pdl(fluid_reaction_stats_kernel<FL, Real, CT>, grid_dims(g), dim3(block_dims(g)),
+      return launch_pdl(fluid_reaction_stats_kernel<FL, Real, CT>, grid_dims(g), dim3(block_dims(g)), 0,
                         stream, cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus,
                         omega_c, k, partials);
     else
       return launch_pdl(fluid_reaction_kernel<FL, Real, CT, true, false>, grid_dims(g),
-                        dim3(block_dims(g)), stream, cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g,
+                        dim3(block_dims(g)), 0, stream, cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g,
                         omega, omega_minus, omega_c, k, partials, (Real*)nullptr);
   }
   return launch_pdl(fluid_reaction_kernel<FL, Real, CT, false, false>, grid_dims(g), dim3(block_dims(g)),
-                    stream, cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c,
+                    0, stream, cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, omega_minus, omega_c,
                     k, (double*)nullptr, (Real*)nullptr);
 }
 

@@ -60,16 +60,16 @@ __device__ __forceinline__ void pdl_enter() {
 }
 
 template <class... KArgs, class... Args>
-inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
-                              Args&&... args) {
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t s, Args&&... args) {
   if (!LBCUBE_PDL) {
-    kernel<<<grid, block, 0, s>>>(std::forward<Args>(args)...);
+    kernel<<<grid, block, smem, s>>>(std::forward<Args>(args)...);
     return cudaGetLastError();
   }
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = grid;
   cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;

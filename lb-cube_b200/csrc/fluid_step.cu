@@ -37,12 +37,11 @@ cudaError_t launch_fluid_step(const Real* cur, Real* nxt, size_t nx, size_t ny, 
     }
   }
   if constexpr (kUsePlanes<L, Real, CT>)
-    fluid_step_planes_kernel<L, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(
-        planes_of<const Real, L::Q>(cur, g), planes_of<Real, L::Q>(nxt, g), g, omega, omega_minus);
-  else
-    fluid_step_kernel<L, Real, CT><<<grid_dims(g), block_dims(g), 0, stream>>>(cur, nxt, g, omega,
-                                                                           omega_minus);
-  return cudaGetLastError();
+    return launch_pdl(fluid_step_planes_kernel<L, Real, CT>, grid_dims(g), dim3(block_dims(g)), 0, stream,
+                      planes_of<const Real, L::Q>(cur, g), planes_of<Real, L::Q>(nxt, g), g, omega,
+                      omega_minus);
+  return launch_pdl(fluid_step_kernel<L, Real, CT, false>, grid_dims(g), dim3(block_dims(g)), 0, stream,
+                    cur, nxt, g, omega, omega_minus, (double*)nullptr);
 }
 
 // One step plus the diagnostics of the state it writes (diag.cuh): the

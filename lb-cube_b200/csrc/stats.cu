@@ -262,7 +262,7 @@ extern "C" int lbm_reactive_stats_append_async(int fluid_lattice, int precision,
   const Span writes[2] = {{table, table_rows * 8 * sizeof(double)}, {row_counter, sizeof(unsigned long long)}};
   if (any_overlap(reads, writes)) return (int)cudaErrorInvalidValue;
   const double k = precision == LBM_FLOAT ? (double)(float)k_react : k_react;
-  return (int)launch_pdl(stats_append_kernel, dim3(kFinalBlocks), dim3(kFinalThreads), as_stream(stream),
+  return (int)launch_pdl(stats_append_kernel, dim3(kFinalBlocks), dim3(kFinalThreads), 0, as_stream(stream),
                          (const double*)partials, (long long)g.blocks(), (long long)g.plane, k, table,
                          (unsigned long long)table_rows, row_counter);
 }

@@ -52,6 +52,7 @@ template <class L, class Real, int CT, bool DIAG = false>
 __global__ void __launch_bounds__(kThreads)
     fluid_step_kernel(const Real* __restrict__ cur, Real* __restrict__ nxt, Grid g, Real omega,
                       Real omega_minus, double* __restrict__ partials = nullptr) {
+  pdl_enter();
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   Real f[L::Q];
@@ -99,6 +100,7 @@ template <class L, class Real, int CT>
 __global__ void __launch_bounds__(kThreads)
     fluid_step_planes_kernel(const Planes<const Real, L::Q> cur, const Planes<Real, L::Q> nxt,
                              Grid g, Real omega, Real omega_minus) {
+  pdl_enter();
   int x, y, z;
   if (!cell_of(g, x, y, z)) return;
   const int xm = x == 0 ? g.nx - 1 : x - 1, xp = x == g.nx - 1 ? 0 : x + 1;

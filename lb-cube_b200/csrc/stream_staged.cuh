@@ -133,6 +133,7 @@ __global__ void __launch_bounds__(kMaxRowThreads, LBCUBE_STAGED_MIN_BLOCKS)
                              float omega_minus, typename S::Params p,
                              SlabArgs<unsigned short> slab = {}) {
   static_assert(S::V == 4, "four cells per thread");
+  pdl_enter();
   // kStages row buffers, then the kStages mbarriers (8-byte aligned: a stage
   // is a multiple of 16 bytes)
   extern __shared__ __align__(128) unsigned char smem[];
@@ -272,9 +273,8 @@ inline cudaError_t launch_staged_step(const Grid& g, cudaStream_t stream, const 
     if (err != cudaSuccess) return err;
   }
   const unsigned blocks = (unsigned)((sg.rows - sg.row0 + kStagedRows - 1) / kStagedRows);
-  kernel<<<blocks, (unsigned)staged_threads(g.nx), smem, stream>>>(cur, nxt, sg, omega, omega_minus, p,
-                                                                    slab);
-  return cudaGetLastError();
+  return launch_pdl(kernel, dim3(blocks), dim3((unsigned)staged_threads(g.nx)), smem, stream, cur, nxt, sg,
+                    omega, omega_minus, p, slab);
 }
 
 }  // namespace lbcube

@@ -356,6 +356,7 @@ __device__ __forceinline__ void fluid_step_vec_body(const typename S::elem* __re
                                                     const typename S::Params& p,
                                                     double* __restrict__ partials,
                                                     const SlabArgs<typename S::elem>& slab) {
+  pdl_enter();
   using R = typename S::compute;
   constexpr int V = S::V;
   const Grid& g = vg.g;
@@ -428,10 +429,13 @@ inline void launch_vec_step(const VecGrid& vg, dim3 grid, unsigned threads, cuda
                             const typename S::elem* cur, typename S::elem* nxt,
                             typename S::compute omega, typename S::compute omega_minus,
                             const typename S::Params& p) {
+  // programmatic dependent launches (pdl_enter opens the body)
   if constexpr (S::kBudgeted && L::Q <= 19)
-    fluid_step_vec16_kernel<L, S, CT><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega, omega_minus, p);
+    launch_pdl(fluid_step_vec16_kernel<L, S, CT>, grid, dim3(threads), 0, stream, cur, nxt, vg, omega,
+               omega_minus, p);
   else
-    fluid_step_vec_kernel<L, S, CT><<<grid, threads, 0, stream>>>(cur, nxt, vg, omega, omega_minus, p);
+    launch_pdl(fluid_step_vec_kernel<L, S, CT, false, false>, grid, dim3(threads), 0, stream, cur, nxt,
+               vg, omega, omega_minus, p, (double*)nullptr, SlabArgs<typename S::elem>{});
 }
 
 template <class S>
