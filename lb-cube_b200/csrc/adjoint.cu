@@ -23,6 +23,7 @@ __global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
     adjoint_step_kernel(const Real* __restrict__ fn, const Real* __restrict__ lam_next,
                         Real* __restrict__ lam, Grid g, AdjointParams ap,
                         double* __restrict__ dtau_slots) {
+  pdl_enter();
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double dtau = 0.0;
@@ -108,20 +109,21 @@ template <class L, class Real>
 cudaError_t launch_adjoint_step(int collision, const Real* fn, const Real* lam_next, Real* lam,
                                 const Grid& g, const AdjointParams& ap, double* dtau_slots,
                                 cudaStream_t s) {
+  // programmatic dependent launches (the kernel opens with pdl_enter)
+  const dim3 grid = grid_dims(g), block(block_dims(g));
   if (collision == kBGK)
-    adjoint_step_kernel<L, Real, kBGK><<<grid_dims(g), block_dims(g), 0, s>>>(fn, lam_next, lam, g, ap,
-                                                                          dtau_slots);
-  else if (collision == kTRT)
-    adjoint_step_kernel<L, Real, kTRT><<<grid_dims(g), block_dims(g), 0, s>>>(fn, lam_next, lam, g, ap,
-                                                                          dtau_slots);
-  else if constexpr (L::Q != 27) {
+    return launch_pdl(adjoint_step_kernel<L, Real, kBGK>, grid, block, 0, s, fn, lam_next, lam, g, ap,
+                      dtau_slots);
+  if (collision == kTRT)
+    return launch_pdl(adjoint_step_kernel<L, Real, kTRT>, grid, block, 0, s, fn, lam_next, lam, g, ap,
+                      dtau_slots);
+  if constexpr (L::Q != 27) {
     if (collision != kMRT) return cudaErrorInvalidValue;
-    adjoint_step_kernel<L, Real, kMRT><<<grid_dims(g), block_dims(g), 0, s>>>(fn, lam_next, lam, g, ap,
-                                                                          dtau_slots);
+    return launch_pdl(adjoint_step_kernel<L, Real, kMRT>, grid, block, 0, s, fn, lam_next, lam, g, ap,
+                      dtau_slots);
   } else {
     return cudaErrorInvalidValue;
   }
-  return cudaGetLastError();
 }
 
 // Forward step used by the gradient driver (same engine launcher as the public API).

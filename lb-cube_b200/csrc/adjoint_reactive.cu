@@ -185,6 +185,7 @@ __global__ void __launch_bounds__(kThreads)
                             Real* __restrict__ lb, Real* __restrict__ ubar_out, Grid g,
                             ReactiveParams rp, double* __restrict__ slots,
                             SlabFaces<typename SP::elem, Real> faces = {}) {
+  pdl_enter();
   using SL = typename ScalarOf<FL>::type;
   const size_t a_off = (size_t)face_planes<FL>() * g.ny * g.nx;
   const size_t b_off = a_off + (size_t)face_planes<SL>() * g.ny * g.nx;
@@ -268,6 +269,7 @@ __global__ void __launch_bounds__(kThreads, kAdjointBlocks<Real>)
                                  Real* __restrict__ lf, Grid g, AdjointParams ap, float rho0,
                                  double* __restrict__ slots,
                                  SlabFaces<typename SP::elem, Real> faces = {}) {
+  pdl_enter();
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double dtau = 0.0;
@@ -424,20 +426,23 @@ cudaError_t launch_reactive_adjoint(int collision, const typename SP::elem* fn,
                                     const Real* lb_next, Real* lf, Real* la, Real* lb, Real* ubar,
                                     const Grid& g, const ReactiveParams& rp, double* slots,
                                     cudaStream_t s) {
-  reaction_adjoint_kernel<FL, Real, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
-      an, bn, u_next, la_next, lb_next, la, lb, ubar, g, rp, slots);
+  // programmatic dependent launches (both kernels open with pdl_enter)
+  using Faces = SlabFaces<typename SP::elem, Real>;
+  const dim3 grid = grid_dims(g), block(block_dims(g));
+  cudaError_t err = launch_pdl(reaction_adjoint_kernel<FL, Real, SP, false>, grid, block, 0, s, an, bn,
+                               u_next, la_next, lb_next, la, lb, ubar, g, rp, slots, Faces{});
+  if (err != cudaSuccess) return err;
   if (collision == kBGK)
-    coupled_fluid_adjoint_kernel<FL, Real, kBGK, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
-        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots);
-  else if (collision == kTRT)
-    coupled_fluid_adjoint_kernel<FL, Real, kTRT, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
-        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots);
-  else if constexpr (FL::Q != 27)
-    coupled_fluid_adjoint_kernel<FL, Real, kMRT, SP><<<grid_dims(g), block_dims(g), 0, s>>>(
-        fn, lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots);
+    return launch_pdl(coupled_fluid_adjoint_kernel<FL, Real, kBGK, SP, false>, grid, block, 0, s, fn,
+                      lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots, Faces{});
+  if (collision == kTRT)
+    return launch_pdl(coupled_fluid_adjoint_kernel<FL, Real, kTRT, SP, false>, grid, block, 0, s, fn,
+                      lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots, Faces{});
+  if constexpr (FL::Q != 27)
+    return launch_pdl(coupled_fluid_adjoint_kernel<FL, Real, kMRT, SP, false>, grid, block, 0, s, fn,
+                      lf_next, ubar, lf, g, rp.fluid, rp.rho0, slots, Faces{});
   else
     return cudaErrorInvalidValue;
-  return cudaGetLastError();
 }
 
 struct ReactiveLayout {
@@ -849,8 +854,8 @@ cudaError_t slab_adjoint_step(int collision, const typename SP::elem* fn,
     gr.z0 = z0;
     dim3 grid = grid_dims(gr);
     grid.y = (unsigned)planes;
-    reaction_adjoint_kernel<FL, Real, SP, SLAB><<<grid, block_dims(gr), 0, s>>>(
-        an, bn, u_next, la_next, lb_next, la, lb, ubar, gr, rp, slots, faces);
+    launch_pdl(reaction_adjoint_kernel<FL, Real, SP, SLAB>, grid, dim3(block_dims(gr)), 0, s, an, bn,
+               u_next, la_next, lb_next, la, lb, ubar, gr, rp, slots, faces);
   });
   ranges([&](int z0, int planes, auto slab) {
     constexpr bool SLAB = decltype(slab)::value;
@@ -858,15 +863,16 @@ cudaError_t slab_adjoint_step(int collision, const typename SP::elem* fn,
     gr.z0 = z0;
     dim3 grid = grid_dims(gr);
     grid.y = (unsigned)planes;
+    const dim3 block(block_dims(gr));
     if (collision == kBGK)
-      coupled_fluid_adjoint_kernel<FL, Real, kBGK, SP, SLAB><<<grid, block_dims(gr), 0, s>>>(
-          fn, lf_next, ubar, lf, gr, rp.fluid, rp.rho0, slots, faces);
+      launch_pdl(coupled_fluid_adjoint_kernel<FL, Real, kBGK, SP, SLAB>, grid, block, 0, s, fn, lf_next,
+                 ubar, lf, gr, rp.fluid, rp.rho0, slots, faces);
     else if (collision == kTRT)
-      coupled_fluid_adjoint_kernel<FL, Real, kTRT, SP, SLAB><<<grid, block_dims(gr), 0, s>>>(
-          fn, lf_next, ubar, lf, gr, rp.fluid, rp.rho0, slots, faces);
+      launch_pdl(coupled_fluid_adjoint_kernel<FL, Real, kTRT, SP, SLAB>, grid, block, 0, s, fn, lf_next,
+                 ubar, lf, gr, rp.fluid, rp.rho0, slots, faces);
     else if constexpr (FL::Q != 27)
-      coupled_fluid_adjoint_kernel<FL, Real, kMRT, SP, SLAB><<<grid, block_dims(gr), 0, s>>>(
-          fn, lf_next, ubar, lf, gr, rp.fluid, rp.rho0, slots, faces);
+      launch_pdl(coupled_fluid_adjoint_kernel<FL, Real, kMRT, SP, SLAB>, grid, block, 0, s, fn, lf_next,
+                 ubar, lf, gr, rp.fluid, rp.rho0, slots, faces);
   });
   return cudaGetLastError();
 }

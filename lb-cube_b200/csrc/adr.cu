@@ -23,6 +23,7 @@ __global__ void __launch_bounds__(kThreads)
     scalar_step_kernel(const Real* __restrict__ cur_s, Real* __restrict__ nxt_s,
                        const Real* __restrict__ cur_f, Grid g, Real omega_c, Real source) {
   using SL = typename ScalarOf<FL>::type;
+  pdl_enter();
   int x, y, z;
   if (!cell_of(g, x, y, z)) return;
   const int cell = (z * g.ny + y) * g.nx + x;
@@ -40,6 +41,7 @@ __global__ void __launch_bounds__(kThreads)
                        const Real* __restrict__ cur_b, Real* __restrict__ nxt_b,
                        const Real* __restrict__ cur_f, Grid g, Real omega_c, Real k) {
   using SL = typename ScalarOf<FL>::type;
+  pdl_enter();
   int x, y, z;
   if (!cell_of(g, x, y, z)) return;
   const int cell = (z * g.ny + y) * g.nx + x;
@@ -159,6 +161,7 @@ __global__ void __launch_bounds__(kThreads)
   const size_t n2 = (size_t)g.ny * g.nx;
   const size_t a_off = (size_t)face_planes<FL>() * n2;
   const size_t b_off = a_off + (size_t)face_planes<SL>() * n2;
+  pdl_enter();
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double sums[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -272,20 +275,22 @@ cudaError_t launch_fluid_reaction_slab(const Real* cur_f, Real* nxt_f, const Rea
     gr.z0 = z0;
     dim3 grid = grid_dims(gr);
     grid.y = (unsigned)(z1 - z0);
+    const dim3 block(block_dims(gr));
+    Real* const none = nullptr;
     if (face && partials != nullptr)
-      fluid_reaction_slab_kernel<FL, Real, CT, true><<<grid, block_dims(gr), 0, stream>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, halo_lo,
-          halo_hi, send_lo, send_hi, partials);
+      launch_pdl(fluid_reaction_slab_kernel<FL, Real, CT, true, false>, grid, block, 0, stream, cur_f, nxt_f,
+                 cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, halo_lo, halo_hi, send_lo,
+                 send_hi, partials, none);
     else if (face)
-      fluid_reaction_slab_kernel<FL, Real, CT, false><<<grid, block_dims(gr), 0, stream>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, halo_lo,
-          halo_hi, send_lo, send_hi, nullptr);
+      launch_pdl(fluid_reaction_slab_kernel<FL, Real, CT, false, false>, grid, block, 0, stream, cur_f,
+                 nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, halo_lo, halo_hi,
+                 send_lo, send_hi, (double*)nullptr, none);
     else if (partials != nullptr)
-      fluid_reaction_kernel<FL, Real, CT, true><<<grid, block_dims(gr), 0, stream>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, partials);
+      launch_pdl(fluid_reaction_kernel<FL, Real, CT, true, false>, grid, block, 0, stream, cur_f, nxt_f,
+                 cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, partials, none);
     else
-      fluid_reaction_kernel<FL, Real, CT, false><<<grid, block_dims(gr), 0, stream>>>(
-          cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, nullptr);
+      launch_pdl(fluid_reaction_kernel<FL, Real, CT, false, false>, grid, block, 0, stream, cur_f, nxt_f,
+                 cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, (double*)nullptr, none);
   };
   const int zb = (int)z_begin, ze = (int)z_end, last = g.nz - 1;
   if (zb == 0) launch(0, 1, true);
@@ -330,9 +335,8 @@ cudaError_t launch_scalar(const Real* cur_s, Real* nxt_s, const Real* cur_f, siz
   const Span reads[2] = {{cur_s, sb}, {cur_f, fb}};
   const Span writes[1] = {{nxt_s, sb}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  scalar_step_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, stream>>>(cur_s, nxt_s, cur_f, g,
-                                                                       omega_c, source);
-  return cudaGetLastError();
+  return launch_pdl(scalar_step_kernel<FL, Real>, grid_dims(g), dim3(block_dims(g)), 0, stream, cur_s,
+                    nxt_s, cur_f, g, omega_c, source);
 }
 
 template <class FL, class Real>
@@ -351,9 +355,8 @@ cudaError_t launch_reaction(const Real* cur_a, Real* nxt_a, const Real* cur_b, R
   const Span reads[3] = {{cur_a, sb}, {cur_b, sb}, {cur_f, fb}};
   const Span writes[2] = {{nxt_a, sb}, {nxt_b, sb}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  reaction_ab_kernel<FL, Real><<<grid_dims(g), block_dims(g), 0, stream>>>(cur_a, nxt_a, cur_b, nxt_b,
-                                                                       cur_f, g, omega_c, k);
-  return cudaGetLastError();
+  return launch_pdl(reaction_ab_kernel<FL, Real>, grid_dims(g), dim3(block_dims(g)), 0, stream, cur_a,
+                    nxt_a, cur_b, nxt_b, cur_f, g, omega_c, k);
 }
 
 template <class FL, class Real, int CT>
@@ -404,20 +407,20 @@ cudaError_t fluid_reaction_with_velocity(int collision, const Real* cur_f, Real*
                                          const Real* cur_a, Real* nxt_a, const Real* cur_b,
                                          Real* nxt_b, Real* u_out, const Grid& g, Real omega,
                                          Real omega_c, Real k, cudaStream_t s) {
-  if (collision == kBGK) {
-    fluid_reaction_kernel<FL, Real, kBGK, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, nullptr, u_out);
-  } else if (collision == kTRT) {
-    fluid_reaction_kernel<FL, Real, kTRT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, trt_omega_minus<Real>(omega), omega_c,
-        k, nullptr, u_out);
-  } else if (collision == kMRT) {
-    fluid_reaction_kernel<FL, Real, kMRT, false, true><<<grid_dims(g), block_dims(g), 0, s>>>(
-        cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, nullptr, u_out);
-  } else {
-    return cudaErrorInvalidValue;
-  }
-  return cudaGetLastError();
+  // programmatic dependent launches (the kernel opens with pdl_enter)
+  const dim3 grid = grid_dims(g), block(block_dims(g));
+  double* const none = nullptr;
+  if (collision == kBGK)
+    return launch_pdl(fluid_reaction_kernel<FL, Real, kBGK, false, true>, grid, block, 0, s, cur_f, nxt_f,
+                      cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, none, u_out);
+  if (collision == kTRT)
+    return launch_pdl(fluid_reaction_kernel<FL, Real, kTRT, false, true>, grid, block, 0, s, cur_f, nxt_f,
+                      cur_a, nxt_a, cur_b, nxt_b, g, omega, trt_omega_minus<Real>(omega), omega_c, k,
+                      none, u_out);
+  if (collision == kMRT)
+    return launch_pdl(fluid_reaction_kernel<FL, Real, kMRT, false, true>, grid, block, 0, s, cur_f, nxt_f,
+                      cur_a, nxt_a, cur_b, nxt_b, g, omega, Real(0), omega_c, k, none, u_out);
+  return cudaErrorInvalidValue;
 }
 
 // The slab form of fluid_reaction_with_velocity (all planes of the slab, no
@@ -440,20 +443,22 @@ cudaError_t fluid_reaction_slab_with_velocity(int collision, const Real* cur_f, 
       gr.z0 = z0;
       dim3 grid = grid_dims(gr);
       grid.y = (unsigned)planes;
+      const dim3 block(block_dims(gr));
+      double* const none = nullptr;
       if (face && u_out != nullptr)
-        fluid_reaction_slab_kernel<FL, Real, CT, false, true><<<grid, block_dims(gr), 0, s>>>(
-            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, halo_lo, halo_hi,
-            send_lo, send_hi, nullptr, u_out);
+        launch_pdl(fluid_reaction_slab_kernel<FL, Real, CT, false, true>, grid, block, 0, s, cur_f, nxt_f,
+                   cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, halo_lo, halo_hi, send_lo,
+                   send_hi, none, u_out);
       else if (face)
-        fluid_reaction_slab_kernel<FL, Real, CT, false><<<grid, block_dims(gr), 0, s>>>(
-            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, halo_lo, halo_hi,
-            send_lo, send_hi, nullptr);
+        launch_pdl(fluid_reaction_slab_kernel<FL, Real, CT, false, false>, grid, block, 0, s, cur_f,
+                   nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, halo_lo, halo_hi,
+                   send_lo, send_hi, none, (Real*)nullptr);
       else if (u_out != nullptr)
-        fluid_reaction_kernel<FL, Real, CT, false, true><<<grid, block_dims(gr), 0, s>>>(
-            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, nullptr, u_out);
+        launch_pdl(fluid_reaction_kernel<FL, Real, CT, false, true>, grid, block, 0, s, cur_f, nxt_f,
+                   cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, none, u_out);
       else
-        fluid_reaction_kernel<FL, Real, CT, false><<<grid, block_dims(gr), 0, s>>>(
-            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, nullptr);
+        launch_pdl(fluid_reaction_kernel<FL, Real, CT, false, false>, grid, block, 0, s, cur_f, nxt_f,
+                   cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, none, (Real*)nullptr);
     };
     if (g.nz >= 3) launch(1, g.nz - 2, false);
     launch(0, 1, true);

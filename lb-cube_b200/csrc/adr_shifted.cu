@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(kThreads)
   using SL = typename ScalarOf<FL>::type;
   const size_t a_off = (size_t)face_planes<FL>() * g.ny * g.nx;
   const size_t b_off = a_off + (size_t)face_planes<SL>() * g.ny * g.nx;
+  pdl_enter();
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double sums[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -143,15 +144,16 @@ cudaError_t launch_shifted_coupled(const unsigned short* cf, unsigned short* nf,
                                    double* partials, const Grid& g, float omega, float omega_c,
                                    float k, float rho0, float c0, cudaStream_t s) {
   const float om = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
+  // programmatic dependent launches (the kernel opens with pdl_enter)
 #define LBCUBE_SC(ST, UO)                                                                          \
-  fluid_reaction_shifted_kernel<FL, FMT, CT, ST, UO><<<grid_dims(g), block_dims(g), 0, s>>>(      \
-      cf, nf, ca, na, cb, nb, g, omega, om, omega_c, k, rho0, c0, partials, u_out)
+  return launch_pdl(fluid_reaction_shifted_kernel<FL, FMT, CT, ST, UO, false>, grid_dims(g),      \
+                    dim3(block_dims(g)), 0, s, cf, nf, ca, na, cb, nb, g, omega, om, omega_c, k,  \
+                    rho0, c0, partials, u_out, CodeFaces{})
   if (partials != nullptr && u_out != nullptr) LBCUBE_SC(true, true);
-  else if (partials != nullptr) LBCUBE_SC(true, false);
-  else if (u_out != nullptr) LBCUBE_SC(false, true);
-  else LBCUBE_SC(false, false);
+  if (partials != nullptr) LBCUBE_SC(true, false);
+  if (u_out != nullptr) LBCUBE_SC(false, true);
+  LBCUBE_SC(false, false);
 #undef LBCUBE_SC
-  return cudaGetLastError();
 }
 
 template <class FL, int FMT>
@@ -201,14 +203,15 @@ cudaError_t fluid_reaction_shifted_slab(int collision, const unsigned short* cur
       gr.z0 = z0;
       dim3 grid = grid_dims(gr);
       grid.y = (unsigned)planes;
+      const dim3 block(block_dims(gr));
+      double* const none = nullptr;
       if (u_out != nullptr)
-        fluid_reaction_shifted_kernel<FL, FMT, CT, false, true, SLAB><<<grid, block_dims(gr), 0, s>>>(
-            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, rho0, c0, nullptr, u_out,
-            faces);
+        launch_pdl(fluid_reaction_shifted_kernel<FL, FMT, CT, false, true, SLAB>, grid, block, 0, s, cur_f,
+                   nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, rho0, c0, none, u_out, faces);
       else
-        fluid_reaction_shifted_kernel<FL, FMT, CT, false, false, SLAB><<<grid, block_dims(gr), 0, s>>>(
-            cur_f, nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, rho0, c0, nullptr, nullptr,
-            faces);
+        launch_pdl(fluid_reaction_shifted_kernel<FL, FMT, CT, false, false, SLAB>, grid, block, 0, s, cur_f,
+                   nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, rho0, c0, none,
+                   (float*)nullptr, faces);
     };
     if (g.nz >= 3) range(1, g.nz - 2, std::false_type{});
     range(0, 1, std::true_type{});

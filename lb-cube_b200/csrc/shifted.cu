@@ -158,8 +158,8 @@ cudaError_t launch_shifted_slab_step(const void* cur_v, void* nxt_v, size_t nx, 
     grid.y = 1;
     SlabArgs<E> f = faces;
     f.z_begin = (int)z;
-    fluid_step_vec_kernel<L, S, CT, false, true><<<grid, vec_block_threads(vg), 0, stream>>>(
-        cur, nxt, vg, omega, omega_minus, p, nullptr, f);
+    launch_pdl(fluid_step_vec_kernel<L, S, CT, false, true>, grid, dim3(vec_block_threads(vg)), 0, stream,
+               cur, nxt, vg, omega, omega_minus, p, (double*)nullptr, f);
   };
   if (lo_face) face(0);
   if (hi_face && nz > 1) face(nz - 1);

@@ -72,16 +72,16 @@ cudaError_t launch_slab_step(const Real* cur, Real* nxt, size_t nx, size_t ny, s
       gi.z0 = (int)ib;
       dim3 grid = grid_dims(gi);
       grid.y = (unsigned)(ie - ib);
-      fluid_step_kernel<L, Real, CT><<<grid, block_dims(gi), 0, s>>>(cur, nxt, gi, omega,
-                                                                     omega_minus);
+      launch_pdl(fluid_step_kernel<L, Real, CT, false>, grid, dim3(block_dims(gi)), 0, s, cur, nxt, gi,
+                 omega, omega_minus, (double*)nullptr);
     }
   }
   auto face = [&](size_t z) {
     dim3 grid = vec_grid_dims(vg);
     grid.y = 1;
     const SlabArgs<Real> slab{halo_lo, halo_hi, send_lo, send_hi, (int)z};
-    fluid_step_vec_kernel<L, S, CT, false, true><<<grid, vec_block_threads(vg), 0, s>>>(
-        cur, nxt, vg, omega, omega_minus, typename S::Params{}, nullptr, slab);
+    launch_pdl(fluid_step_vec_kernel<L, S, CT, false, true>, grid, dim3(vec_block_threads(vg)), 0, s, cur,
+               nxt, vg, omega, omega_minus, typename S::Params{}, (double*)nullptr, slab);
   };
   if (lo_face) face(0);
   if (hi_face && nz > 1) face(nz - 1);
@@ -236,6 +236,7 @@ struct CopyList {
 
 static __global__ void __launch_bounds__(256)
     copy_buffers_kernel(const CopyList list, size_t bytes) {
+  pdl_enter();
   const unsigned char* __restrict__ src = list.src[blockIdx.y];
   unsigned char* __restrict__ dst = list.dst[blockIdx.y];
   const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -276,6 +277,7 @@ extern "C" int lbm_copy_buffers_async(int count, const void* const* src, void* c
     }
   const size_t words = (bytes + 15) / 16;
   const unsigned blocks_x = (unsigned)std::min<size_t>((words + 255) / 256, 64);
-  copy_buffers_kernel<<<dim3(blocks_x, (unsigned)count), 256, 0, as_stream(stream)>>>(list, bytes);
-  return (int)cudaGetLastError();
+  // a programmatic dependent launch, like the slab steps around it
+  return (int)launch_pdl(copy_buffers_kernel, dim3(blocks_x, (unsigned)count), dim3(256), 0, as_stream(stream),
+                         list, bytes);
 }
