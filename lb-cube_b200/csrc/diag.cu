@@ -20,6 +20,7 @@ namespace lbcube {
 template <class L, class Real>
 __global__ void __launch_bounds__(kThreads)
     diag_partials_kernel(const Real* __restrict__ f, Grid g, double* __restrict__ partials) {
+  pdl_enter();
   int x, y, z;
   DiagAcc acc;
   if (cell_of(g, x, y, z)) {
@@ -45,6 +46,7 @@ __global__ void __cluster_dims__(kDiagFinalBlocks, 1, 1) __launch_bounds__(kDiag
     diag_finalize_kernel(const double* __restrict__ partials, long long count,
                          double speed_limit, double* __restrict__ out) {
   __shared__ double sh[kDiagFinalThreads][kDiagPartials];
+  pdl_enter();
   double m = 0.0, k = 0.0, n = 0.0, v = 0.0;
   for (long long b = (long long)blockIdx.x * kDiagFinalThreads + threadIdx.x; b < count;
        b += (long long)kDiagFinalBlocks * kDiagFinalThreads) {
@@ -97,8 +99,9 @@ __global__ void __cluster_dims__(kDiagFinalBlocks, 1, 1) __launch_bounds__(kDiag
 
 cudaError_t launch_diag_finalize(const double* partials, long long count, double speed_limit,
                                  double* out, cudaStream_t s) {
-  diag_finalize_kernel<<<kDiagFinalBlocks, kDiagFinalThreads, 0, s>>>(partials, count, speed_limit, out);
-  return cudaGetLastError();
+  // programmatic dependent launches (the diagnostics kernels open with pdl_enter)
+  return launch_pdl(diag_finalize_kernel, dim3(kDiagFinalBlocks), dim3(kDiagFinalThreads), 0, s, partials,
+                    count, speed_limit, out);
 }
 
 template <class L, class Real>
@@ -114,8 +117,7 @@ cudaError_t launch_diagnostics(const void* vf, size_t nx, size_t ny, size_t nz, 
   const Span reads[1] = {{f, (size_t)L::Q * g.plane * sizeof(Real)}};
   const Span writes[2] = {{partials, need}, {out, kDiagOut * sizeof(double)}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  diag_partials_kernel<L, Real><<<grid_dims(g), block_dims(g), 0, s>>>(f, g, partials);
-  err = cudaGetLastError();
+  err = launch_pdl(diag_partials_kernel<L, Real>, grid_dims(g), dim3(block_dims(g)), 0, s, f, g, partials);
   if (err != cudaSuccess) return err;
   return launch_diag_finalize(partials, g.blocks(), speed_limit, out, s);
 }

@@ -69,16 +69,16 @@ cudaError_t launch_fluid_step_diag(const Real* cur, Real* nxt, size_t nx, size_t
       const VecGrid vg = make_vec_grid(g, S::V);
       const dim3 grid = vec_grid_dims(vg);
       count = (long long)grid.x * grid.y;  // <= g.blocks(): a vector block spans >= one row block
-      fluid_step_vec_kernel<L, S, CT, true><<<grid, vec_block_threads(vg), 0, stream>>>(
-          cur, nxt, vg, omega, omega_minus, typename S::Params{}, partials);
+      err = launch_pdl(fluid_step_vec_kernel<L, S, CT, true, false>, grid, dim3(vec_block_threads(vg)), 0,
+                       stream, cur, nxt, vg, omega, omega_minus, typename S::Params{}, partials,
+                       SlabArgs<Real>{});
     }
   }
   if (count < 0) {
     count = g.blocks();
-    fluid_step_kernel<L, Real, CT, true><<<grid_dims(g), block_dims(g), 0, stream>>>(
-        cur, nxt, g, omega, omega_minus, partials);
+    err = launch_pdl(fluid_step_kernel<L, Real, CT, true>, grid_dims(g), dim3(block_dims(g)), 0, stream, cur,
+                     nxt, g, omega, omega_minus, partials);
   }
-  err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   return launch_diag_finalize(partials, count, speed_limit, out, stream);
 }

@@ -19,6 +19,7 @@ template <class SL, class Real>
 __global__ void __launch_bounds__(kThreads)
     stats_partials_kernel(const Real* __restrict__ a, const Real* __restrict__ b, Grid g,
                           double* __restrict__ partials) {
+  pdl_enter();
   int x, y, z;
   const bool active = cell_of(g, x, y, z);
   double sums[kStatSums] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -122,6 +123,7 @@ __device__ __forceinline__ void diagnostics_from_sums(const double (&s)[kStatSum
 __global__ void __cluster_dims__(kFinalBlocks, 1, 1) __launch_bounds__(kFinalThreads)
     stats_finalize_kernel(const double* __restrict__ partials, long long blocks, long long cells,
                           double k, double* __restrict__ out) {
+  pdl_enter();
   double s[kStatSums];
   if (sum_partials(partials, blocks, s)) diagnostics_from_sums(s, (double)cells, k, out);
 }
@@ -146,6 +148,7 @@ __global__ void __cluster_dims__(kFinalBlocks, 1, 1) __launch_bounds__(kFinalThr
 // The five sums alone: a rank's share of the statistics of a decomposed domain.
 __global__ void __cluster_dims__(kFinalBlocks, 1, 1) __launch_bounds__(kFinalThreads)
     stats_sums_kernel(const double* __restrict__ partials, long long blocks, double* __restrict__ out) {
+  pdl_enter();
   double s[kStatSums];
   if (sum_partials(partials, blocks, s)) {
 #pragma unroll
@@ -163,8 +166,9 @@ __global__ void stats_from_sums_kernel(const double* __restrict__ sums, double c
 
 cudaError_t launch_finalize(const Grid& g, double k, const double* partials, double* out,
                             cudaStream_t s) {
-  stats_finalize_kernel<<<kFinalBlocks, kFinalThreads, 0, s>>>(partials, g.blocks(), g.plane, k, out);
-  return cudaGetLastError();
+  // programmatic dependent launches (the statistics kernels open with pdl_enter)
+  return launch_pdl(stats_finalize_kernel, dim3(kFinalBlocks), dim3(kFinalThreads), 0, s, partials,
+                    (long long)g.blocks(), (long long)g.plane, k, out);
 }
 
 template <class SL, class Real>
@@ -183,8 +187,8 @@ cudaError_t launch_stats(const void* va, const void* vb, size_t nx, size_t ny, s
   const Span reads[2] = {{a, sb}, {b, sb}};
   const Span writes[2] = {{partials, need}, {out, 8 * sizeof(double)}};
   if (any_overlap(reads, writes)) return cudaErrorInvalidValue;
-  stats_partials_kernel<SL, Real><<<grid_dims(g), block_dims(g), 0, s>>>(a, b, g, partials);
-  err = cudaGetLastError();
+  err = launch_pdl(stats_partials_kernel<SL, Real>, grid_dims(g), dim3(block_dims(g)), 0, s, a, b, g,
+                   partials);
   if (err != cudaSuccess) return err;
   // k_react has the population precision, as in compute_reactive_stats<SL, Real>.
   return launch_finalize(g, (double)(Real)k, partials, out, s);
@@ -281,8 +285,8 @@ extern "C" int lbm_reactive_stats_sums_async(int fluid_lattice, size_t x_extent,
                                     x_extent, y_extent, z_extent, g);
   if (err != cudaSuccess) return (int)err;
   if (partials_bytes < (size_t)g.blocks() * kStatSums * sizeof(double)) return (int)cudaErrorInvalidValue;
-  stats_sums_kernel<<<kFinalBlocks, kFinalThreads, 0, as_stream(stream)>>>(partials, g.blocks(), sums);
-  return (int)cudaGetLastError();
+  return (int)launch_pdl(stats_sums_kernel, dim3(kFinalBlocks), dim3(kFinalThreads), 0, as_stream(stream),
+                         partials, (long long)g.blocks(), sums);
 }
 
 extern "C" int lbm_reactive_stats_from_sums_async(int precision, const double* sums, double cells,
