@@ -111,8 +111,18 @@ struct Codec<kE3M12S> {
   __device__ __forceinline__ static float2 decode2(unsigned int w) {
     return make_float2(e3m12_to_float((unsigned short)w), e3m12_to_float((unsigned short)(w >> 16)));
   }
+  // float_to_e3m12 of a (low half) and b (high half), regrouped: the bias
+  // subtraction joins the rounding add (the same sum mod 2^32; the bias has
+  // no bits below 23, so bit 11 of the biased and unbiased words agree), and
+  // the two signs go into the packed word at the end.
   __device__ __forceinline__ static unsigned int encode2(float a, float b) {
-    return (unsigned int)float_to_e3m12(a) | ((unsigned int)float_to_e3m12(b) << 16);
+    constexpr unsigned int kRound = 0x3FFu - ((127u - 6u) << 23);
+    const unsigned int ya = __float_as_uint(fabsf(a) + 0.015625f);
+    const unsigned int yb = __float_as_uint(fabsf(b) + 0.015625f);
+    const unsigned int ra = min((ya + kRound + ((ya >> 11) & 1u)) >> 11, 0x7FFFu);
+    const unsigned int rb = min((yb + kRound + ((yb >> 11) & 1u)) >> 11, 0x7FFFu);
+    return __byte_perm(ra, rb, 0x5410) | ((__float_as_uint(a) >> 16) & 0x8000u) |
+           (__float_as_uint(b) & 0x80000000u);
   }
 };
 template <>
