@@ -701,7 +701,7 @@ def run_kernel_survey(torch, E, dev, n=128, reps=10):
         d27.compute(f27, g27)
         ex27.exchange_all()
         return 0
-    timed("slab step D3Q27 f32 BGK (3 launches + face copies)", cells * 216, slab_step27)
+    timed("slab step D3Q27 f32 BGK (interior + faces + face copies)", cells * 216, slab_step27)
     del d27, ex27, f27, g27
     h = torch.empty((19, n, n, n), dtype=torch.int16, device=dev)
     hg = torch.empty_like(h)
@@ -763,7 +763,7 @@ def run_kernel_survey(torch, E, dev, n=128, reps=10):
         d.compute(f, g)
         ex.exchange_all()
         return 0
-    timed("slab step D3Q19 f32 TRT (3 launches + face copies)", cells * 152, slab_step)
+    timed("slab step D3Q19 f32 TRT (interior + faces + face copies)", cells * 152, slab_step)
     del a, b, a2, b2, part, dpart, mr, mu, ms
     # 2-D: D2Q9 MRT + two D2Q5 at (8n)^2
     m2 = 8 * n

@@ -844,23 +844,24 @@ cudaError_t slab_adjoint_step(int collision, const typename SP::elem* fn,
   // forms. Every reaction launch precedes the fluid launches (they read its
   // ubar); slots are indexed by absolute plane.
   auto ranges = [&](auto each) {
-    if (g.nz >= 3) each(1, g.nz - 2, std::false_type{});
-    each(0, 1, std::true_type{});
-    if (g.nz >= 2) each(g.nz - 1, 1, std::true_type{});
+    if (g.nz >= 3) each(1, g.nz - 2, 1, std::false_type{});
+    each(0, g.nz >= 2 ? 2 : 1, g.nz - 1, std::true_type{});  // both face planes in one launch
   };
-  ranges([&](int z0, int planes, auto slab) {
+  ranges([&](int z0, int planes, int zs, auto slab) {
     constexpr bool SLAB = decltype(slab)::value;
     Grid gr = g;
     gr.z0 = z0;
+    gr.zs = zs;
     dim3 grid = grid_dims(gr);
     grid.y = (unsigned)planes;
     launch_pdl(reaction_adjoint_kernel<FL, Real, SP, SLAB>, grid, dim3(block_dims(gr)), 0, s, an, bn,
                u_next, la_next, lb_next, la, lb, ubar, gr, rp, slots, faces);
   });
-  ranges([&](int z0, int planes, auto slab) {
+  ranges([&](int z0, int planes, int zs, auto slab) {
     constexpr bool SLAB = decltype(slab)::value;
     Grid gr = g;
     gr.z0 = z0;
+    gr.zs = zs;
     dim3 grid = grid_dims(gr);
     grid.y = (unsigned)planes;
     const dim3 block(block_dims(gr));

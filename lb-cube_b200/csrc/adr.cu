@@ -102,10 +102,10 @@ __device__ __forceinline__ void fluid_reaction_body(const Real* __restrict__ cur
       sums[4] = ca * cb;
     }
   }
-  // partials by absolute plane: a launch over planes [g.z0, g.z0 + gridDim.y)
-  // writes the partials of those planes' blocks
+  // partials by absolute plane (plane_of): a launch over some planes writes
+  // the partials of those planes' blocks
   if constexpr (STATS)
-    block_sum_to<kStatSums>(sums, partials + (((long long)g.z0 + blockIdx.y) * gridDim.x + blockIdx.x) *
+    block_sum_to<kStatSums>(sums, partials + ((long long)plane_of(g) * gridDim.x + blockIdx.x) *
                                                  kStatSums);
 }
 
@@ -143,9 +143,9 @@ __global__ void __launch_bounds__(kThreads, LBCUBE_STATS_MIN_BLOCKS)
 // does the arithmetic of fluid_reaction_kernel, so a box stepped as slabs is
 // bit-identical to the box stepped whole.
 
-// Launch over planes [g.z0, g.z0 + gridDim.y); statistics partials indexed by
-// the absolute plane, so a step split into several plane ranges writes every
-// block's partial once.
+// Launch over planes g.z0 + k * g.zs (k < gridDim.y); statistics partials
+// indexed by the absolute plane, so a step split into several launches writes
+// every block's partial once.
 // UOUT: also store the advecting velocity (the reactive adjoint keeps it with
 // each stored state).
 template <class FL, class Real, int CT, bool STATS, bool UOUT = false>
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   if constexpr (STATS) {
-    const long long blk = ((long long)g.z0 + blockIdx.y) * gridDim.x + blockIdx.x;
+    const long long blk = (long long)plane_of(g) * gridDim.x + blockIdx.x;
     block_sum_to<kStatSums>(sums, partials + blk * kStatSums);
   }
 }
@@ -269,12 +269,14 @@ cudaError_t launch_fluid_reaction_slab(const Real* cur_f, Real* nxt_f, const Rea
   const Real omega_minus = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
   // planes 0 and nz-1 of the range: the SLAB form; planes in between pull and
   // send nothing across a face: the whole-box kernel (fewer registers)
-  auto launch = [&](int z0, int z1, bool face) {
-    if (z0 >= z1) return;
+  // `planes` planes from z0, `zs` apart
+  auto launch = [&](int z0, int planes, int zs, bool face) {
+    if (planes <= 0) return;
     Grid gr = g;
     gr.z0 = z0;
+    gr.zs = zs;
     dim3 grid = grid_dims(gr);
-    grid.y = (unsigned)(z1 - z0);
+    grid.y = (unsigned)planes;
     const dim3 block(block_dims(gr));
     Real* const none = nullptr;
     if (face && partials != nullptr)
@@ -293,9 +295,14 @@ cudaError_t launch_fluid_reaction_slab(const Real* cur_f, Real* nxt_f, const Rea
                  cur_a, nxt_a, cur_b, nxt_b, gr, omega, omega_minus, omega_c, k, (double*)nullptr, none);
   };
   const int zb = (int)z_begin, ze = (int)z_end, last = g.nz - 1;
-  if (zb == 0) launch(0, 1, true);
-  launch(std::max(zb, 1), std::min(ze, last), false);
-  if (ze - 1 == last && last > 0 && zb <= last) launch(last, last + 1, true);
+  const bool lo = zb == 0, hi = ze - 1 == last && last > 0 && zb <= last;
+  launch(std::max(zb, 1), std::min(ze, last) - std::max(zb, 1), 1, false);
+  if (lo && hi) {
+    launch(0, 2, last, true);  // both face planes in one launch
+  } else {
+    if (lo) launch(0, 1, 1, true);
+    if (hi) launch(last, 1, 1, true);
+  }
   return cudaGetLastError();
 }
 
@@ -438,9 +445,10 @@ cudaError_t fluid_reaction_slab_with_velocity(int collision, const Real* cur_f, 
   auto run = [&](auto ct) -> cudaError_t {
     constexpr int CT = decltype(ct)::value;
     const Real om = CT == kTRT ? trt_omega_minus<Real>(omega) : Real(0);
-    auto launch = [&](int z0, int planes, bool face) {
+    auto launch = [&](int z0, int planes, int zs, bool face) {
       Grid gr = g;
       gr.z0 = z0;
+      gr.zs = zs;
       dim3 grid = grid_dims(gr);
       grid.y = (unsigned)planes;
       const dim3 block(block_dims(gr));
@@ -460,9 +468,8 @@ cudaError_t fluid_reaction_slab_with_velocity(int collision, const Real* cur_f, 
         launch_pdl(fluid_reaction_kernel<FL, Real, CT, false, false>, grid, block, 0, s, cur_f, nxt_f,
                    cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, none, (Real*)nullptr);
     };
-    if (g.nz >= 3) launch(1, g.nz - 2, false);
-    launch(0, 1, true);
-    if (g.nz >= 2) launch(g.nz - 1, 1, true);
+    if (g.nz >= 3) launch(1, g.nz - 2, 1, false);
+    launch(0, g.nz >= 2 ? 2 : 1, g.nz - 1, true);  // both face planes in one launch
     return cudaGetLastError();
   };
   if (collision == kBGK) return run(std::integral_constant<int, kBGK>{});

@@ -197,10 +197,11 @@ cudaError_t fluid_reaction_shifted_slab(int collision, const unsigned short* cur
   auto launch = [&](auto ct) -> cudaError_t {
     constexpr int CT = decltype(ct)::value;
     const float om = CT == kTRT ? trt_omega_minus<float>(omega) : 0.0f;
-    auto range = [&](int z0, int planes, auto slab) {
+    auto range = [&](int z0, int planes, int zs, auto slab) {
       constexpr bool SLAB = decltype(slab)::value;
       Grid gr = g;
       gr.z0 = z0;
+      gr.zs = zs;
       dim3 grid = grid_dims(gr);
       grid.y = (unsigned)planes;
       const dim3 block(block_dims(gr));
@@ -213,9 +214,8 @@ cudaError_t fluid_reaction_shifted_slab(int collision, const unsigned short* cur
                    nxt_f, cur_a, nxt_a, cur_b, nxt_b, gr, omega, om, omega_c, k, rho0, c0, none,
                    (float*)nullptr, faces);
     };
-    if (g.nz >= 3) range(1, g.nz - 2, std::false_type{});
-    range(0, 1, std::true_type{});
-    if (g.nz >= 2) range(g.nz - 1, 1, std::true_type{});
+    if (g.nz >= 3) range(1, g.nz - 2, 1, std::false_type{});
+    range(0, g.nz >= 2 ? 2 : 1, g.nz - 1, std::true_type{});  // both face planes in one launch
     return cudaGetLastError();
   };
   switch (collision) {

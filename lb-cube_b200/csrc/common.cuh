@@ -26,17 +26,22 @@ struct Grid {
   int xblocks;
   int bx;           // threads per block
   long long plane;  // cells per population plane, nx * ny * nz (< 2^31)
-  int z0 = 0;       // first z plane of the launch (blockIdx.y = z - z0)
+  int z0 = 0;       // first z plane of the launch
+  int zs = 1;       // planes between consecutive blockIdx.y: z = z0 + blockIdx.y * zs (both face
+                    // planes of a slab in one launch: z0 = 0, zs = nz - 1)
 
   __host__ __device__ long long blocks() const { return (long long)xblocks * ny * nz; }
 };
+
+// The z plane of this block.
+__device__ __forceinline__ int plane_of(const Grid& g) { return g.z0 + (int)blockIdx.y * g.zs; }
 
 __device__ __forceinline__ bool cell_of(const Grid& g, int& x, int& y, int& z) {
   const int row = blockIdx.x / g.xblocks;
   const int xb = blockIdx.x - row * g.xblocks;
   x = xb * g.bx + threadIdx.x;
   y = row;
-  z = g.z0 + blockIdx.y;
+  z = plane_of(g);
   return x < g.nx;
 }
 

@@ -57,11 +57,11 @@ __device__ __forceinline__ long long warp_slot() {
   return (long long)block_linear() * (kThreads / 32) + (long long)(threadIdx.x >> 5);
 }
 
-// The same for a launch over planes [g.z0, g.z0 + gridDim.y): blocks indexed by
-// their absolute plane, so launches over different plane ranges of one field
-// use disjoint slots (the same slots as one launch over every plane).
+// The same for a launch over some planes of a field (plane_of): blocks indexed
+// by their absolute plane, so launches over different planes of one field use
+// disjoint slots (the same slots as one launch over every plane).
 __device__ __forceinline__ long long warp_slot(const Grid& g) {
-  return ((long long)(g.z0 + (int)blockIdx.y) * gridDim.x + blockIdx.x) * (kThreads / 32) +
+  return ((long long)plane_of(g) * gridDim.x + blockIdx.x) * (kThreads / 32) +
          (long long)(threadIdx.x >> 5);
 }
 

@@ -153,16 +153,23 @@ cudaError_t launch_shifted_slab_step(const void* cur_v, void* nxt_v, size_t nx, 
     launch_vec_step<L, S, CT>(vg, grid, vec_block_threads(vg), stream, cur, nxt, omega, omega_minus, p);
     vg.z0 = 0;
   }
-  auto face = [&](size_t z) {
+  // `count` face planes from z, `step` apart (both faces in one launch where
+  // the range has both)
+  auto face = [&](size_t z, unsigned count, int step) {
     dim3 grid = vec_grid_dims(vg);
-    grid.y = 1;
+    grid.y = count;
     SlabArgs<E> f = faces;
     f.z_begin = (int)z;
+    f.z_step = step;
     launch_pdl(fluid_step_vec_kernel<L, S, CT, false, true>, grid, dim3(vec_block_threads(vg)), 0, stream,
                cur, nxt, vg, omega, omega_minus, p, (double*)nullptr, f);
   };
-  if (lo_face) face(0);
-  if (hi_face && nz > 1) face(nz - 1);
+  if (lo_face && hi_face && nz > 1) {
+    face(0, 2, (int)nz - 1);
+  } else {
+    if (lo_face) face(0, 1, 1);
+    if (hi_face && nz > 1) face(nz - 1, 1, 1);
+  }
   return cudaGetLastError();
 }
 

@@ -76,15 +76,22 @@ cudaError_t launch_slab_step(const Real* cur, Real* nxt, size_t nx, size_t ny, s
                  omega, omega_minus, (double*)nullptr);
     }
   }
-  auto face = [&](size_t z) {
+  // the face planes: `count` planes from z, `step` apart (both faces of the
+  // slab in one launch where the range has both)
+  auto faces = [&](size_t z, unsigned count, int step) {
     dim3 grid = vec_grid_dims(vg);
-    grid.y = 1;
-    const SlabArgs<Real> slab{halo_lo, halo_hi, send_lo, send_hi, (int)z};
+    grid.y = count;
+    SlabArgs<Real> slab{halo_lo, halo_hi, send_lo, send_hi, (int)z};
+    slab.z_step = step;
     launch_pdl(fluid_step_vec_kernel<L, S, CT, false, true>, grid, dim3(vec_block_threads(vg)), 0, s, cur,
                nxt, vg, omega, omega_minus, typename S::Params{}, (double*)nullptr, slab);
   };
-  if (lo_face) face(0);
-  if (hi_face && nz > 1) face(nz - 1);
+  if (lo_face && hi_face && nz > 1) {
+    faces(0, 2, (int)nz - 1);
+  } else {
+    if (lo_face) faces(0, 1, 1);
+    if (hi_face && nz > 1) faces(nz - 1, 1, 1);
+  }
   return cudaGetLastError();
 }
 

@@ -10,7 +10,7 @@
 // and writes the Q results to the next buffer at its own cell. A warp covers 32
 // consecutive x cells, so each of the Q gathers and Q stores is one coalesced
 // 128-byte row segment (shifted by at most one element for c_x != 0, which the
-// L1/L2 sector reuse absorbs). Planes g.z0 .. g.z0 + gridDim.y - 1 are stepped.
+// L1/L2 sector reuse absorbs). Planes g.z0 + k * g.zs (k < gridDim.y) are stepped.
 #pragma once
 #include "collide.cuh"
 #include "common.cuh"

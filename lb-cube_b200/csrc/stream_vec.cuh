@@ -248,7 +248,8 @@ struct SlabArgs {
   const E* halo_hi;  // c_z = -1 populations of the upper neighbour's bottom plane
   E* send_lo;        // this step's c_z = -1 populations of plane 0 (for the lower neighbour)
   E* send_hi;        // this step's c_z = +1 populations of plane nz - 1 (for the upper one)
-  int z_begin;       // first plane of this launch (grid.y planes from here)
+  int z_begin;       // first plane of this launch
+  int z_step = 1;    // planes between consecutive blockIdx.y (both faces in one launch: nz - 1)
 };
 
 // Gathers the Q populations of V cells (x0 .. x0+V-1, row y, slice z) and
@@ -346,8 +347,8 @@ __device__ __forceinline__ void store_vec(typename S::elem* __restrict__ nxt, co
 // block into partials[block_linear() * kDiagPartials ..]. In the pull scheme
 // the populations a thread writes are exactly the next buffer's populations of
 // its own cells, so this costs no memory traffic. Native storage only.
-// SLAB: one launch over planes [slab.z_begin, slab.z_begin + gridDim.y) of a
-// z-slab, with halo planes at the slab faces (see SlabArgs).
+// SLAB: one launch over planes slab.z_begin + k * slab.z_step (k < gridDim.y)
+// of a z-slab, with halo planes at the slab faces (see SlabArgs).
 template <class L, class S, int CT, bool DIAG, bool SLAB>
 __device__ __forceinline__ void fluid_step_vec_body(const typename S::elem* __restrict__ cur,
                                                     typename S::elem* __restrict__ nxt,
@@ -364,7 +365,7 @@ __device__ __forceinline__ void fluid_step_vec_body(const typename S::elem* __re
   const int xb = blockIdx.x - yb * vg.xblocks;
   const int x0 = (xb * vg.tx + (int)(threadIdx.x % vg.tx)) * V;
   const int y = yb * vg.ty + (int)(threadIdx.x / vg.tx);
-  const int z = SLAB ? slab.z_begin + (int)blockIdx.y : vg.z0 + (int)blockIdx.y;
+  const int z = SLAB ? slab.z_begin + (int)blockIdx.y * slab.z_step : vg.z0 + (int)blockIdx.y;
   const bool active = x0 < g.nx && y < g.ny;
   R f[V][L::Q];
   gather_vec<L, S, SLAB>(cur, g, x0, y < g.ny ? y : 0, z, active, p, f, slab);
